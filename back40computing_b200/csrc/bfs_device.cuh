@@ -1,0 +1,209 @@
+// Device-side building blocks of the B200 BFS kernels (sm_100a).
+//
+// Replaces b40c/util/{global_barrier,cta_work_progress,io/*,scan/*}.cuh with
+// sm_100 idioms:
+//   * a grid barrier of one arrival counter and a generation word, with
+//     release/acquire at GPU scope and a %globaltimer spin limit, in place of
+//     GlobalBarrier::Sync (util/global_barrier.cuh:80-126), which polls one
+//     flag per CTA from block 0 and spins without bound;
+//   * queue/steal/big-list counters in a 4-entry ring indexed by iteration,
+//     as CtaWorkProgress keeps queue counters at [iteration & 3]
+//     (util/cta_work_progress.cuh:69-223);
+//   * warp-shuffle scans in place of the raking smem scans
+//     (util/scan/cooperative_scan.cuh:173-195);
+//   * visited-bitmask culling with atomicOr, which makes the mask exact (the
+//     reference's mask store is a best-effort race, contract_expand_atomic/
+//     cta.cuh:213-258, backed by a label check, :264-304).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace b40c_b200 {
+
+// ---- error bits raised on the device (Counters::error) ----------------------
+enum : unsigned {
+    ERR_OVERFLOW = 1u,         // frontier queue capacity exceeded
+    ERR_BARRIER_TIMEOUT = 2u,  // a grid barrier wait ran past its limit
+    ERR_BAD_VERTEX = 4u,       // a column index >= nodes (malformed CSR)
+    ERR_LEVEL_LIMIT = 8u,      // more levels than vertices: visited state inconsistent
+};
+
+// A BFS has at most nodes levels; the level loops stop (with ERR_LEVEL_LIMIT)
+// past this bound so no persistent kernel can spin without end.
+__device__ __forceinline__ bool level_limit_hit(int it, int nodes) { return it > nodes + 2; }
+
+// Per-search device counters.  ring[x][it & 3] as CtaWorkProgress does.
+struct alignas(128) Counters {
+    unsigned qlen[4];    // qlen[it&3]: length of the input frontier of iteration it
+    unsigned steal[4];   // steal[it&3]: next tile to hand out in iteration it
+    unsigned big[4];     // big[it&3]: big-list items pushed in iteration it
+    unsigned error;      // ERR_* bits
+    int iteration;       // iteration counter at exit (reference d_iteration)
+    int cur_it;          // current iteration for per-level (graph-driven) kernels
+    unsigned done;       // 1 once the search has finished (per-level variants)
+    unsigned long long total_queued;  // sum of frontier lengths (instrumented)
+    unsigned pad0[8];
+    // Grid barrier in its own 128-byte line.
+    alignas(128) unsigned bar_count;
+    unsigned bar_gen;
+    unsigned pad1[29];
+    unsigned sticky;  // OR of error over searches since the host last read it (not reset per search)
+};
+
+// ---- PTX helpers ---------------------------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_gpu(unsigned *p, unsigned v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned atom_add_acqrel_gpu(unsigned *p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// L2-coherent load of data written by other CTAs during this kernel (skips L1).
+__device__ __forceinline__ int ld_cg(const int *p) { return __ldcg(p); }
+__device__ __forceinline__ unsigned ld_cg(const unsigned *p) { return __ldcg(p); }
+
+// L2 eviction-priority policies (createpolicy, sm_80+): stream the column
+// indices through L2 with evict_first so the visited mask, labels and row
+// offsets stay resident.
+__device__ __forceinline__ uint64_t policy_evict_first() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ int4 ldg_stream_v4(const int *p, uint64_t pol) {
+    int4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ldg_stream(const int *p, uint64_t pol) {
+    int v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
+                 : "=r"(v)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ---- grid barrier ----------------------------------------------------------------
+// All CTAs of a cooperative launch call this the same number of times.  Each
+// CTA's thread 0 reads the generation, arrives with an acq_rel add, and either
+// (last arrival) resets the count and publishes generation+1, or spins with an
+// acquire load until the generation moves, the error word becomes non-zero, or
+// wait_ns of %globaltimer time pass (then ERR_BARRIER_TIMEOUT is raised and
+// the CTA leaves the wait).  Returns false on any raised error, identically
+// for every thread of the CTA.
+__device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wait_ns,
+                                             unsigned *smem_flag, unsigned expected) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned gen = ld_acquire_gpu(&c->bar_gen);
+        unsigned arrived = atom_add_acqrel_gpu(&c->bar_count, 1u);
+        if (arrived == expected - 1) {
+            st_relaxed_gpu(&c->bar_count, 0u);
+            st_release_gpu(&c->bar_gen, gen + 1u);
+        } else {
+            unsigned long long t0 = globaltimer_ns();
+            unsigned ns = 32;
+            while (ld_acquire_gpu(&c->bar_gen) == gen) {
+                if (ld_relaxed_gpu(&c->error) != 0u) break;
+                if (globaltimer_ns() - t0 > wait_ns) {
+                    atomicOr(&c->error, ERR_BARRIER_TIMEOUT);
+                    break;
+                }
+                __nanosleep(ns);
+                if (ns < 256) ns <<= 1;
+            }
+        }
+        *smem_flag = ld_relaxed_gpu(&c->error);
+    }
+    __syncthreads();
+    return *smem_flag == 0u;
+}
+__device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wait_ns,
+                                             unsigned *smem_flag) {
+    return grid_barrier(c, wait_ns, smem_flag, gridDim.x);
+}
+
+// ---- scans -------------------------------------------------------------------------
+__device__ __forceinline__ int warp_inclusive_scan(int x) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, d);
+        if ((int)lane_id() >= d) x += y;
+    }
+    return x;
+}
+
+// Block-wide exclusive scan of two components at once (the reference's SoA
+// scan of (coarse, fine) ranks, contract_expand_atomic/cta.cuh:624-633).
+// warp_tot must hold THREADS/32 int2 in shared memory.  Ends with a barrier
+// so warp_tot may be reused right after.
+template <int THREADS>
+__device__ __forceinline__ int2 block_exclusive_scan2(int2 v, int2 &total, int2 *warp_tot) {
+    constexpr int WARPS = THREADS / 32;
+    const int lane = lane_id(), warp = threadIdx.x >> 5;
+    int ix = warp_inclusive_scan(v.x);
+    int iy = warp_inclusive_scan(v.y);
+    if (lane == 31) warp_tot[warp] = make_int2(ix, iy);
+    __syncthreads();
+    if (warp == 0) {
+        int2 t = lane < WARPS ? warp_tot[lane] : make_int2(0, 0);
+        int sx = warp_inclusive_scan(t.x);
+        int sy = warp_inclusive_scan(t.y);
+        if (lane < WARPS) warp_tot[lane] = make_int2(sx - t.x, sy - t.y);  // exclusive warp bases
+        if (lane == WARPS - 1) warp_tot[WARPS] = make_int2(sx, sy);       // block total
+    }
+    __syncthreads();
+    int2 base = warp_tot[warp];
+    total = warp_tot[WARPS];
+    __syncthreads();
+    return make_int2(base.x + ix - v.x, base.y + iy - v.y);
+}
+
+template <int THREADS>
+__device__ __forceinline__ int block_exclusive_scan(int v, int &total, int2 *warp_tot) {
+    int2 t2;
+    int2 r = block_exclusive_scan2<THREADS>(make_int2(v, 0), t2, warp_tot);
+    total = t2.x;
+    return r.x;
+}
+
+// ---- visited mask ------------------------------------------------------------------
+// Exact test-and-set of vertex u's bit: a cheap L2 read first, and an atomicOr
+// only when the bit looked clear.  Returns true for exactly one caller per
+// vertex over the whole search.
+__device__ __forceinline__ bool mark_visited(unsigned *mask, int u) {
+    unsigned w = unsigned(u) >> 5, bit = 1u << (unsigned(u) & 31u);
+    if (ld_cg(mask + w) & bit) return false;
+    return (atomicOr(mask + w, bit) & bit) == 0u;
+}
+
+}  // namespace b40c_b200

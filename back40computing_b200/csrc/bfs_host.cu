@@ -1,0 +1,673 @@
+// Host orchestration and C ABI of libb40c_bfs: CsrProblem and the enactors.
+//
+// b40c_problem mirrors bfs::CsrProblem<int,int,MARK_PREDECESSORS>
+// (b40c/graph/bfs/csr_problem.cuh:68-751) for one GPU: it owns the device CSR,
+// labels, visited mask and frontier queues.  b40c_enactor mirrors the
+// Enactor{ExpandContract,ContractExpand,TwoPhase} classes: it owns the search
+// counters, the big-list table, its stream, timing events and the cached
+// per-level CUDA graph.  Each entry point returns a cudaError_t value and
+// records a message in the thread's error slot (B40CPerror,
+// b40c/util/error_utils.cuh:44-103).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "b40c_bfs.h"
+#include "bfs_kernels.cuh"
+#include "host_common.h"
+
+namespace b40c_b200 {
+
+static thread_local char g_error[512];
+
+int set_error(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_error, sizeof(g_error), fmt, ap);
+    va_end(ap);
+    if (code && getenv("B40C_VERBOSE_ERRORS")) fprintf(stderr, "[b40c_bfs] %s (error %d)\n", g_error, code);
+    return code;
+}
+void clear_error() { g_error[0] = 0; }
+const char *last_error() { return g_error; }
+
+static int cuda_fail(cudaError_t e, const char *what) {
+    return set_error(int(e), "%s failed (CUDA error %d: %s)", what, int(e), cudaGetErrorString(e));
+}
+#define CUDA_TRY(call, what)                            \
+    do {                                                \
+        cudaError_t _e = (call);                        \
+        if (_e != cudaSuccess) return cuda_fail(_e, what); \
+    } while (0)
+
+}  // namespace b40c_b200
+
+using namespace b40c_b200;
+
+struct b40c_problem {
+    int device = 0;
+    bool mark_pred = false;
+    int64_t nodes = 0, edges = 0;
+    bool mapped = false;  // stream_from_host
+    std::vector<void *> registered;
+    int *d_row_offsets = nullptr;
+    int *d_col = nullptr;
+    int *d_labels = nullptr;
+    unsigned *d_mask = nullptr;
+    size_t mask_bytes = 0;
+    int *d_queue[2] = {nullptr, nullptr};
+    int *d_pred[2] = {nullptr, nullptr};
+    long long queue_elems[2] = {0, 0};
+    long long pred_elems[2] = {0, 0};
+    bool reset_once = false;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+};
+
+struct b40c_enactor {
+    int device = 0;
+    int strategy = B40C_EXPAND_CONTRACT;
+    bool instrument = false, debug = false;
+    int threads = 256;
+    int warp_th = 32, cta_th = 512, big_th = 8192;
+    unsigned cull_flags = 0;
+    unsigned long long wait_ns = 5000000000ull;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    Counters *d_ctr = nullptr;
+    Counters *h_ctr = nullptr;  // pinned
+    int4 *d_big = nullptr;
+    int big_cap = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.f;
+    int last_iteration = 0;
+    long long last_total_queued = 0;
+    bool have_stats = false;
+    bool timing_pending = false;
+    // cached per-level graph
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    BfsParams gparams{};
+    KernelConfig gkc{};
+    int ggrid = 0;
+};
+
+namespace {
+
+cudaStream_t problem_stream(b40c_problem *p) { return p->stream ? p->stream : p->own_stream; }
+cudaStream_t enactor_stream(b40c_enactor *e) { return e->stream ? e->stream : e->own_stream; }
+
+int check_csr(int64_t nodes, int64_t edges, const int *row, const int *col) {
+    if (row[0] != 0) return set_error(B40C_ERR_INVALID_VALUE, "CSR row_offsets[0] = %d, expected 0", row[0]);
+    if (row[nodes] != edges)
+        return set_error(B40C_ERR_INVALID_VALUE, "CSR row_offsets[nodes] = %d, expected edges = %lld",
+                         row[nodes], (long long)edges);
+    for (int64_t v = 0; v < nodes; v++)
+        if (row[v + 1] < row[v])
+            return set_error(B40C_ERR_INVALID_VALUE, "CSR row_offsets decrease at row %lld", (long long)v);
+    // Column ids checked on several threads (the arrays can be ~10^8 entries).
+    unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<int64_t> bad(nt, -1);
+    std::vector<std::thread> pool;
+    int64_t chunk = (edges + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; t++) {
+        pool.emplace_back([&, t] {
+            int64_t lo = std::min<int64_t>(edges, t * chunk), hi = std::min<int64_t>(edges, lo + chunk);
+            for (int64_t k = lo; k < hi; k++)
+                if ((unsigned)col[k] >= (unsigned)nodes) {
+                    bad[t] = k;
+                    break;
+                }
+        });
+    }
+    for (auto &th : pool) th.join();
+    for (unsigned t = 0; t < nt; t++)
+        if (bad[t] >= 0)
+            return set_error(B40C_ERR_INVALID_VALUE, "CSR column index %d at edge %lld outside [0, %lld)",
+                             col[bad[t]], (long long)bad[t], (long long)nodes);
+    return B40C_SUCCESS;
+}
+
+void free_problem_device(b40c_problem *p) {
+    if (!p->mapped) {
+        cudaFree(p->d_row_offsets);
+        cudaFree(p->d_col);
+    }
+    for (void *h : p->registered) cudaHostUnregister(h);
+    p->registered.clear();
+    p->d_row_offsets = nullptr;
+    p->d_col = nullptr;
+    cudaFree(p->d_labels);
+    cudaFree(p->d_mask);
+    p->d_labels = nullptr;
+    p->d_mask = nullptr;
+    for (int i = 0; i < 2; i++) {
+        cudaFree(p->d_queue[i]);
+        cudaFree(p->d_pred[i]);
+        p->d_queue[i] = p->d_pred[i] = nullptr;
+        p->queue_elems[i] = p->pred_elems[i] = 0;
+    }
+}
+
+int map_host(b40c_problem *p, const void *h, size_t bytes, void **d) {
+    cudaPointerAttributes attr{};
+    cudaError_t e = cudaPointerGetAttributes(&attr, h);
+    if (e != cudaSuccess) cudaGetLastError();
+    if (e != cudaSuccess || attr.type != cudaMemoryTypeHost) {
+        e = cudaHostRegister(const_cast<void *>(h), bytes, cudaHostRegisterMapped | cudaHostRegisterReadOnly);
+        if (e != cudaSuccess) return cuda_fail(e, "CsrProblem cudaHostRegister (stream_from_host)");
+        p->registered.push_back(const_cast<void *>(h));
+    }
+    CUDA_TRY(cudaHostGetDevicePointer(d, const_cast<void *>(h), 0), "CsrProblem cudaHostGetDevicePointer");
+    return B40C_SUCCESS;
+}
+
+int translate_device_error(unsigned err) {
+    if (err & ERR_BAD_VERTEX)
+        return set_error(B40C_ERR_INVALID_VALUE, "column index outside [0, nodes) met during the search");
+    if (err & ERR_BARRIER_TIMEOUT)
+        return set_error(B40C_ERR_LAUNCH_TIMEOUT,
+                         "grid barrier wait exceeded its limit; search abandoned (context still usable)");
+    if (err & ERR_LEVEL_LIMIT)
+        return set_error(B40C_ERR_LAUNCH_TIMEOUT, "level loop passed nodes + 2 levels; search abandoned");
+    if (err & ERR_OVERFLOW)
+        return set_error(B40C_ERR_INVALID_CONFIGURATION,
+                         "Frontier queue overflow.  Please increase queue-sizing factor.");
+    return B40C_SUCCESS;
+}
+
+int ensure_enactor_buffers(b40c_enactor *e, b40c_problem *p) {
+    if (!e->d_ctr) {
+        CUDA_TRY(cudaMalloc(&e->d_ctr, sizeof(Counters)), "Enactor cudaMalloc counters");
+        CUDA_TRY(cudaMemset(e->d_ctr, 0, sizeof(Counters)), "Enactor cudaMemset counters");
+        CUDA_TRY(cudaHostAlloc(&e->h_ctr, sizeof(Counters), cudaHostAllocDefault), "Enactor cudaHostAlloc");
+        std::memset(e->h_ctr, 0, sizeof(Counters));
+    }
+    // Big lists per level are at most edges / big_th (each vertex expands once).
+    long long need = p->edges / std::max(1, e->big_th) + 64;
+    if (need > (1ll << 30)) need = 1ll << 30;
+    if (e->big_cap < need) {
+        cudaFree(e->d_big);
+        e->d_big = nullptr;
+        e->big_cap = 0;
+        CUDA_TRY(cudaMalloc(&e->d_big, sizeof(int4) * size_t(need)), "Enactor cudaMalloc big-list table");
+        e->big_cap = int(need);
+    }
+    return B40C_SUCCESS;
+}
+
+int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
+    bp = BfsParams{};
+    bp.row_offsets = p->d_row_offsets;
+    bp.col = p->d_col;
+    bp.labels = p->d_labels;
+    bp.mask = p->d_mask;
+    for (int i = 0; i < 2; i++) {
+        bp.queue[i] = p->d_queue[i];
+        bp.pred_queue[i] = p->d_pred[i];
+    }
+    bp.big_items = e->d_big;
+    bp.ctr = e->d_ctr;
+    bp.wait_ns = e->wait_ns;
+    long long qcap = std::min(p->queue_elems[0], p->queue_elems[1]);
+    if (p->mark_pred && e->strategy != B40C_EXPAND_CONTRACT)
+        qcap = std::min(qcap, std::min(p->pred_elems[0], p->pred_elems[1]));
+    if (qcap > 0xffffffffll) qcap = 0xffffffffll;
+    bp.qcap = qcap;
+    bp.big_cap = e->big_cap;
+    bp.vec_end = p->mapped ? int(p->edges & ~int64_t(3)) : int(p->edges + 4);
+    bp.nodes = int(p->nodes);
+    bp.src = src;
+    bp.warp_th = e->warp_th;
+    bp.cta_th = std::max(e->cta_th, e->warp_th);
+    bp.big_th = std::max(e->big_th, bp.cta_th);
+    bp.cull_flags = e->cull_flags;
+    if (qcap < 1) return set_error(B40C_ERR_ILLEGAL_STATE, "frontier queues not allocated: call Reset first");
+    if (p->mark_pred && e->strategy != B40C_EXPAND_CONTRACT && (!p->d_pred[0] || !p->d_pred[1]))
+        return set_error(B40C_ERR_ILLEGAL_STATE,
+                         "predecessor queues missing: Reset with this enactor's frontier type");
+    return B40C_SUCCESS;
+}
+
+int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size, int variant) {
+    if (!e || !p) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor or problem");
+    if (!p->d_col || !p->d_labels || !p->reset_once)
+        return set_error(B40C_ERR_ILLEGAL_STATE, "problem needs FromHostProblem and Reset before a search");
+    if (src < 0 || src >= p->nodes)
+        return set_error(B40C_ERR_INVALID_VALUE, "source %d outside [0, %lld)", src, (long long)p->nodes);
+    if (e->strategy == B40C_HYBRID)
+        return set_error(B40C_ERR_NOT_SUPPORTED, "hybrid strategy not available in this build");
+    int rc = ensure_enactor_buffers(e, p);
+    if (rc) return rc;
+    BfsParams bp;
+    if ((rc = fill_params(e, p, src, bp))) return rc;
+    KernelConfig kc{e->strategy, e->threads, p->mark_pred};
+    cudaStream_t s = enactor_stream(e);
+    // The problem's pending work (Reset) precedes the search.
+    cudaStream_t ps = problem_stream(p);
+    if (ps != s) {
+        cudaEvent_t dep;
+        CUDA_TRY(cudaEventCreateWithFlags(&dep, cudaEventDisableTiming), "cudaEventCreate");
+        cudaEventRecord(dep, ps);
+        cudaStreamWaitEvent(s, dep, 0);
+        cudaEventDestroy(dep);
+    }
+    if (variant == B40C_VARIANT_DEFAULT) variant = B40C_VARIANT_FUSED;
+    CUDA_TRY(cudaEventRecord(e->ev0, s), "cudaEventRecord");
+    CUDA_TRY(launch_search_init(bp, kc, s), "search init kernel launch");
+    if (variant == B40C_VARIANT_FUSED) {
+        int limit = 0;
+        CUDA_TRY(fused_grid_limit(kc, &limit), "occupancy query");
+        int grid = max_grid_size > 0 ? std::min(max_grid_size, limit) : limit;
+        CUDA_TRY(launch_fused(bp, kc, grid, s), "cooperative launch of the fused BFS kernel");
+    } else if (variant == B40C_VARIANT_ITERATIVE) {
+        int limit = 0;
+        CUDA_TRY(level_grid_limit(kc, &limit), "occupancy query");
+        int grid = max_grid_size > 0 ? std::min(max_grid_size, limit) : limit;
+        BfsParams key = bp;
+        key.cond_handle = e->gparams.cond_handle;
+        bool reuse = e->gexec && e->ggrid == grid && e->gkc.strategy == kc.strategy &&
+                     e->gkc.threads == kc.threads && e->gkc.mark_pred == kc.mark_pred &&
+                     std::memcmp(&key, &e->gparams, sizeof(BfsParams)) == 0;
+        if (!reuse) {
+            if (e->gexec) cudaGraphExecDestroy(e->gexec);
+            if (e->graph) cudaGraphDestroy(e->graph);
+            e->gexec = nullptr;
+            e->graph = nullptr;
+            BfsParams gp = bp;
+            CUDA_TRY(build_level_graph(gp, kc, grid, &e->gexec, &e->graph), "building the per-level BFS graph");
+            e->gparams = gp;
+            e->gkc = kc;
+            e->ggrid = grid;
+        }
+        CUDA_TRY(cudaGraphLaunch(e->gexec, s), "cudaGraphLaunch");
+    } else {
+        return set_error(B40C_ERR_INVALID_VALUE, "unknown variant %d", variant);
+    }
+    CUDA_TRY(cudaEventRecord(e->ev1, s), "cudaEventRecord");
+    CUDA_TRY(cudaMemcpyAsync(e->h_ctr, e->d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, s),
+             "counters copy");
+    e->timing_pending = true;
+    e->have_stats = false;
+    return B40C_SUCCESS;
+}
+
+// Waits for the enactor stream; reads counters, timing and the sticky error.
+int finish_search(b40c_enactor *e) {
+    cudaStream_t s = enactor_stream(e);
+    CUDA_TRY(cudaStreamSynchronize(s), "BFS search");
+    if (e->timing_pending) {
+        cudaEventElapsedTime(&e->last_ms, e->ev0, e->ev1);
+        e->timing_pending = false;
+    }
+    e->last_iteration = e->h_ctr->iteration;
+    e->last_total_queued = (long long)e->h_ctr->total_queued;
+    e->have_stats = true;
+    unsigned err = e->h_ctr->sticky | e->h_ctr->error;
+    if (err) {
+        CUDA_TRY(cudaMemsetAsync(&e->d_ctr->sticky, 0, sizeof(unsigned), s), "clear sticky error");
+        CUDA_TRY(cudaStreamSynchronize(s), "clear sticky error");
+        e->h_ctr->sticky = 0;
+        return translate_device_error(err);
+    }
+    return B40C_SUCCESS;
+}
+
+}  // namespace
+
+// ---- library ----------------------------------------------------------------------------
+
+extern "C" const char *b40c_last_error_string(void) { return last_error(); }
+extern "C" const char *b40c_version(void) { return "b40c-bfs-b200 0.1 (sm_100a)"; }
+
+// ---- CsrProblem -----------------------------------------------------------------------
+
+extern "C" int b40c_problem_create(int mark_predecessors, b40c_problem_t **out) {
+    clear_error();
+    if (!out) return set_error(B40C_ERR_INVALID_VALUE, "NULL out");
+    b40c_problem *p = new (std::nothrow) b40c_problem();
+    if (!p) return set_error(B40C_ERR_MEMORY_ALLOCATION, "problem allocation");
+    p->mark_pred = mark_predecessors != 0;
+    cudaError_t e = cudaGetDevice(&p->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete p;
+        return cuda_fail(e, "CsrProblem stream creation");
+    }
+    *out = p;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_problem_destroy(b40c_problem_t *p) {
+    clear_error();
+    if (!p) return B40C_SUCCESS;
+    cudaSetDevice(p->device);
+    cudaStreamSynchronize(problem_stream(p));
+    free_problem_device(p);
+    if (p->own_stream) cudaStreamDestroy(p->own_stream);
+    delete p;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_problem_from_host(b40c_problem_t *p, int stream_from_host, int nodes, int edges,
+                                      const int *h_col, const int *h_row, int num_gpus) {
+    clear_error();
+    if (!p || nodes <= 0 || edges < 0 || !h_row || (edges > 0 && !h_col))
+        return set_error(B40C_ERR_INVALID_VALUE, "FromHostProblem: invalid arguments");
+    if (num_gpus > 1)
+        return set_error(B40C_ERR_NOT_SUPPORTED, "FromHostProblem: multi-GPU slices are not provided");
+    if (edges > INT32_MAX - 8192)
+        return set_error(B40C_ERR_INVALID_VALUE, "FromHostProblem: %d edges too many for int32 SizeT", edges);
+    int rc = check_csr(nodes, edges, h_row, h_col);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(p->device), "cudaSetDevice");
+    cudaStreamSynchronize(problem_stream(p));
+    free_problem_device(p);
+    p->nodes = nodes;
+    p->edges = edges;
+    p->reset_once = false;
+    p->mapped = stream_from_host != 0;
+    if (p->mapped) {
+        if ((rc = map_host(p, h_row, sizeof(int) * (size_t(nodes) + 1), (void **)&p->d_row_offsets))) return rc;
+        if (edges > 0 && (rc = map_host(p, h_col, sizeof(int) * size_t(edges), (void **)&p->d_col))) return rc;
+        if (edges == 0) {
+            CUDA_TRY(cudaMalloc(&p->d_col, 16), "cudaMalloc column_indices");
+            p->mapped = false;  // nothing to stream; treat as device copy
+            CUDA_TRY(cudaMalloc(&p->d_row_offsets, sizeof(int) * (size_t(nodes) + 1)), "cudaMalloc row_offsets");
+            CUDA_TRY(cudaMemcpy(p->d_row_offsets, h_row, sizeof(int) * (size_t(nodes) + 1), cudaMemcpyHostToDevice),
+                     "cudaMemcpy row_offsets");
+        }
+    } else {
+        // Column array padded with 4 entries for 16-byte tail loads.
+        CUDA_TRY(cudaMalloc(&p->d_col, sizeof(int) * (size_t(edges) + 4)), "CsrProblem cudaMalloc d_column_indices");
+        CUDA_TRY(cudaMemset(p->d_col + edges, 0, 4 * sizeof(int)), "cudaMemset column padding");
+        if (edges)
+            CUDA_TRY(cudaMemcpy(p->d_col, h_col, sizeof(int) * size_t(edges), cudaMemcpyHostToDevice),
+                     "CsrProblem cudaMemcpy d_column_indices");
+        CUDA_TRY(cudaMalloc(&p->d_row_offsets, sizeof(int) * (size_t(nodes) + 1)), "CsrProblem cudaMalloc d_row_offsets");
+        CUDA_TRY(cudaMemcpy(p->d_row_offsets, h_row, sizeof(int) * (size_t(nodes) + 1), cudaMemcpyHostToDevice),
+                 "CsrProblem cudaMemcpy d_row_offsets");
+    }
+    return B40C_SUCCESS;
+}
+
+static int problem_reset(b40c_problem *p, int frontier_type, double queue_sizing, bool sync) {
+    if (!p || !p->d_row_offsets) return set_error(B40C_ERR_ILLEGAL_STATE, "Reset before FromHostProblem");
+    if (frontier_type < B40C_VERTEX_FRONTIERS || frontier_type > B40C_MIXED_FRONTIERS)
+        return set_error(B40C_ERR_INVALID_VALUE, "Reset: frontier type %d not provided", frontier_type);
+    if (!(queue_sizing > 0.0)) queue_sizing = 1.3;  // test_bfs.cu:802 default
+    CUDA_TRY(cudaSetDevice(p->device), "cudaSetDevice");
+    cudaStream_t s = problem_stream(p);
+    if (!p->d_labels)
+        CUDA_TRY(cudaMalloc(&p->d_labels, sizeof(int) * size_t(p->nodes)), "CsrProblem cudaMalloc d_labels");
+    if (!p->d_mask) {
+        // ceil(nodes / 8) bytes as the reference (csr_problem.cuh:581-583), rounded to whole words.
+        p->mask_bytes = size_t((p->nodes + 31) / 32) * 4;
+        CUDA_TRY(cudaMalloc(&p->d_mask, p->mask_bytes), "CsrProblem cudaMalloc d_visited_mask");
+    }
+    long long n = p->nodes, m = p->edges;
+    long long want[2] = {0, 0}, wpred[2] = {0, 0};
+    // Queue sizes by frontier type (csr_problem.cuh:600-641).  Exact bitmask
+    // culling bounds a vertex frontier by n and an edge frontier by m, so a
+    // sizing of 1.0 never overflows; smaller factors can, and then the search
+    // reports cudaErrorInvalidConfiguration as the reference does.
+    auto sized = [&](long long base) {
+        long long q = (long long)(double(base) * queue_sizing);
+        return std::max(q, 1ll);
+    };
+    switch (frontier_type) {
+    case B40C_VERTEX_FRONTIERS:
+        want[0] = want[1] = sized(n);
+        break;
+    case B40C_EDGE_FRONTIERS:
+        want[0] = want[1] = sized(std::max(m, n));
+        if (p->mark_pred) wpred[0] = wpred[1] = want[0];
+        break;
+    case B40C_MIXED_FRONTIERS:
+        want[0] = sized(n);
+        want[1] = sized(std::max(m, n));
+        if (p->mark_pred) wpred[1] = want[1];
+        break;
+    }
+    for (int i = 0; i < 2; i++) {
+        if (p->queue_elems[i] < want[i]) {
+            cudaStreamSynchronize(s);
+            cudaFree(p->d_queue[i]);
+            p->d_queue[i] = nullptr;
+            p->queue_elems[i] = 0;
+            CUDA_TRY(cudaMalloc(&p->d_queue[i], sizeof(int) * size_t(want[i])),
+                     "CsrProblem cudaMalloc frontier_queues.d_keys");
+            p->queue_elems[i] = want[i];
+        }
+        if (p->pred_elems[i] < wpred[i]) {
+            cudaStreamSynchronize(s);
+            cudaFree(p->d_pred[i]);
+            p->d_pred[i] = nullptr;
+            p->pred_elems[i] = 0;
+            CUDA_TRY(cudaMalloc(&p->d_pred[i], sizeof(int) * size_t(wpred[i])),
+                     "CsrProblem cudaMalloc frontier_queues.d_values");
+            p->pred_elems[i] = wpred[i];
+        }
+    }
+    // labels := -1, visited mask := 0 (csr_problem.cuh:719-745).
+    CUDA_TRY(cudaMemsetAsync(p->d_labels, 0xff, sizeof(int) * size_t(p->nodes), s), "labels memset");
+    CUDA_TRY(cudaMemsetAsync(p->d_mask, 0, p->mask_bytes, s), "visited mask memset");
+    p->reset_once = true;
+    if (sync) CUDA_TRY(cudaStreamSynchronize(s), "Reset");
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_problem_reset(b40c_problem_t *p, int frontier_type, double queue_sizing) {
+    clear_error();
+    return problem_reset(p, frontier_type, queue_sizing, true);
+}
+
+extern "C" int b40c_problem_reset_async(b40c_problem_t *p, int frontier_type, double queue_sizing) {
+    clear_error();
+    return problem_reset(p, frontier_type, queue_sizing, false);
+}
+
+extern "C" int b40c_problem_extract_results(b40c_problem_t *p, int *h_labels) {
+    clear_error();
+    if (!p || !h_labels) return set_error(B40C_ERR_INVALID_VALUE, "ExtractResults: NULL argument");
+    if (!p->d_labels) return set_error(B40C_ERR_ILLEGAL_STATE, "ExtractResults before Reset");
+    cudaStream_t s = problem_stream(p);
+    CUDA_TRY(cudaMemcpyAsync(h_labels, p->d_labels, sizeof(int) * size_t(p->nodes), cudaMemcpyDeviceToHost, s),
+             "CsrProblem cudaMemcpy d_labels");
+    CUDA_TRY(cudaStreamSynchronize(s), "ExtractResults");
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_problem_extract_results_async(b40c_problem_t *p, int *h_labels) {
+    clear_error();
+    if (!p || !h_labels) return set_error(B40C_ERR_INVALID_VALUE, "ExtractResults: NULL argument");
+    if (!p->d_labels) return set_error(B40C_ERR_ILLEGAL_STATE, "ExtractResults before Reset");
+    CUDA_TRY(cudaMemcpyAsync(h_labels, p->d_labels, sizeof(int) * size_t(p->nodes), cudaMemcpyDeviceToHost,
+                             problem_stream(p)),
+             "CsrProblem cudaMemcpyAsync d_labels");
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_problem_info(b40c_problem_t *p, int64_t *nodes, int64_t *edges, void **d_row_offsets,
+                                 void **d_column_indices, void **d_labels, void **d_visited_mask) {
+    clear_error();
+    if (!p) return set_error(B40C_ERR_INVALID_VALUE, "NULL problem");
+    if (nodes) *nodes = p->nodes;
+    if (edges) *edges = p->edges;
+    if (d_row_offsets) *d_row_offsets = p->d_row_offsets;
+    if (d_column_indices) *d_column_indices = p->d_col;
+    if (d_labels) *d_labels = p->d_labels;
+    if (d_visited_mask) *d_visited_mask = p->d_mask;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_problem_set_stream(b40c_problem_t *p, void *stream) {
+    clear_error();
+    if (!p) return set_error(B40C_ERR_INVALID_VALUE, "NULL problem");
+    p->stream = (cudaStream_t)stream;
+    return B40C_SUCCESS;
+}
+
+// ---- Enactors ---------------------------------------------------------------------------
+
+extern "C" int b40c_enactor_create(int strategy, int instrument, int debug, b40c_enactor_t **out) {
+    clear_error();
+    if (!out) return set_error(B40C_ERR_INVALID_VALUE, "NULL out");
+    if (strategy < B40C_EXPAND_CONTRACT || strategy > B40C_HYBRID)
+        return set_error(B40C_ERR_INVALID_VALUE, "unknown strategy %d", strategy);
+    b40c_enactor *e = new (std::nothrow) b40c_enactor();
+    if (!e) return set_error(B40C_ERR_MEMORY_ALLOCATION, "enactor allocation");
+    e->strategy = strategy;
+    e->instrument = instrument != 0;
+    e->debug = debug != 0;
+    cudaError_t ce = cudaGetDevice(&e->device);
+    if (!ce) ce = cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking);
+    if (!ce) ce = cudaEventCreate(&e->ev0);
+    if (!ce) ce = cudaEventCreate(&e->ev1);
+    if (ce) {
+        if (e->ev0) cudaEventDestroy(e->ev0);
+        if (e->own_stream) cudaStreamDestroy(e->own_stream);
+        delete e;
+        return cuda_fail(ce, "enactor creation");
+    }
+    *out = e;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_destroy(b40c_enactor_t *e) {
+    clear_error();
+    if (!e) return B40C_SUCCESS;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(enactor_stream(e));
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    cudaFree(e->d_ctr);
+    cudaFree(e->d_big);
+    if (e->h_ctr) cudaFreeHost(e->h_ctr);
+    cudaEventDestroy(e->ev0);
+    cudaEventDestroy(e->ev1);
+    if (e->own_stream) cudaStreamDestroy(e->own_stream);
+    delete e;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_frontier_type(b40c_enactor_t *e, int *ft) {
+    clear_error();
+    if (!e || !ft) return set_error(B40C_ERR_INVALID_VALUE, "NULL argument");
+    // EnactorBase(frontier_type): expand-contract uses O(n) vertex queues
+    // (enactor_expand_contract.cuh), the others O(m) edge queues
+    // (enactor_contract_expand.cuh:207, enactor_two_phase.cuh:222).
+    *ft = e->strategy == B40C_EXPAND_CONTRACT ? B40C_VERTEX_FRONTIERS : B40C_EDGE_FRONTIERS;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enact_search(b40c_enactor_t *e, b40c_problem_t *p, int src, int max_grid_size, int variant) {
+    clear_error();
+    int rc = enqueue_search(e, p, src, max_grid_size, variant);
+    if (rc) {
+        if (e) cudaStreamSynchronize(enactor_stream(e));
+        return rc;
+    }
+    rc = finish_search(e);
+    if (!rc) {
+        // Later problem-stream work (ExtractResults) must see the labels.
+        cudaStream_t ps = problem_stream(p);
+        if (ps != enactor_stream(e)) cudaStreamSynchronize(enactor_stream(e));
+    }
+    return rc;
+}
+
+extern "C" int b40c_enact_search_async(b40c_enactor_t *e, b40c_problem_t *p, int src, int max_grid_size,
+                                       int variant) {
+    clear_error();
+    int rc = enqueue_search(e, p, src, max_grid_size, variant);
+    if (rc) return rc;
+    // Order later problem-stream work (reset, extract) after the search.
+    cudaStream_t ps = problem_stream(p), s = enactor_stream(e);
+    if (ps != s) {
+        cudaEvent_t dep;
+        CUDA_TRY(cudaEventCreateWithFlags(&dep, cudaEventDisableTiming), "cudaEventCreate");
+        cudaEventRecord(dep, s);
+        cudaStreamWaitEvent(ps, dep, 0);
+        cudaEventDestroy(dep);
+    }
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_sync(b40c_enactor_t *e) {
+    clear_error();
+    if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
+    if (!e->h_ctr) return B40C_SUCCESS;
+    return finish_search(e);
+}
+
+extern "C" int b40c_enactor_get_statistics(b40c_enactor_t *e, long long *total_queued, int *search_depth,
+                                           double *avg_duty) {
+    clear_error();
+    if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
+    if (!e->have_stats && e->h_ctr) {
+        int rc = finish_search(e);
+        if (rc) return rc;
+    }
+    // GetStatistics: search_depth = iteration - 1 (enactor_contract_expand.cuh:245).
+    if (total_queued) *total_queued = e->instrument ? e->last_total_queued : 0;
+    if (search_depth) *search_depth = e->last_iteration - 1;
+    if (avg_duty) *avg_duty = 0.0;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_last_elapsed_ms(b40c_enactor_t *e, float *ms) {
+    clear_error();
+    if (!e || !ms) return set_error(B40C_ERR_INVALID_VALUE, "NULL argument");
+    *ms = e->last_ms;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_set_stream(b40c_enactor_t *e, void *stream) {
+    clear_error();
+    if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
+    e->stream = (cudaStream_t)stream;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_set_policy(b40c_enactor_t *e, int cta_threads, int warp_th, int cta_th, int big_th,
+                                       int cull_flags) {
+    clear_error();
+    if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
+    if (cta_threads && cta_threads != 128 && cta_threads != 256 && cta_threads != 512)
+        return set_error(B40C_ERR_INVALID_VALUE, "cta_threads must be 128, 256 or 512");
+    if (warp_th < 0 || cta_th < 0 || big_th < 0 || cull_flags < 0 || cull_flags > 3)
+        return set_error(B40C_ERR_INVALID_VALUE, "invalid policy field");
+    if (cta_threads) e->threads = cta_threads;
+    if (warp_th) e->warp_th = warp_th;
+    if (cta_th) e->cta_th = cta_th;
+    if (big_th) e->big_th = big_th;
+    e->cull_flags = unsigned(cull_flags);
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_set_wait_limit_us(b40c_enactor_t *e, long long us) {
+    clear_error();
+    if (!e || us <= 0) return set_error(B40C_ERR_INVALID_VALUE, "invalid wait limit");
+    e->wait_ns = (unsigned long long)us * 1000ull;
+    return B40C_SUCCESS;
+}
+
+// ---- failure detection ------------------------------------------------------------------
+
+extern "C" int b40c_debug_barrier_timeout(int grid_size, long long wait_limit_us) {
+    clear_error();
+    if (grid_size < 1 || grid_size > 4096 || wait_limit_us <= 0 || wait_limit_us > 10000000)
+        return set_error(B40C_ERR_INVALID_VALUE, "invalid probe arguments");
+    unsigned err = 0;
+    cudaError_t e = run_barrier_timeout_probe(grid_size, (unsigned long long)wait_limit_us * 1000ull, &err);
+    if (e) return cuda_fail(e, "barrier timeout probe");
+    return translate_device_error(err);
+}

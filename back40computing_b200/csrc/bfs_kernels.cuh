@@ -1,0 +1,68 @@
+// Launch interface between the host orchestration (bfs_host.cu) and the
+// sm_100a BFS kernels (bfs_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bfs_device.cuh"
+
+namespace b40c_b200 {
+
+enum Strategy : int {
+    STRATEGY_EXPAND_CONTRACT = 0,
+    STRATEGY_CONTRACT_EXPAND = 1,
+    STRATEGY_TWO_PHASE = 2,
+};
+
+enum CullFlags : unsigned {
+    CULL_WARP = 1u,     // __match_any_sync duplicate cull inside a warp
+    CULL_HISTORY = 2u,  // per-CTA shared-memory history hash
+};
+
+// Everything a BFS kernel needs, passed by value.
+struct BfsParams {
+    const int *row_offsets;  // nodes + 1
+    const int *col;          // edges (+4 padding entries for 16-byte tail loads)
+    int *labels;             // nodes: depth, or predecessor when mark_pred
+    unsigned *mask;          // visited bitmask, bit (v & 31) of word v >> 5
+    int *queue[2];           // frontier ping-pong
+    int *pred_queue[2];      // predecessor ping-pong (edge frontiers, mark_pred)
+    int4 *big_items;         // lists gathered grid-wide: {start, len, pred, out}
+    Counters *ctr;
+    unsigned long long wait_ns;      // grid-barrier spin limit
+    unsigned long long cond_handle;  // cudaGraphConditionalHandle (per-level graphs)
+    long long qcap;                  // elements per frontier queue
+    int big_cap;                     // entries of big_items
+    int vec_end;                     // 16-byte loads of col are safe below this index
+    int nodes;
+    int src;
+    int warp_th;  // lists >= warp_th are gathered by a warp
+    int cta_th;   // lists >= cta_th are gathered by the whole CTA
+    int big_th;   // lists >= big_th are gathered by every CTA of the grid
+    unsigned cull_flags;
+};
+
+struct KernelConfig {
+    int strategy;
+    int threads;  // 128, 256 or 512
+    bool mark_pred;
+};
+
+// Enqueues the per-search initialisation (counters, source) on stream.
+cudaError_t launch_search_init(const BfsParams &p, const KernelConfig &kc, cudaStream_t stream);
+// Largest co-resident grid of the fused kernel (SMs x occupancy).
+cudaError_t fused_grid_limit(const KernelConfig &kc, int *grid);
+// Grid of the per-level kernels (SMs x occupancy).
+cudaError_t level_grid_limit(const KernelConfig &kc, int *grid);
+// Cooperative launch of the persistent kernel that runs every BFS level.
+cudaError_t launch_fused(const BfsParams &p, const KernelConfig &kc, int grid, cudaStream_t stream);
+// Builds a graph whose conditional-while node runs one BFS level per pass:
+// level kernel(s), then a control kernel that advances the iteration and
+// sets the loop condition on the device.  p.cond_handle is filled in.
+cudaError_t build_level_graph(BfsParams &p, const KernelConfig &kc, int grid,
+                              cudaGraphExec_t *exec, cudaGraph_t *graph);
+// Debug/failure-detection probe: a cooperative grid whose barrier expects one
+// more arrival than there are CTAs.  Returns the device error word.
+cudaError_t run_barrier_timeout_probe(int grid, unsigned long long wait_ns, unsigned *error_out);
+
+}  // namespace b40c_b200

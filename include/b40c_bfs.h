@@ -1,0 +1,169 @@
+/*
+ * b40c_bfs.h -- C ABI of libb40c_bfs.so, a B200 (sm_100a) breadth-first search
+ * that stands in for b40c::graph::bfs of back40computing (b40c v1.0.1042).
+ *
+ * Every entry point returns an int whose value is a cudaError_t code
+ * (0 = success), the way every reference method returns cudaError_t.  The
+ * message of the last failure on the calling thread is available from
+ * b40c_last_error_string().  Signatures use plain pointers and sizes only.
+ *
+ * Reference interfaces are cited as file:line inside the back40computing tree.
+ */
+#ifndef B40C_BFS_H
+#define B40C_BFS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes (numeric values of cudaError_t) ----------------------- */
+#define B40C_SUCCESS                      0
+#define B40C_ERR_INVALID_VALUE            1    /* cudaErrorInvalidValue */
+#define B40C_ERR_MEMORY_ALLOCATION        2    /* cudaErrorMemoryAllocation */
+#define B40C_ERR_INVALID_CONFIGURATION    9    /* cudaErrorInvalidConfiguration: frontier queue overflow
+                                                  (enactor_contract_expand.cuh:318-324) */
+#define B40C_ERR_INVALID_DEVICE_FUNCTION  98   /* cudaErrorInvalidDeviceFunction */
+#define B40C_ERR_ILLEGAL_STATE            401  /* cudaErrorIllegalState: call out of order */
+#define B40C_ERR_LAUNCH_TIMEOUT           702  /* cudaErrorLaunchTimeout: a bounded device wait gave up */
+#define B40C_ERR_NOT_SUPPORTED            801  /* cudaErrorNotSupported */
+
+/* ---- enumerations -------------------------------------------------------- */
+/* FrontierType, b40c/graph/bfs/csr_problem.cuh:54-61 */
+#define B40C_VERTEX_FRONTIERS     0
+#define B40C_EDGE_FRONTIERS       1
+#define B40C_MIXED_FRONTIERS      2
+#define B40C_MULTI_GPU_FRONTIERS  3
+
+/* Strategy, test/bfs/test_bfs.cu:71-78 (MULTI_GPU is not provided) */
+#define B40C_EXPAND_CONTRACT  0
+#define B40C_CONTRACT_EXPAND  1
+#define B40C_TWO_PHASE        2
+#define B40C_HYBRID           3
+
+/* Which enact method: EnactSearch / EnactFusedSearch / EnactIterativeSearch */
+#define B40C_VARIANT_DEFAULT    0
+#define B40C_VARIANT_FUSED      1
+#define B40C_VARIANT_ITERATIVE  2
+
+typedef struct b40c_problem b40c_problem_t;   /* bfs::CsrProblem<int,int,MARK_PREDECESSORS> */
+typedef struct b40c_enactor b40c_enactor_t;   /* bfs::Enactor{ContractExpand,ExpandContract,TwoPhase,Hybrid} */
+
+/* ---- library ------------------------------------------------------------- */
+/* Message of the last failure on this thread ("" if none). */
+const char *b40c_last_error_string(void);
+/* Library version string. */
+const char *b40c_version(void);
+
+/* ---- CsrProblem (b40c/graph/bfs/csr_problem.cuh:68-751) ------------------ */
+/* CsrProblem() ctor (:229-233), on the current CUDA device.  mark_predecessors
+ * selects the MARK_PREDECESSORS template flag (:66). */
+int b40c_problem_create(int mark_predecessors, b40c_problem_t **out);
+/* ~CsrProblem (:240-249) and GraphSlice::~GraphSlice (:152-172). */
+int b40c_problem_destroy(b40c_problem_t *problem);
+/* FromHostProblem(stream_from_host, nodes, edges, h_column_indices,
+ * h_row_offsets, num_gpus) (:328-403).  The host CSR stays caller-owned; it is
+ * validated (monotone offsets, ids in range) and copied to the device.
+ * stream_from_host maps the host arrays instead (they must be pinned and
+ * mapped, or are registered here).  num_gpus must be <= 1. */
+int b40c_problem_from_host(b40c_problem_t *problem, int stream_from_host,
+                           int nodes, int edges,
+                           const int *h_column_indices, const int *h_row_offsets,
+                           int num_gpus);
+/* Reset(frontier_type, queue_sizing) (:547-750): lazily (re)allocates the
+ * frontier queues, sets labels := -1 and the visited mask := 0; synchronous. */
+int b40c_problem_reset(b40c_problem_t *problem, int frontier_type, double queue_sizing);
+/* Same, but only enqueues the label/mask initialisation on the problem's
+ * stream (allocation, when needed, is still done before returning). */
+int b40c_problem_reset_async(b40c_problem_t *problem, int frontier_type, double queue_sizing);
+/* ExtractResults(h_label) (:255-273): copies nodes labels to the host. */
+int b40c_problem_extract_results(b40c_problem_t *problem, int *h_labels);
+/* Enqueues the label copy on the problem's stream without waiting. */
+int b40c_problem_extract_results_async(b40c_problem_t *problem, int *h_labels);
+/* nodes, edges and the GraphSlice device pointers (:99-173). Any out pointer may be NULL. */
+int b40c_problem_info(b40c_problem_t *problem, int64_t *nodes, int64_t *edges,
+                      void **d_row_offsets, void **d_column_indices,
+                      void **d_labels, void **d_visited_mask);
+/* Stream (a cudaStream_t) for every later operation on this problem; NULL = the
+ * library's own stream for this problem. */
+int b40c_problem_set_stream(b40c_problem_t *problem, void *stream);
+
+/* ---- Enactors (b40c/graph/bfs/enactor_*.cuh) ----------------------------- */
+/* Enactor{ExpandContract,ContractExpand,TwoPhase,Hybrid}<INSTRUMENT>(DEBUG)
+ * ctor (enactor_expand_contract.cuh:~200, enactor_contract_expand.cuh:206-214,
+ * enactor_two_phase.cuh:221-229, enactor_hybrid.cuh:64). */
+int b40c_enactor_create(int strategy, int instrument, int debug, b40c_enactor_t **out);
+int b40c_enactor_destroy(b40c_enactor_t *enactor);
+/* GetFrontierType() (enactor_base.cuh:72). */
+int b40c_enactor_frontier_type(b40c_enactor_t *enactor, int *frontier_type);
+/* EnactSearch / EnactFusedSearch / EnactIterativeSearch(problem, src,
+ * max_grid_size) (enactor_contract_expand.cuh:259-407, :416-596;
+ * enactor_expand_contract.cuh:258-373; enactor_two_phase.cuh:416-765;
+ * enactor_hybrid.cuh:279-560).  Synchronous: returns after the search, with
+ * cudaErrorInvalidConfiguration on frontier overflow. */
+int b40c_enact_search(b40c_enactor_t *enactor, b40c_problem_t *problem,
+                      int src, int max_grid_size, int variant);
+/* Enqueues the search on the enactor's stream and returns; overflow and
+ * barrier-timeout flags are checked by the next b40c_enactor_sync. */
+int b40c_enact_search_async(b40c_enactor_t *enactor, b40c_problem_t *problem,
+                            int src, int max_grid_size, int variant);
+/* Waits for the enactor's stream and reports flags raised by async searches. */
+int b40c_enactor_sync(b40c_enactor_t *enactor);
+/* GetStatistics(total_queued, search_depth, avg_duty)
+ * (enactor_contract_expand.cuh:237-250).  search_depth = iteration - 1. */
+int b40c_enactor_get_statistics(b40c_enactor_t *enactor, long long *total_queued,
+                                int *search_depth, double *avg_duty);
+/* Device time of the last synchronous search (CUDA events around its kernels). */
+int b40c_enactor_last_elapsed_ms(b40c_enactor_t *enactor, float *ms);
+/* Stream (a cudaStream_t) for later searches; NULL = the enactor's own stream. */
+int b40c_enactor_set_stream(b40c_enactor_t *enactor, void *stream);
+/* Tuning policy (the reference's compile-time KernelPolicy, kernel_policy.cuh:61-87):
+ * cta_threads in {128,256,512}; warp/cta/grid gather thresholds in edges;
+ * flags: bit0 warp-level cull, bit1 history-hash cull.  0 keeps a field. */
+int b40c_enactor_set_policy(b40c_enactor_t *enactor, int cta_threads,
+                            int warp_gather_threshold, int cta_gather_threshold,
+                            int grid_gather_threshold, int cull_flags);
+/* Spin limit of every device-side wait (grid barrier), in microseconds. */
+int b40c_enactor_set_wait_limit_us(b40c_enactor_t *enactor, long long us);
+
+/* ---- host CSR graph builders (b40c/graph/builder/*.cuh, csr_graph.cuh) ---- */
+typedef struct b40c_csr {
+    int64_t nodes;
+    int64_t edges;
+    int *row_offsets;     /* nodes + 1 */
+    int *column_indices;  /* edges */
+} b40c_csr_t;
+/* BuildGrid2dGraph (builder/grid2d.cuh:53-114): 4-neighbour lattice; the
+ * reference appends one self-loop per vertex, kept here only if self_loops. */
+int b40c_graph_grid2d(int width, int self_loops, b40c_csr_t *out);
+/* BuildGrid3dGraph (builder/grid3d.cuh:53-129): 6-neighbour lattice. */
+int b40c_graph_grid3d(int width, int self_loops, b40c_csr_t *out);
+/* Graph500-style R-MAT (cf. BuildRmatGraph, builder/rmat.cuh:127-206):
+ * 2^scale vertices, edge_factor * 2^scale generated edges with quadrant
+ * probabilities a, b, c (d = 1-a-b-c), counter-based RNG from seed; self-loops
+ * dropped; undirected adds the reverse of every edge; duplicates kept; rows
+ * keep generation order. */
+int b40c_graph_rmat(int scale, int edge_factor, double a, double b, double c,
+                    uint64_t seed, int undirected, b40c_csr_t *out);
+/* Erdos-Renyi G(n, p), undirected, no self-loops or duplicate edges. */
+int b40c_graph_erdos_renyi(int nodes, double p, uint64_t seed, b40c_csr_t *out);
+/* CsrGraph::FromCoo (csr_graph.cuh:108-152): stable sort by row. */
+int b40c_graph_from_coo(int nodes, int64_t num_edges, const int *rows,
+                        const int *cols, b40c_csr_t *out);
+/* Frees the arrays of a b40c_csr_t filled by this library. */
+int b40c_csr_free(b40c_csr_t *csr);
+/* num_sources vertex ids drawn uniformly (with a seeded RNG) among vertices of degree > 0. */
+int b40c_graph_sample_sources(const b40c_csr_t *csr, int num_sources, uint64_t seed, int *sources);
+
+/* ---- failure detection -------------------------------------------------- */
+/* Runs the bounded grid barrier on a cooperative grid with one arrival that
+ * never comes: every block gives up after wait_limit_us and the call returns
+ * B40C_ERR_LAUNCH_TIMEOUT with the context still usable. */
+int b40c_debug_barrier_timeout(int grid_size, long long wait_limit_us);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B40C_BFS_H */

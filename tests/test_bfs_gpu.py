@@ -1,0 +1,256 @@
+"""GPU parity of the sm_100a BFS against the oracle and the reference's golden labels.
+
+Depth labels must be bit-exact (test/bfs/test_bfs.cu:385, CompareResults);
+predecessor labels must pass the reference's validity check (:389-438).
+Everything goes through the C ABI of libb40c_bfs.so via the Python mirror of
+b40c::graph::bfs.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_paths, load_golden
+
+pytestmark = pytest.mark.gpu
+
+STRATEGIES = [0, 1, 2]  # expand-contract, contract-expand, two-phase
+VARIANTS = [1, 2]       # fused (persistent kernel), iterative (graph-driven per-level)
+
+
+def bfs_mod():
+    import back40computing_b200 as b
+    return b
+
+
+def expected_search_depth(strategy, g, labels):
+    """GetStatistics search_depth (= iteration - 1) by strategy, derived from the
+    reference's level loops: expand-contract and two-phase stop after the level
+    that discovers nothing (depth d); contract-expand runs one more sweep over
+    the edges of the deepest level when it has any (d + 1)."""
+    d = int(labels.max())
+    if strategy == 1:
+        deg = np.diff(g.row_offsets)
+        return d + 1 if (deg[labels == d] > 0).any() else d
+    return d
+
+
+def run_search(g, strategy, variant, src, mark_pred=False, sizing=1.3, policy=None, problem=None,
+               max_grid=0):
+    b = bfs_mod()
+    prob = problem or b.CsrProblem(mark_pred).from_graph(g)
+    en = b.make_enactor(strategy)
+    if policy:
+        en.set_policy(**policy)
+    b.check(prob.Reset(en.GetFrontierType(), sizing))
+    rc = en.EnactSearch(prob, int(src), max_grid) if variant == 0 else (
+        en.EnactFusedSearch(prob, int(src), max_grid) if variant == 1 else
+        en.EnactIterativeSearch(prob, int(src), max_grid))
+    b.check(rc)
+    labels = prob.labels()
+    stats = en.GetStatistics()
+    return labels, stats
+
+
+@pytest.mark.parametrize("path", golden_paths(), ids=lambda p: p.stem)
+@pytest.mark.parametrize("strategy", STRATEGIES)
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_golden_labels_bit_exact(cuda_device, path, strategy, variant):
+    g, sources, golden, depths = load_golden(path)
+    b = bfs_mod()
+    prob = b.CsrProblem(False).from_graph(g)
+    for i, s in enumerate(sources):
+        labels, (_, search_depth, _) = run_search(g, strategy, variant, s, problem=prob)
+        assert np.array_equal(labels, golden[i]), f"{path.stem} src {s}: first mismatch at " \
+            f"{int(np.nonzero(labels != golden[i])[0][0])}"
+        assert search_depth == expected_search_depth(strategy, g, golden[i])
+        assert depths[i] == golden[i].max() + 1  # SimpleReferenceBfs search_depth
+
+
+@pytest.mark.parametrize("path", golden_paths()[:6], ids=lambda p: p.stem)
+@pytest.mark.parametrize("strategy", STRATEGIES)
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_golden_predecessors_valid(cuda_device, oracle, path, strategy, variant):
+    g, sources, golden, _ = load_golden(path)
+    for i, s in enumerate(sources):
+        preds, _ = run_search(g, strategy, variant, s, mark_pred=True)
+        assert preds[s] == -2  # source convention (contract_expand_atomic/kernel.cuh:321-325)
+        bad, reason = oracle.check_predecessors(g, preds, golden[i])
+        assert bad == -1, f"{path.stem} src {s}: node {bad} fails check {reason}"
+        assert np.array_equal(preds >= 0, golden[i] > 0)
+
+
+@pytest.fixture(scope="module")
+def rmat16():
+    return bfs_mod().rmat(16, 16, seed=1)
+
+
+@pytest.mark.parametrize("strategy", STRATEGIES)
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_rmat16_vs_oracle(cuda_device, oracle, rmat16, strategy, variant):
+    g = rmat16
+    for s in g.sample_sources(3, 2):
+        ref, _ = oracle.bfs(g, int(s))
+        labels, _ = run_search(g, strategy, variant, s)
+        assert oracle.first_mismatch(labels, ref) == -1
+
+
+# Policies that route lists through every gather path: tiny thresholds push
+# most lists to the CTA and grid-wide (big-list) phases; culls on and off.
+POLICIES = [
+    dict(cta_threads=128),
+    dict(cta_threads=512),
+    dict(warp_gather_threshold=4, cta_gather_threshold=16, grid_gather_threshold=64),
+    dict(warp_gather_threshold=1, cta_gather_threshold=1, grid_gather_threshold=1),
+    dict(cta_threads=512, warp_gather_threshold=8, cta_gather_threshold=512, grid_gather_threshold=600),
+    dict(cull_flags=1),
+    dict(cull_flags=2),
+    dict(cull_flags=3, cta_threads=128, grid_gather_threshold=100),
+]
+
+
+@pytest.mark.parametrize("policy", POLICIES, ids=lambda p: ",".join(f"{k}={v}" for k, v in p.items()))
+@pytest.mark.parametrize("strategy", STRATEGIES)
+def test_policies_rmat(cuda_device, oracle, rmat16, policy, strategy):
+    g = rmat16
+    s = int(g.sample_sources(1, 9)[0])
+    ref, _ = oracle.bfs(g, s)
+    for variant in VARIANTS:
+        labels, _ = run_search(g, strategy, variant, s, policy=policy)
+        assert oracle.first_mismatch(labels, ref) == -1
+        preds, _ = run_search(g, strategy, variant, s, policy=policy, mark_pred=True)
+        assert oracle.check_predecessors(g, preds, ref)[0] == -1
+
+
+def _graph(rows, cols, n):
+    return bfs_mod().from_coo(n, np.asarray(rows, np.int32), np.asarray(cols, np.int32))
+
+
+EDGE_CASES = {
+    "single_vertex": lambda: _graph([], [], 1),
+    "isolated_source": lambda: _graph([1, 2], [2, 1], 4),
+    "no_edges": lambda: _graph([], [], 50),
+    "self_loops_dups": lambda: _graph([0, 0, 0, 1, 1, 2, 2, 2], [0, 1, 1, 0, 2, 2, 1, 0], 3),
+    "directed_chain": lambda: _graph(list(range(999)), list(range(1, 1000)), 1000),
+    "path_5000": lambda: _graph(list(range(4999)) + list(range(1, 5000)),
+                                list(range(1, 5000)) + list(range(4999)), 5000),
+    "star_200k": lambda: _graph([0] * 200000 + list(range(1, 200001)),
+                                list(range(1, 200001)) + [0] * 200000, 200001),
+}
+
+
+@pytest.mark.parametrize("case", sorted(EDGE_CASES))
+@pytest.mark.parametrize("strategy", STRATEGIES)
+def test_edge_cases(cuda_device, oracle, case, strategy):
+    g = EDGE_CASES[case]()
+    for s in sorted({0, g.nodes - 1, g.nodes // 2}):
+        ref, _ = oracle.bfs(g, s)
+        for variant in VARIANTS:
+            labels, (_, depth, _) = run_search(g, strategy, variant, s)
+            assert oracle.first_mismatch(labels, ref) == -1, (case, s, variant)
+            assert depth == expected_search_depth(strategy, g, ref)
+            preds, _ = run_search(g, strategy, variant, s, mark_pred=True)
+            assert oracle.check_predecessors(g, preds, ref)[0] == -1
+
+
+@pytest.mark.parametrize("strategy", STRATEGIES)
+def test_small_grids(cuda_device, oracle, strategy):
+    """A grid of 1 and 2 CTAs must give the same labels (barrier with few arrivals)."""
+    g = bfs_mod().grid2d(64)
+    ref, _ = oracle.bfs(g, 32 * 64 + 32)
+    for grid in (1, 2, 7):
+        for variant in VARIANTS:
+            labels, _ = run_search(g, strategy, variant, 32 * 64 + 32, max_grid=grid)
+            assert oracle.first_mismatch(labels, ref) == -1
+
+
+def test_grid2d_1024_contract_expand(cuda_device, oracle):
+    """The 1024x1024 lattice, source (512, 512), contract-expand (plain EnactSearch)."""
+    g = bfs_mod().grid2d(1024)
+    src = 512 * 1024 + 512
+    ref, _ = oracle.bfs(g, src)
+    for strategy in STRATEGIES:
+        labels, (_, depth, _) = run_search(g, strategy, 0, src)
+        assert oracle.first_mismatch(labels, ref) == -1
+        assert depth == expected_search_depth(strategy, g, ref)
+
+
+def test_overflow_reports_invalid_configuration(cuda_device, rmat16):
+    b = bfs_mod()
+    prob = b.CsrProblem(False).from_graph(rmat16)
+    en = b.EnactorContractExpand()
+    b.check(prob.Reset(en.GetFrontierType(), 0.001))
+    rc = en.EnactSearch(prob, int(rmat16.sample_sources(1, 2)[0]))
+    assert rc == b.bfs.cudaErrorInvalidConfiguration
+    # Recovers after a proper reset.
+    b.check(prob.Reset(en.GetFrontierType(), 1.0))
+    b.check(en.EnactSearch(prob, int(rmat16.sample_sources(1, 2)[0])))
+
+
+def test_barrier_timeout_is_reported_and_context_survives(cuda_device, oracle):
+    b = bfs_mod()
+    assert b.bfs.debug_barrier_timeout(8, 20000) == b.bfs.cudaErrorLaunchTimeout
+    g = b.grid2d(32)
+    ref, _ = oracle.bfs(g, 5)
+    labels, _ = run_search(g, 0, 1, 5)
+    assert oracle.first_mismatch(labels, ref) == -1
+
+
+def test_bad_csr_rejected_on_host(cuda_device):
+    b = bfs_mod()
+    prob = b.CsrProblem(False)
+    row = np.array([0, 1, 2], np.int32)
+    assert prob.FromHostProblem(False, 2, 2, np.array([1, 5], np.int32), row, 1) == 1
+    assert prob.FromHostProblem(False, 2, 2, np.array([1, 0], np.int32), np.array([0, 2, 1], np.int32), 1) == 1
+    assert prob.FromHostProblem(False, 2, 2, np.array([1, 0], np.int32), row, 1) == 0
+
+
+def test_source_out_of_range(cuda_device):
+    b = bfs_mod()
+    g = b.grid2d(8)
+    prob = b.CsrProblem(False).from_graph(g)
+    en = b.EnactorExpandContract()
+    b.check(prob.Reset(en.GetFrontierType(), 1.3))
+    assert en.EnactSearch(prob, g.nodes) == 1
+    assert en.EnactSearch(prob, -1) == 1
+
+
+def test_async_back_to_back(cuda_device, oracle, rmat16):
+    """Searches enqueued without host syncs, each followed by its label copy."""
+    b = bfs_mod()
+    g = rmat16
+    sources = g.sample_sources(6, 4)
+    for strategy in STRATEGIES:
+        prob = b.CsrProblem(False).from_graph(g)
+        en = b.make_enactor(strategy)
+        outs = [np.empty(g.nodes, np.int32) for _ in sources]
+        for s, out in zip(sources, outs):
+            b.check(prob.ResetAsync(en.GetFrontierType(), 1.3))
+            b.check(en.EnactSearchAsync(prob, int(s)))
+            b.check(prob.ExtractResultsAsync(out))
+        b.check(en.Sync())
+        for s, out in zip(sources, outs):
+            ref, _ = oracle.bfs(g, int(s))
+            assert oracle.first_mismatch(out, ref) == -1
+
+
+def test_stream_from_host(cuda_device, oracle):
+    b = bfs_mod()
+    g = b.rmat(12, 8, seed=3)
+    s = int(g.sample_sources(1, 1)[0])
+    ref, _ = oracle.bfs(g, s)
+    for strategy in STRATEGIES:
+        prob = b.CsrProblem(False).from_graph(g, stream_from_host=True)
+        labels, _ = run_search(g, strategy, 1, s, problem=prob)
+        assert oracle.first_mismatch(labels, ref) == -1
+
+
+def test_problem_reused_across_strategies(cuda_device, oracle, rmat16):
+    b = bfs_mod()
+    g = rmat16
+    prob = b.CsrProblem(False).from_graph(g)
+    for s in g.sample_sources(2, 8):
+        ref, _ = oracle.bfs(g, int(s))
+        for strategy in [0, 1, 2, 0]:
+            labels, _ = run_search(g, strategy, 1, s, problem=prob)
+            assert oracle.first_mismatch(labels, ref) == -1
