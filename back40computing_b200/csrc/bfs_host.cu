@@ -16,6 +16,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -135,13 +137,14 @@ int check_csr(int64_t nodes, int64_t edges, const int *row, const int *col) {
     return B40C_SUCCESS;
 }
 
+void unmap_host(b40c_problem *p);
+
 void free_problem_device(b40c_problem *p) {
     if (!p->mapped) {
         cudaFree(p->d_row_offsets);
         cudaFree(p->d_col);
     }
-    for (void *h : p->registered) cudaHostUnregister(h);
-    p->registered.clear();
+    unmap_host(p);
     p->d_row_offsets = nullptr;
     p->d_col = nullptr;
     cudaFree(p->d_labels);
@@ -156,17 +159,48 @@ void free_problem_device(b40c_problem *p) {
     }
 }
 
+// Host ranges this library registered for stream_from_host, with the number
+// of problems using each.  Several problems may map the same caller arrays;
+// the range is unregistered when the last of them lets go.  Memory the
+// caller pinned itself (cudaHostAlloc, or registered outside the library) is
+// never registered or unregistered here.
+std::mutex g_reg_mutex;
+std::map<void *, int> g_registrations;
+
 int map_host(b40c_problem *p, const void *h, size_t bytes, void **d) {
-    cudaPointerAttributes attr{};
-    cudaError_t e = cudaPointerGetAttributes(&attr, h);
-    if (e != cudaSuccess) cudaGetLastError();
-    if (e != cudaSuccess || attr.type != cudaMemoryTypeHost) {
-        e = cudaHostRegister(const_cast<void *>(h), bytes, cudaHostRegisterMapped | cudaHostRegisterReadOnly);
-        if (e != cudaSuccess) return cuda_fail(e, "CsrProblem cudaHostRegister (stream_from_host)");
-        p->registered.push_back(const_cast<void *>(h));
+    void *ptr = const_cast<void *>(h);
+    {
+        std::lock_guard<std::mutex> lock(g_reg_mutex);
+        auto it = g_registrations.find(ptr);
+        if (it != g_registrations.end()) {
+            it->second++;
+            p->registered.push_back(ptr);
+        } else {
+            cudaPointerAttributes attr{};
+            cudaError_t e = cudaPointerGetAttributes(&attr, h);
+            if (e != cudaSuccess) cudaGetLastError();
+            if (e != cudaSuccess || attr.type != cudaMemoryTypeHost) {
+                e = cudaHostRegister(ptr, bytes, cudaHostRegisterMapped | cudaHostRegisterReadOnly);
+                if (e != cudaSuccess) return cuda_fail(e, "CsrProblem cudaHostRegister (stream_from_host)");
+                g_registrations[ptr] = 1;
+                p->registered.push_back(ptr);
+            }
+        }
     }
-    CUDA_TRY(cudaHostGetDevicePointer(d, const_cast<void *>(h), 0), "CsrProblem cudaHostGetDevicePointer");
+    CUDA_TRY(cudaHostGetDevicePointer(d, ptr, 0), "CsrProblem cudaHostGetDevicePointer");
     return B40C_SUCCESS;
+}
+
+void unmap_host(b40c_problem *p) {
+    std::lock_guard<std::mutex> lock(g_reg_mutex);
+    for (void *h : p->registered) {
+        auto it = g_registrations.find(h);
+        if (it != g_registrations.end() && --it->second == 0) {
+            cudaHostUnregister(h);
+            g_registrations.erase(it);
+        }
+    }
+    p->registered.clear();
 }
 
 int translate_device_error(unsigned err) {
