@@ -4,7 +4,7 @@
 // (b40c/graph/bfs/csr_problem.cuh:68-751) for one GPU: it owns the device CSR,
 // labels, visited mask and frontier queues.  b40c_enactor mirrors the
 // Enactor{ExpandContract,ContractExpand,TwoPhase} classes: it owns the search
-// counters, the big-list table, its stream, timing events and the cached
+// counters, the grid-wide chunk table, its stream, timing events, the cached
 // per-level CUDA graph.  Each entry point returns a cudaError_t value and
 // records a message in the thread's error slot (B40CPerror,
 // b40c/util/error_utils.cuh:44-103).
@@ -78,15 +78,17 @@ struct b40c_enactor {
     int strategy = B40C_EXPAND_CONTRACT;
     bool instrument = false, debug = false;
     int threads = 256;
-    int warp_th = 32, cta_th = 512, big_th = 8192;
+    int warp_th = 32, cta_th = 256, big_th = 1024;
     unsigned cull_flags = 0;
     unsigned long long wait_ns = 5000000000ull;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     Counters *d_ctr = nullptr;
     Counters *h_ctr = nullptr;  // pinned
-    int4 *d_big = nullptr;
-    int big_cap = 0;
+    int4 *d_chunks = nullptr;
+    int chunk_cap = 0;
+    LevelRecord *d_levels = nullptr;  // per-level log, when enabled
+    bool log_levels = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.f;
     int last_iteration = 0;
@@ -102,6 +104,8 @@ struct b40c_enactor {
 };
 
 namespace {
+
+constexpr int LEVEL_LOG_CAP = 4096;
 
 cudaStream_t problem_stream(b40c_problem *p) { return p->stream ? p->stream : p->own_stream; }
 cudaStream_t enactor_stream(b40c_enactor *e) { return e->stream ? e->stream : e->own_stream; }
@@ -224,16 +228,20 @@ int ensure_enactor_buffers(b40c_enactor *e, b40c_problem *p) {
         CUDA_TRY(cudaHostAlloc(&e->h_ctr, sizeof(Counters), cudaHostAllocDefault), "Enactor cudaHostAlloc");
         std::memset(e->h_ctr, 0, sizeof(Counters));
     }
-    // Big lists per level are at most edges / big_th (each vertex expands once).
-    long long need = p->edges / std::max(1, e->big_th) + 64;
+    // Chunks per level: each vertex expands once per search, and a list of
+    // len >= big_th edges takes at most len / CH + 2 chunks (CH >= 512 edges).
+    const long long bt = std::max(1, std::max(e->big_th, std::max(e->cta_th, e->warp_th)));
+    long long need = p->edges / chunk_edges<128>() + 2 * (p->edges / bt) + 64;
     if (need > (1ll << 30)) need = 1ll << 30;
-    if (e->big_cap < need) {
-        cudaFree(e->d_big);
-        e->d_big = nullptr;
-        e->big_cap = 0;
-        CUDA_TRY(cudaMalloc(&e->d_big, sizeof(int4) * size_t(need)), "Enactor cudaMalloc big-list table");
-        e->big_cap = int(need);
+    if (e->chunk_cap < need) {
+        cudaFree(e->d_chunks);
+        e->d_chunks = nullptr;
+        e->chunk_cap = 0;
+        CUDA_TRY(cudaMalloc(&e->d_chunks, sizeof(int4) * size_t(need)), "Enactor cudaMalloc chunk table");
+        e->chunk_cap = int(need);
     }
+    if (e->log_levels && !e->d_levels)
+        CUDA_TRY(cudaMalloc(&e->d_levels, sizeof(LevelRecord) * LEVEL_LOG_CAP), "Enactor cudaMalloc level log");
     return B40C_SUCCESS;
 }
 
@@ -247,7 +255,9 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
         bp.queue[i] = p->d_queue[i];
         bp.pred_queue[i] = p->d_pred[i];
     }
-    bp.big_items = e->d_big;
+    bp.chunks = e->d_chunks;
+    bp.levels = e->log_levels ? e->d_levels : nullptr;
+    bp.level_cap = LEVEL_LOG_CAP;
     bp.ctr = e->d_ctr;
     bp.wait_ns = e->wait_ns;
     long long qcap = std::min(p->queue_elems[0], p->queue_elems[1]);
@@ -255,7 +265,7 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
         qcap = std::min(qcap, std::min(p->pred_elems[0], p->pred_elems[1]));
     if (qcap > 0xffffffffll) qcap = 0xffffffffll;
     bp.qcap = qcap;
-    bp.big_cap = e->big_cap;
+    bp.chunk_cap = e->chunk_cap;
     bp.vec_end = p->mapped ? int(p->edges & ~int64_t(3)) : int(p->edges + 4);
     bp.nodes = int(p->nodes);
     bp.src = src;
@@ -294,6 +304,8 @@ int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size,
         cudaEventDestroy(dep);
     }
     if (variant == B40C_VARIANT_DEFAULT) variant = B40C_VARIANT_FUSED;
+    if (bp.levels)
+        CUDA_TRY(cudaMemsetAsync(bp.levels, 0, sizeof(LevelRecord) * LEVEL_LOG_CAP, s), "level log clear");
     CUDA_TRY(cudaEventRecord(e->ev0, s), "cudaEventRecord");
     CUDA_TRY(launch_search_init(bp, kc, s), "search init kernel launch");
     if (variant == B40C_VARIANT_FUSED) {
@@ -583,7 +595,8 @@ extern "C" int b40c_enactor_destroy(b40c_enactor_t *e) {
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     if (e->graph) cudaGraphDestroy(e->graph);
     cudaFree(e->d_ctr);
-    cudaFree(e->d_big);
+    cudaFree(e->d_chunks);
+    cudaFree(e->d_levels);
     if (e->h_ctr) cudaFreeHost(e->h_ctr);
     cudaEventDestroy(e->ev0);
     cudaEventDestroy(e->ev1);
@@ -684,6 +697,43 @@ extern "C" int b40c_enactor_set_policy(b40c_enactor_t *e, int cta_threads, int w
     if (cta_th) e->cta_th = cta_th;
     if (big_th) e->big_th = big_th;
     e->cull_flags = unsigned(cull_flags);
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_set_level_log(b40c_enactor_t *e, int enable) {
+    clear_error();
+    if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
+    e->log_levels = enable != 0;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_level_log(b40c_enactor_t *e, int max_records, int64_t *t_start_ns, int64_t *t_tiles_ns,
+                                      int *frontier, int *chunks, int *count) {
+    clear_error();
+    if (!e || !count || max_records < 0) return set_error(B40C_ERR_INVALID_VALUE, "invalid argument");
+    *count = 0;
+    if (!e->log_levels || !e->d_levels) return set_error(B40C_ERR_ILLEGAL_STATE, "level log not enabled");
+    if (e->h_ctr && !e->have_stats) {
+        int rc = finish_search(e);
+        if (rc) return rc;
+    }
+    std::vector<LevelRecord> h(LEVEL_LOG_CAP);
+    CUDA_TRY(cudaMemcpy(h.data(), e->d_levels, sizeof(LevelRecord) * LEVEL_LOG_CAP, cudaMemcpyDeviceToHost),
+             "level log copy");
+    // Records run up to the end-of-search marker (frontier 0).
+    int n = 0;
+    while (n < LEVEL_LOG_CAP && h[n].t_start != 0) {
+        n++;
+        if (h[n - 1].frontier == 0u) break;
+    }
+    n = std::min(n, max_records);
+    for (int i = 0; i < n; i++) {
+        if (t_start_ns) t_start_ns[i] = (int64_t)h[i].t_start;
+        if (t_tiles_ns) t_tiles_ns[i] = (int64_t)h[i].t_tiles;
+        if (frontier) frontier[i] = (int)h[i].frontier;
+        if (chunks) chunks[i] = (int)h[i].chunks;
+    }
+    *count = n;
     return B40C_SUCCESS;
 }
 

@@ -9,19 +9,23 @@
 // 416-516, enactor_two_phase.cuh:465-598), which keeps the level loop on the
 // device instead of polling a host-mapped "done" word.
 //
-// Neighbour-list gather follows the reference's three-way split by list length
+// Neighbour-list gather follows the reference's split by list length
 // (two_phase/expand_atomic/cta.cuh:215-423): lists >= cta_th are streamed by the
 // whole CTA, lists >= warp_th by one warp, and shorter lists are packed into a
 // shared-memory gather-offset scratch by a block-wide prefix sum and read by the
-// CTA together.  Two additions: CTA and warp lists are read with 16-byte
-// vector loads that carry an L2 evict_first policy, and lists >= big_th are
-// deferred to a grid-wide phase in which every CTA takes chunks of them, so one
-// hub vertex cannot serialise a level behind a single CTA.
+// CTA together.  A fourth tier takes lists >= big_th: they are cut into
+// fixed-size chunks (one 16-byte load per thread of a CTA) that every CTA of
+// the grid takes in turn after the tile phase, so a hub vertex never
+// serialises a level behind one CTA.  Tiles shrink when the frontier is small
+// so that every CTA gets work.  CTA and warp lists are read with 16-byte loads
+// carrying an L2 evict_first policy, one pass ahead of use.
 //
 // Culling: the visited bitmask is the authority and is updated with atomicOr
-// (exact), so each vertex is labelled and expanded once; optional warp-level
-// (__match_any_sync) and per-CTA history-hash culls drop repeats before they
-// reach the mask (contract_atomic/cta.cuh:276-327).
+// (exact), so each vertex is labelled and expanded once.  Each thread tests 4
+// elements at a time: 4 mask loads in flight, then at most 4 atomicOr, then one
+// warp-aggregated queue reservation.  Optional warp-level (__match_any_sync)
+// and per-CTA history-hash culls drop repeats first (contract_atomic/cta.cuh:
+// 276-327).
 
 #include <cuda_runtime.h>
 
@@ -38,10 +42,12 @@ constexpr unsigned NO_SPACE = 0xffffffffu;
 template <int THREADS, bool MP>
 struct Smem {
     static constexpr int SCRATCH = THREADS * 4;  // gather-offset scratch entries
+    static constexpr int CTILE = THREADS * 4;    // edge-frontier elements per contract tile
     int2 warp_tot[THREADS / 32 + 1];
     int gofs[SCRATCH];
     int gpred[MP ? SCRATCH : 1];
     int hist[HIST_SIZE];
+    int surv[CTILE];
     int owner;
     int c_start, c_len, c_pred;
     unsigned c_out;
@@ -51,11 +57,10 @@ struct Smem {
 };
 
 // ---------------------------------------------------------------------------------------
-// Sinks: what happens to each gathered neighbour.  Called by every lane of a
-// warp together (valid marks the lanes that hold an element).
+// Culling and enqueueing, 4 elements per thread
 // ---------------------------------------------------------------------------------------
 
-// Optional culls shared by both kinds of sink.  Returns the surviving validity.
+// Optional culls.  Called by every lane of the warp (match_any needs them all).
 template <int THREADS, bool MP>
 __device__ __forceinline__ bool pre_cull(bool valid, int u, unsigned flags, Smem<THREADS, MP> &sm) {
     if (flags & CULL_WARP) {
@@ -72,39 +77,93 @@ __device__ __forceinline__ bool pre_cull(bool valid, int u, unsigned flags, Smem
     return valid;
 }
 
-// Expand-contract: mark and label each neighbour, then enqueue the ones this
-// thread discovered with one atomicAdd per warp.
+// Exact test-and-set of the visited bits of up to 4 vertices (bit j of valid
+// marks u[j]).  Returns the bits of the vertices this thread claimed first.
+template <int THREADS, bool MP>
+__device__ __forceinline__ unsigned cull4(const BfsParams &p, Smem<THREADS, MP> &sm, unsigned valid,
+                                          const int (&u)[4]) {
+    if (p.cull_flags) {
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (!pre_cull<THREADS, MP>((valid >> j) & 1u, u[j], p.cull_flags, sm)) valid &= ~(1u << j);
+    }
+    unsigned w[4], bit[4], m[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        bool ok = (valid >> j) & 1u;
+        if (ok && (unsigned)u[j] >= (unsigned)p.nodes) {
+            atomicOr(&p.ctr->error, ERR_BAD_VERTEX);
+            valid &= ~(1u << j);
+            ok = false;
+        }
+        w[j] = ok ? (unsigned)u[j] >> 5 : 0u;
+        bit[j] = 1u << ((unsigned)u[j] & 31u);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) m[j] = ld_cg(p.mask + w[j]);  // 4 probes in flight
+    unsigned need = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        if (((valid >> j) & 1u) && !(m[j] & bit[j])) need |= 1u << j;
+    unsigned old[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) old[j] = ((need >> j) & 1u) ? atomicOr(p.mask + w[j], bit[j]) : bit[j];
+    unsigned claimed = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        if (!(old[j] & bit[j])) claimed |= 1u << j;
+    return claimed;
+}
+
+// Appends the flagged elements of every lane to queue q with one atomicAdd
+// per warp.  Called by all lanes together.
+__device__ __forceinline__ void enqueue4(unsigned flags, const int (&u)[4], int *q, unsigned *qlen, long long qcap,
+                                         unsigned *err) {
+    const unsigned lt = lanemask_lt();
+    unsigned total = 0, pre[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        unsigned b = __ballot_sync(FULL, (flags >> j) & 1u);
+        pre[j] = total + __popc(b & lt);
+        total += __popc(b);
+    }
+    if (total == 0u) return;  // warp-uniform
+    unsigned base = 0;
+    if (lane_id() == 0) base = atomicAdd(qlen, total);
+    base = __shfl_sync(FULL, base, 0);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if ((flags >> j) & 1u) {
+            unsigned long long pos = (unsigned long long)base + pre[j];
+            if (pos < (unsigned long long)qcap) q[pos] = u[j];
+            else atomicOr(err, ERR_OVERFLOW);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Sinks: what happens to each gathered neighbour.  Called by every lane of a
+// warp together with up to 4 elements per lane; bit j of valid marks u[j];
+// output positions are out0 + j.
+// ---------------------------------------------------------------------------------------
+
+// Expand-contract: mark and label each neighbour at discovery (label it+1,
+// expand_contract_atomic/cta.cuh:181-218), enqueue the discovered ones.
 template <int THREADS, bool MP>
 struct DiscoverSink {
     const BfsParams &p;
     Smem<THREADS, MP> &sm;
     int *q_out;
     unsigned *qlen_out;
-    int label;  // iteration + 1
+    int label;
 
-    __device__ __forceinline__ void operator()(bool valid, int u, int pred, unsigned) const {
-        bool disc = false;
-        valid = pre_cull<THREADS, MP>(valid, u, p.cull_flags, sm);
-        if (valid) {
-            if ((unsigned)u >= (unsigned)p.nodes) {
-                atomicOr(&p.ctr->error, ERR_BAD_VERTEX);
-            } else if (mark_visited(p.mask, u)) {
-                disc = true;
-                p.labels[u] = MP ? pred : label;
-            }
-        }
-        unsigned b = __ballot_sync(FULL, disc);
-        if (b) {
-            int leader = __ffs(b) - 1;
-            unsigned base = 0;
-            if ((int)lane_id() == leader) base = atomicAdd(qlen_out, (unsigned)__popc(b));
-            base = __shfl_sync(FULL, base, leader);
-            if (disc) {
-                unsigned long long pos = (unsigned long long)base + __popc(b & lanemask_lt());
-                if (pos < (unsigned long long)p.qcap) q_out[pos] = u;
-                else atomicOr(&p.ctr->error, ERR_OVERFLOW);
-            }
-        }
+    __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
+                                               unsigned) const {
+        unsigned disc = cull4<THREADS, MP>(p, sm, valid, u);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if ((disc >> j) & 1u) p.labels[u[j]] = MP ? pred[j] : label;
+        enqueue4(disc, u, q_out, qlen_out, p.qcap, &p.ctr->error);
     }
 };
 
@@ -114,10 +173,14 @@ template <bool MP>
 struct PositionSink {
     int *q_out;
     int *pq_out;
-    __device__ __forceinline__ void operator()(bool valid, int u, int pred, unsigned pos) const {
-        if (valid) {
-            q_out[pos] = u;
-            if (MP) pq_out[pos] = pred;
+    __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
+                                               unsigned out0) const {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if ((valid >> j) & 1u) {
+                q_out[out0 + j] = u[j];
+                if (MP) pq_out[out0 + j] = pred[j];
+            }
         }
     }
 };
@@ -126,30 +189,43 @@ struct PositionSink {
 // Gather strategies
 // ---------------------------------------------------------------------------------------
 
-// The calling group (CTA of THREADS, or one warp with GROUP = 32) streams list
-// [s, s+l) with 16-byte loads from the aligned-down start; elements outside the
-// list are masked off.  col must have 3 readable entries past the last edge.
+__device__ __forceinline__ int4 load_col4(const int *col, int vec_end, int e, int end, uint64_t pol) {
+    int4 c = make_int4(-1, -1, -1, -1);
+    if (e < end) {
+        if (e + 4 <= vec_end) {
+            c = ldg_stream_v4(col + e, pol);
+        } else {  // unpadded (host-mapped) array tail: scalar loads inside the list
+            c.x = __ldg(col + e);
+            if (e + 1 < end) c.y = __ldg(col + e + 1);
+            if (e + 2 < end) c.z = __ldg(col + e + 2);
+            if (e + 3 < end) c.w = __ldg(col + e + 3);
+        }
+    }
+    return c;
+}
+
+// The calling group (CTA of THREADS, or one warp with GROUP = 32) streams the
+// list [s, s+l) with 16-byte loads starting from the 4-aligned index a0 <= s;
+// each pass covers GROUP*4 elements; the next pass's load is issued before the
+// current elements are processed.  Elements outside [s, s+l) are masked off.
 template <int GROUP, class Sink>
-__device__ __forceinline__ void gather_list(const int *col, int vec_end, int s, int l, int pred,
+__device__ __forceinline__ void gather_list(const int *col, int vec_end, int a0, int s, int l, int pred,
                                             unsigned out, int rank, const Sink &sink, uint64_t pol) {
     const int end = s + l;
-    for (int base = s & ~3; base < end; base += GROUP * 4) {
-        int e = base + rank * 4;
-        int4 c = make_int4(-1, -1, -1, -1);
-        if (e < end) {
-            if (e + 4 <= vec_end) {
-                c = ldg_stream_v4(col + e, pol);
-            } else {  // unpadded (host-mapped) array tail: scalar loads inside the list
-                c.x = __ldg(col + e);
-                if (e + 1 < end) c.y = __ldg(col + e + 1);
-                if (e + 2 < end) c.z = __ldg(col + e + 2);
-                if (e + 3 < end) c.w = __ldg(col + e + 3);
-            }
-        }
-        sink(e >= s && e < end, c.x, pred, out + unsigned(e - s));
-        sink(e + 1 >= s && e + 1 < end, c.y, pred, out + unsigned(e + 1 - s));
-        sink(e + 2 >= s && e + 2 < end, c.z, pred, out + unsigned(e + 2 - s));
-        sink(e + 3 >= s && e + 3 < end, c.w, pred, out + unsigned(e + 3 - s));
+    int e = a0 + rank * 4;
+    int4 cur = load_col4(col, vec_end, e, end, pol);
+    const int pv[4] = {pred, pred, pred, pred};
+    for (int base = a0; base < end; base += GROUP * 4) {
+        const int en = e + GROUP * 4;
+        int4 nxt = load_col4(col, vec_end, en, end, pol);
+        unsigned valid = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (e + j >= s && e + j < end) valid |= 1u << j;
+        const int u[4] = {cur.x, cur.y, cur.z, cur.w};
+        sink(valid, u, pv, out + unsigned(e - s));
+        cur = nxt;
+        e = en;
     }
 }
 
@@ -158,10 +234,9 @@ __device__ __forceinline__ void gather_list(const int *col, int vec_end, int s, 
 // small_off / small_total: block exclusive scan of the lengths of lists shorter
 // than warp_th, whose outputs are contiguous from small_base.
 template <int THREADS, bool MP, class Sink>
-__device__ __forceinline__ void expand_lists(const BfsParams &p, Smem<THREADS, MP> &sm,
-                                             const Sink &sink, uint64_t pol, int start, int len,
-                                             int pred, unsigned out, int small_off,
-                                             int small_total, unsigned small_base) {
+__device__ __forceinline__ void expand_lists(const BfsParams &p, Smem<THREADS, MP> &sm, const Sink &sink,
+                                             uint64_t pol, int start, int len, int pred, unsigned out,
+                                             int small_off, int small_total, unsigned small_base) {
     const bool small = len < p.warp_th;
     // (1) whole-CTA gather of lists >= cta_th, one list at a time
     for (;;) {
@@ -169,7 +244,7 @@ __device__ __forceinline__ void expand_lists(const BfsParams &p, Smem<THREADS, M
         __syncthreads();
         if (len >= p.cta_th) sm.owner = threadIdx.x;
         __syncthreads();
-        int owner = sm.owner;
+        const int owner = sm.owner;
         if (owner < 0) break;
         if (owner == (int)threadIdx.x) {
             sm.c_start = start;
@@ -179,69 +254,90 @@ __device__ __forceinline__ void expand_lists(const BfsParams &p, Smem<THREADS, M
             len = 0;
         }
         __syncthreads();
-        gather_list<THREADS>(p.col, p.vec_end, sm.c_start, sm.c_len, sm.c_pred, sm.c_out, threadIdx.x, sink, pol);
+        const int s = sm.c_start;
+        gather_list<THREADS>(p.col, p.vec_end, s & ~3, s, sm.c_len, sm.c_pred, sm.c_out, threadIdx.x, sink, pol);
     }
     // (2) warp gather of lists >= warp_th
     unsigned wm;
     while ((wm = __ballot_sync(FULL, len >= p.warp_th)) != 0u) {
-        int leader = __ffs(wm) - 1;
-        int s = __shfl_sync(FULL, start, leader);
-        int l = __shfl_sync(FULL, len, leader);
-        int pv = __shfl_sync(FULL, pred, leader);
-        unsigned o = __shfl_sync(FULL, out, leader);
+        const int leader = __ffs(wm) - 1;
+        const int s = __shfl_sync(FULL, start, leader);
+        const int l = __shfl_sync(FULL, len, leader);
+        const int pv = __shfl_sync(FULL, pred, leader);
+        const unsigned o = __shfl_sync(FULL, out, leader);
         if ((int)lane_id() == leader) len = 0;
-        gather_list<32>(p.col, p.vec_end, s, l, pv, o, lane_id(), sink, pol);
+        gather_list<32>(p.col, p.vec_end, s & ~3, s, l, pv, o, lane_id(), sink, pol);
     }
     // (3) scan-based gather of the short lists through shared memory
     constexpr int SCRATCH = Smem<THREADS, MP>::SCRATCH;
     const int my_len = small ? len : 0;
     for (int round = 0; round < small_total; round += SCRATCH) {
-        int lo = max(small_off, round), hi = min(small_off + my_len, round + SCRATCH);
+        const int lo = max(small_off, round), hi = min(small_off + my_len, round + SCRATCH);
         for (int j = lo; j < hi; j++) {
             sm.gofs[j - round] = start + (j - small_off);
             if (MP) sm.gpred[j - round] = pred;
         }
         __syncthreads();
         const int cnt = min(SCRATCH, small_total - round);
-        for (int k0 = 0; k0 < cnt; k0 += THREADS) {
-            int k = k0 + threadIdx.x;
-            bool valid = k < cnt;
-            int u = -1, pv = 0;
-            if (valid) {
-                u = __ldg(p.col + sm.gofs[k]);
-                if (MP) pv = sm.gpred[k];
+        const int k = threadIdx.x * 4;  // SCRATCH = 4 * THREADS: one pass
+        unsigned valid = 0;
+        int u[4], pv[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            u[j] = -1;
+            pv[j] = 0;
+            if (k + j < cnt) {
+                valid |= 1u << j;
+                u[j] = __ldg(p.col + sm.gofs[k + j]);
+                if (MP) pv[j] = sm.gpred[k + j];
             }
-            sink(valid, u, pv, small_base + unsigned(round + k));
         }
+        sink(valid, u, pv, small_base + unsigned(round + k));
         __syncthreads();
     }
 }
 
-// Grid-wide phase: every CTA takes chunks of the deferred big lists, chunk g of
-// the concatenated chunk sequence going to CTA g mod gridDim.x.
-template <int THREADS, class Sink>
-__device__ __forceinline__ void gather_big_lists(const BfsParams &p, unsigned nbig, const Sink &sink,
-                                                 uint64_t pol) {
-    constexpr int CHUNK = THREADS * 16;
-    const unsigned G = gridDim.x;
-    unsigned g0 = 0;
-    if (nbig > (unsigned)p.big_cap) nbig = p.big_cap;
-    for (unsigned i = 0; i < nbig; i++) {
-        int4 item = __ldcg(p.big_items + i);
-        int s = item.x, l = item.y;
-        unsigned chunks = unsigned((l + CHUNK - 1) / CHUNK);
-        unsigned c = (blockIdx.x + G - (g0 % G)) % G;
-        for (; c < chunks; c += G) {
-            int cs = s + int(c) * CHUNK;
-            int cl = min(CHUNK, l - int(c) * CHUNK);
-            gather_list<THREADS>(p.col, p.vec_end, cs, cl, item.z, unsigned(item.w) + c * CHUNK, threadIdx.x, sink,
-                                 pol);
+// Cuts list [start, start+len) into grid-wide chunks aligned to CHUNK-element
+// windows from the 4-aligned start.  Returns false when the chunk table is
+// full; the entries it reserved are then written empty and the caller's CTA
+// gathers the list itself.
+template <int THREADS>
+__device__ __forceinline__ bool push_chunks(const BfsParams &p, unsigned *chunk_count, int start, int len, int pred,
+                                            unsigned out) {
+    constexpr int CH = chunk_edges<THREADS>();
+    const int a0 = start & ~3, end = start + len;
+    const unsigned nch = unsigned((end - a0 + CH - 1) / CH);
+    const unsigned base = atomicAdd(chunk_count, nch);
+    const unsigned cap = (unsigned)p.chunk_cap;
+    if (base + nch <= cap) {
+        for (unsigned c = 0; c < nch; c++) {
+            const int ws = a0 + int(c) * CH;
+            const int cs = max(ws, start), ce = min(ws + CH, end);
+            p.chunks[base + c] = make_int4(cs, ce - cs, pred, int(out + unsigned(cs - start)));
         }
-        g0 += chunks;
+        return true;
+    }
+    for (unsigned c = base; c < cap && c < base + nch; c++) p.chunks[c] = make_int4(0, 0, 0, 0);
+    return false;
+}
+
+// Grid-wide phase: CTA b gathers chunks b, b + G, b + 2G, ...
+template <int THREADS, class Sink>
+__device__ __forceinline__ void gather_chunks(const BfsParams &p, unsigned n, const Sink &sink, uint64_t pol) {
+    if (n > (unsigned)p.chunk_cap) n = p.chunk_cap;
+    const unsigned G = gridDim.x;
+    unsigned k = blockIdx.x;
+    int4 cur = k < n ? __ldcg(p.chunks + k) : make_int4(0, 0, 0, 0);
+    for (; k < n; k += G) {
+        int4 nxt = (k + G < n) ? __ldcg(p.chunks + k + G) : make_int4(0, 0, 0, 0);
+        if (cur.y > 0)
+            gather_list<THREADS>(p.col, p.vec_end, cur.x & ~3, cur.x, cur.y, cur.z, unsigned(cur.w), threadIdx.x,
+                                 sink, pol);
+        cur = nxt;
     }
 }
 
-// Hand out tiles of the input frontier to CTAs with one atomic each.
+// Hands out tiles of the input frontier to CTAs with one atomic each.
 template <int THREADS, bool MP>
 __device__ __forceinline__ unsigned next_tile(unsigned *steal, Smem<THREADS, MP> &sm) {
     __syncthreads();
@@ -250,15 +346,12 @@ __device__ __forceinline__ unsigned next_tile(unsigned *steal, Smem<THREADS, MP>
     return sm.tile;
 }
 
-// Defers a list to the grid-wide phase; returns true when it was taken.
-__device__ __forceinline__ bool push_big(const BfsParams &p, unsigned *bigc, int start, int len,
-                                         int pred, unsigned out) {
-    unsigned item = atomicAdd(bigc, 1u);
-    if (item < (unsigned)p.big_cap) {
-        p.big_items[item] = make_int4(start, len, pred, int(out));
-        return true;
-    }
-    return false;  // table full: the caller's CTA gathers the list itself
+// Tile size for a frontier of L elements: at most `most`, small enough that
+// there are about two tiles per CTA when the frontier is short.
+__device__ __forceinline__ unsigned tile_size(unsigned L, unsigned most) {
+    const unsigned G2 = 2u * gridDim.x;
+    unsigned t = (L + G2 - 1) / G2;
+    return t < 1u ? 1u : (t > most ? most : t);
 }
 
 __device__ __forceinline__ void row_range(const BfsParams &p, int v, int &start, int &len) {
@@ -270,54 +363,53 @@ __device__ __forceinline__ void row_range(const BfsParams &p, int v, int &start,
 // Level bodies
 // ---------------------------------------------------------------------------------------
 
-// Expand-contract level `it`: vertex frontier queue[it&1] -> queue[(it+1)&1].
-// Neighbours are labelled it+1 when discovered (expand_contract_atomic/cta.cuh:
-// 181-218).  Lists >= big_th are deferred to big[it&3].
+// Expand-contract tile phase of level `it`: vertex frontier queue[it&1] ->
+// discovered vertices in queue[(it+1)&1]; lists >= big_th become chunks counted
+// in big[it&3].
 template <int THREADS, bool MP>
 __device__ void ec_level(const BfsParams &p, int it, unsigned L, Smem<THREADS, MP> &sm, uint64_t pol) {
     Counters *c = p.ctr;
     const int *q_in = p.queue[it & 1];
     DiscoverSink<THREADS, MP> sink{p, sm, p.queue[(it + 1) & 1], &c->qlen[(it + 1) & 3], it + 1};
-    const unsigned ntiles = (L + THREADS - 1) / THREADS;
+    const unsigned tv = tile_size(L, THREADS);
+    const unsigned ntiles = (L + tv - 1) / tv;
     for (;;) {
-        unsigned tile = next_tile<THREADS, MP>(&c->steal[it & 3], sm);
+        const unsigned tile = next_tile<THREADS, MP>(&c->steal[it & 3], sm);
         if (tile >= ntiles) break;
-        unsigned idx = tile * THREADS + threadIdx.x;
+        const unsigned idx = tile * tv + threadIdx.x;
         int v = -1, start = 0, len = 0;
-        if (idx < L) {
+        if (threadIdx.x < tv && idx < L) {
             v = ld_cg(q_in + idx);
             row_range(p, v, start, len);
-            if (len >= p.big_th && push_big(p, &c->big[it & 3], start, len, v, 0u)) len = 0;
+            if (len >= p.big_th && push_chunks<THREADS>(p, &c->big[it & 3], start, len, v, 0u)) len = 0;
         }
         int small_total;
-        int small_off = block_exclusive_scan<THREADS>(len < p.warp_th ? len : 0, small_total, sm.warp_tot);
+        const int small_off = block_exclusive_scan<THREADS>(len < p.warp_th ? len : 0, small_total, sm.warp_tot);
         expand_lists<THREADS, MP>(p, sm, sink, pol, start, len, v, 0u, small_off, small_total, 0u);
     }
 }
 
 template <int THREADS, bool MP>
-__device__ void ec_big(const BfsParams &p, int it, unsigned nbig, Smem<THREADS, MP> &sm, uint64_t pol) {
-    Counters *c = p.ctr;
-    DiscoverSink<THREADS, MP> sink{p, sm, p.queue[(it + 1) & 1], &c->qlen[(it + 1) & 3], it + 1};
-    gather_big_lists<THREADS>(p, nbig, sink, pol);
+__device__ void ec_chunks(const BfsParams &p, int it, unsigned n, Smem<THREADS, MP> &sm, uint64_t pol) {
+    DiscoverSink<THREADS, MP> sink{p, sm, p.queue[(it + 1) & 1], &p.ctr->qlen[(it + 1) & 3], it + 1};
+    gather_chunks<THREADS>(p, n, sink, pol);
 }
 
-// Expands the per-thread lists (start, len, owner pred) of one tile into the
-// edge frontier queue q_out: a two-component block scan sizes the short and
-// the long lists, thread 0 reserves the tile's output with one atomicAdd
-// (ScanTileWithEnqueue, util/scan/cooperative_scan.cuh:173-195), big lists are
-// deferred with their reserved output position.
+// Expands one list per thread into the edge-frontier queue q_out: a
+// two-component block scan sizes the short and the long lists, thread 0
+// reserves the tile's output with one atomicAdd (ScanTileWithEnqueue,
+// util/scan/cooperative_scan.cuh:173-195), lists >= big_th become chunks with
+// their reserved output positions.
 template <int THREADS, bool MP>
-__device__ __forceinline__ void expand_tile_to_edges(const BfsParams &p, Smem<THREADS, MP> &sm,
-                                                     uint64_t pol, int start, int len, int pred,
-                                                     int *q_out, int *pq_out, unsigned *qlen_out,
-                                                     unsigned *bigc) {
+__device__ __forceinline__ void expand_tile_to_edges(const BfsParams &p, Smem<THREADS, MP> &sm, uint64_t pol,
+                                                     int start, int len, int pred, int *q_out, int *pq_out,
+                                                     unsigned *qlen_out, unsigned *chunk_count) {
     const bool small = len < p.warp_th;
     int2 total;
-    int2 off = block_exclusive_scan2<THREADS>(make_int2(small ? len : 0, small ? 0 : len), total,
-                                              sm.warp_tot);
+    const int2 off =
+        block_exclusive_scan2<THREADS>(make_int2(small ? len : 0, small ? 0 : len), total, sm.warp_tot);
     if (threadIdx.x == 0) {
-        unsigned need = unsigned(total.x + total.y);
+        const unsigned need = unsigned(total.x + total.y);
         unsigned base = 0;
         if (need) {
             base = atomicAdd(qlen_out, need);
@@ -330,68 +422,80 @@ __device__ __forceinline__ void expand_tile_to_edges(const BfsParams &p, Smem<TH
     }
     __syncthreads();
     const unsigned base = sm.out_base;
-    if (base == NO_SPACE) return;  // uniform: the whole tile is dropped on overflow
-    const unsigned small_base = base;
-    unsigned out = small ? small_base + off.x : base + unsigned(total.x) + off.y;
-    if (len >= p.big_th && push_big(p, bigc, start, len, pred, out)) len = 0;
+    if (base == NO_SPACE) return;  // uniform: the tile's output is dropped on overflow
+    const unsigned out = small ? base + off.x : base + unsigned(total.x) + off.y;
+    if (len >= p.big_th && push_chunks<THREADS>(p, chunk_count, start, len, pred, out)) len = 0;
     PositionSink<MP> sink{q_out, pq_out};
-    expand_lists<THREADS, MP>(p, sm, sink, pol, start, len, pred, out, off.x, total.x, small_base);
+    expand_lists<THREADS, MP>(p, sm, sink, pol, start, len, pred, out, off.x, total.x, base);
 }
 
-// Culls one edge-frontier element: optional warp / history culls, then the
-// exact bitmask test-and-set.  Survivors are labelled (iteration or pred).
+// Loads up to 4 edge-frontier elements of tile `tile` (tile size te) per
+// thread, strided by THREADS, and culls them.  Returns the survivors' bits.
 template <int THREADS, bool MP>
-__device__ __forceinline__ bool contract_one(const BfsParams &p, Smem<THREADS, MP> &sm, bool valid,
-                                             int u, int pred, int it) {
-    valid = pre_cull<THREADS, MP>(valid, u, p.cull_flags, sm);
-    if (valid) {
-        if ((unsigned)u >= (unsigned)p.nodes) {
-            atomicOr(&p.ctr->error, ERR_BAD_VERTEX);
-            valid = false;
-        } else if (mark_visited(p.mask, u)) {
-            p.labels[u] = MP ? pred : it;
-        } else {
-            valid = false;
+__device__ __forceinline__ unsigned contract_tile_load(const BfsParams &p, Smem<THREADS, MP> &sm, const int *q_in,
+                                                       const int *pq_in, unsigned L, unsigned tile, unsigned te,
+                                                       int (&u)[4], int (&pr)[4]) {
+    unsigned valid = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const unsigned r = j * THREADS + threadIdx.x;
+        const unsigned idx = tile * te + r;
+        u[j] = -1;
+        pr[j] = 0;
+        if (r < te && idx < L) {
+            valid |= 1u << j;
+            u[j] = ld_cg(q_in + idx);
+            if (MP) pr[j] = ld_cg(pq_in + idx);
         }
     }
-    return valid;
+    return cull4<THREADS, MP>(p, sm, valid, u);
 }
 
 // Contract-expand level `it` (contract_expand_atomic/cta.cuh:573-709): edge
-// frontier queue[it&1] -> cull + label it -> expand -> queue[(it+1)&1].
+// frontier queue[it&1] -> cull, label it -> survivors compacted in shared
+// memory -> expanded into queue[(it+1)&1].
 template <int THREADS, bool MP>
 __device__ void ce_level(const BfsParams &p, int it, unsigned L, Smem<THREADS, MP> &sm, uint64_t pol) {
     Counters *c = p.ctr;
     const int *q_in = p.queue[it & 1];
     const int *pq_in = p.pred_queue[it & 1];
-    const unsigned ntiles = (L + THREADS - 1) / THREADS;
+    const unsigned te = tile_size(L, Smem<THREADS, MP>::CTILE);
+    const unsigned ntiles = (L + te - 1) / te;
     for (;;) {
-        unsigned tile = next_tile<THREADS, MP>(&c->steal[it & 3], sm);
+        const unsigned tile = next_tile<THREADS, MP>(&c->steal[it & 3], sm);
         if (tile >= ntiles) break;
-        unsigned idx = tile * THREADS + threadIdx.x;
-        bool valid = idx < L;
-        int u = -1, pred = 0;
-        if (valid) {
-            u = ld_cg(q_in + idx);
-            if (MP) pred = ld_cg(pq_in + idx);
+        int u[4], pr[4];
+        const unsigned surv = contract_tile_load<THREADS, MP>(p, sm, q_in, pq_in, L, tile, te, u, pr);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if ((surv >> j) & 1u) p.labels[u[j]] = MP ? pr[j] : it;
+        int nsurv;
+        int off = block_exclusive_scan<THREADS>(__popc(surv), nsurv, sm.warp_tot);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if ((surv >> j) & 1u) sm.surv[off++] = u[j];
+        __syncthreads();
+        for (int r0 = 0; r0 < nsurv; r0 += THREADS) {
+            int v = -1, start = 0, len = 0;
+            if (r0 + (int)threadIdx.x < nsurv) {
+                v = sm.surv[r0 + threadIdx.x];
+                row_range(p, v, start, len);
+            }
+            expand_tile_to_edges<THREADS, MP>(p, sm, pol, start, len, v, p.queue[(it + 1) & 1],
+                                              p.pred_queue[(it + 1) & 1], &c->qlen[(it + 1) & 3], &c->big[it & 3]);
         }
-        valid = contract_one<THREADS, MP>(p, sm, valid, u, pred, it);
-        int start = 0, len = 0;
-        if (valid) row_range(p, u, start, len);
-        expand_tile_to_edges<THREADS, MP>(p, sm, pol, start, len, u, p.queue[(it + 1) & 1],
-                                          p.pred_queue[(it + 1) & 1], &c->qlen[(it + 1) & 3],
-                                          &c->big[it & 3]);
     }
 }
 
+// Chunk phase after a level that wrote an edge frontier to queue[out_sel].
 template <int THREADS, bool MP>
-__device__ void edges_big(const BfsParams &p, int out_sel, unsigned nbig, uint64_t pol) {
+__device__ void edge_chunks(const BfsParams &p, int out_sel, unsigned n, uint64_t pol) {
     PositionSink<MP> sink{p.queue[out_sel], p.pred_queue[out_sel]};
-    gather_big_lists<THREADS>(p, nbig, sink, pol);
+    gather_chunks<THREADS>(p, n, sink, pol);
 }
 
 // Two-phase contract (two_phase/contract_atomic/cta.cuh:494-572): edge frontier
-// queue[qi&1] -> cull + label `it` -> compacted vertex frontier queue[(qi+1)&1],
+// queue[qi&1] -> cull, label `it` -> compacted vertex frontier queue[(qi+1)&1],
 // allocated by a block scan and one atomicAdd per tile.
 template <int THREADS, bool MP>
 __device__ void tp_contract(const BfsParams &p, int it, int qi, unsigned L, Smem<THREADS, MP> &sm) {
@@ -399,20 +503,18 @@ __device__ void tp_contract(const BfsParams &p, int it, int qi, unsigned L, Smem
     const int *q_in = p.queue[qi & 1];
     const int *pq_in = p.pred_queue[qi & 1];
     int *q_out = p.queue[(qi + 1) & 1];
-    const unsigned ntiles = (L + THREADS - 1) / THREADS;
+    const unsigned te = tile_size(L, Smem<THREADS, MP>::CTILE);
+    const unsigned ntiles = (L + te - 1) / te;
     for (;;) {
-        unsigned tile = next_tile<THREADS, MP>(&c->steal[qi & 3], sm);
+        const unsigned tile = next_tile<THREADS, MP>(&c->steal[qi & 3], sm);
         if (tile >= ntiles) break;
-        unsigned idx = tile * THREADS + threadIdx.x;
-        bool valid = idx < L;
-        int u = -1, pred = 0;
-        if (valid) {
-            u = ld_cg(q_in + idx);
-            if (MP) pred = ld_cg(pq_in + idx);
-        }
-        valid = contract_one<THREADS, MP>(p, sm, valid, u, pred, it);
+        int u[4], pr[4];
+        const unsigned surv = contract_tile_load<THREADS, MP>(p, sm, q_in, pq_in, L, tile, te, u, pr);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if ((surv >> j) & 1u) p.labels[u[j]] = MP ? pr[j] : it;
         int total;
-        int off = block_exclusive_scan<THREADS>(valid ? 1 : 0, total, sm.warp_tot);
+        int off = block_exclusive_scan<THREADS>(__popc(surv), total, sm.warp_tot);
         if (threadIdx.x == 0) {
             unsigned base = total ? atomicAdd(&c->qlen[(qi + 1) & 3], (unsigned)total) : 0u;
             if ((unsigned long long)base + total > (unsigned long long)p.qcap) {
@@ -422,7 +524,12 @@ __device__ void tp_contract(const BfsParams &p, int it, int qi, unsigned L, Smem
             sm.out_base = base;
         }
         __syncthreads();
-        if (valid && sm.out_base != NO_SPACE) q_out[sm.out_base + off] = u;
+        const unsigned base = sm.out_base;
+        if (base != NO_SPACE) {
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if ((surv >> j) & 1u) q_out[base + off++] = u[j];
+        }
     }
 }
 
@@ -432,19 +539,19 @@ template <int THREADS, bool MP>
 __device__ void tp_expand(const BfsParams &p, int qi, unsigned L, Smem<THREADS, MP> &sm, uint64_t pol) {
     Counters *c = p.ctr;
     const int *q_in = p.queue[qi & 1];
-    const unsigned ntiles = (L + THREADS - 1) / THREADS;
+    const unsigned tv = tile_size(L, THREADS);
+    const unsigned ntiles = (L + tv - 1) / tv;
     for (;;) {
-        unsigned tile = next_tile<THREADS, MP>(&c->steal[qi & 3], sm);
+        const unsigned tile = next_tile<THREADS, MP>(&c->steal[qi & 3], sm);
         if (tile >= ntiles) break;
-        unsigned idx = tile * THREADS + threadIdx.x;
+        const unsigned idx = tile * tv + threadIdx.x;
         int v = -1, start = 0, len = 0;
-        if (idx < L) {
+        if (threadIdx.x < tv && idx < L) {
             v = ld_cg(q_in + idx);
             row_range(p, v, start, len);
         }
         expand_tile_to_edges<THREADS, MP>(p, sm, pol, start, len, v, p.queue[(qi + 1) & 1],
-                                          p.pred_queue[(qi + 1) & 1], &c->qlen[(qi + 1) & 3],
-                                          &c->big[qi & 3]);
+                                          p.pred_queue[(qi + 1) & 1], &c->qlen[(qi + 1) & 3], &c->big[qi & 3]);
     }
 }
 
@@ -456,11 +563,30 @@ __device__ __forceinline__ void ring_prepare(Counters *c, int q) {
     c->big[(q + 1) & 3] = 0u;
 }
 
+__device__ __forceinline__ void log_level_start(const BfsParams &p, int idx, unsigned frontier) {
+    if (p.levels && idx < p.level_cap) {
+        LevelRecord r;
+        r.t_start = globaltimer_ns();
+        r.t_tiles = 0;
+        r.frontier = frontier;
+        r.chunks = 0;
+        p.levels[idx] = r;
+    }
+}
+__device__ __forceinline__ void log_level_tiles(const BfsParams &p, int idx, unsigned chunks) {
+    if (p.levels && idx < p.level_cap) {
+        p.levels[idx].t_tiles = globaltimer_ns();
+        p.levels[idx].chunks = chunks;
+    }
+}
+
 template <int THREADS, bool MP>
 __device__ __forceinline__ void init_hist(Smem<THREADS, MP> &sm, unsigned flags) {
     if (flags & CULL_HISTORY)
         for (int i = threadIdx.x; i < HIST_SIZE; i += THREADS) sm.hist[i] = -1;
 }
+
+__device__ __forceinline__ bool leader() { return blockIdx.x == 0 && threadIdx.x == 0; }
 
 // ---------------------------------------------------------------------------------------
 // Kernels
@@ -488,6 +614,25 @@ __global__ void search_init_kernel(BfsParams p, int strategy, int mark_pred) {
     }
 }
 
+// Leaves the loop of a fused kernel (every CTA decides alike: L and the level
+// index are the same everywhere after a barrier).
+__device__ __forceinline__ bool stop_level_loop(const BfsParams &p, int level, unsigned L) {
+    if (L == 0u) return true;
+    if (level_limit_hit(level, p.nodes)) {
+        if (leader()) atomicOr(&p.ctr->error, ERR_LEVEL_LIMIT);
+        return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void finish_search(const BfsParams &p, int iteration, int log_idx) {
+    if (leader()) {
+        p.ctr->iteration = iteration;
+        log_level_start(p, log_idx, 0u);  // end-of-search timestamp
+        atomicOr(&p.ctr->sticky, ld_relaxed_gpu(&p.ctr->error));
+    }
+}
+
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS) ec_fused_kernel(BfsParams p) {
     __shared__ Smem<THREADS, MP> sm;
@@ -496,29 +641,24 @@ __global__ void __launch_bounds__(THREADS) ec_fused_kernel(BfsParams p) {
     Counters *c = p.ctr;
     int it = 0;
     for (;;) {
-        unsigned L = ld_cg(&c->qlen[it & 3]);
-        if (L == 0u) break;
-        if (level_limit_hit(it, p.nodes)) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&c->error, ERR_LEVEL_LIMIT);
-            break;
-        }
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const unsigned L = ld_cg(&c->qlen[it & 3]);
+        if (stop_level_loop(p, it, L)) break;
+        if (leader()) {
             ring_prepare(c, it);
             c->total_queued += L;
+            log_level_start(p, it, L);
         }
         ec_level<THREADS, MP>(p, it, L, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
-        unsigned nbig = ld_cg(&c->big[it & 3]);
-        if (nbig) {
-            ec_big<THREADS, MP>(p, it, nbig, sm, pol);
+        const unsigned nch = ld_cg(&c->big[it & 3]);
+        if (leader()) log_level_tiles(p, it, nch);
+        if (nch) {
+            ec_chunks<THREADS, MP>(p, it, nch, sm, pol);
             if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         }
         it++;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        c->iteration = it;
-        atomicOr(&c->sticky, ld_relaxed_gpu(&c->error));
-    }
+    finish_search(p, it, it);
 }
 
 template <int THREADS, bool MP>
@@ -529,34 +669,30 @@ __global__ void __launch_bounds__(THREADS) ce_fused_kernel(BfsParams p) {
     Counters *c = p.ctr;
     int it = 0;
     for (;;) {
-        unsigned L = ld_cg(&c->qlen[it & 3]);
-        if (L == 0u) break;
-        if (level_limit_hit(it, p.nodes)) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&c->error, ERR_LEVEL_LIMIT);
-            break;
-        }
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const unsigned L = ld_cg(&c->qlen[it & 3]);
+        if (stop_level_loop(p, it, L)) break;
+        if (leader()) {
             ring_prepare(c, it);
             c->total_queued += L;
+            log_level_start(p, it, L);
         }
         ce_level<THREADS, MP>(p, it, L, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
-        unsigned nbig = ld_cg(&c->big[it & 3]);
-        if (nbig) {
-            edges_big<THREADS, MP>(p, (it + 1) & 1, nbig, pol);
+        const unsigned nch = ld_cg(&c->big[it & 3]);
+        if (leader()) log_level_tiles(p, it, nch);
+        if (nch) {
+            edge_chunks<THREADS, MP>(p, (it + 1) & 1, nch, pol);
             if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         }
         it++;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        c->iteration = it;
-        atomicOr(&c->sticky, ld_relaxed_gpu(&c->error));
-    }
+    finish_search(p, it, it);
 }
 
 // Fused two-phase: contract and expand phases alternate across grid barriers
 // (the reference's fused two-phase kernel, two_phase/kernel.cuh:60-313, which
-// its enactor cannot instantiate, enactor_two_phase.cuh:302).
+// its enactor cannot instantiate, enactor_two_phase.cuh:302).  The level log is
+// indexed by phase (2 * iteration for contract, + 1 for expand).
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS) tp_fused_kernel(BfsParams p) {
     __shared__ Smem<THREADS, MP> sm;
@@ -566,35 +702,33 @@ __global__ void __launch_bounds__(THREADS) tp_fused_kernel(BfsParams p) {
     int it = 0, qi = 0;
     for (;;) {
         unsigned L = ld_cg(&c->qlen[qi & 3]);
-        if (L == 0u) break;
-        if (level_limit_hit(it, p.nodes)) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&c->error, ERR_LEVEL_LIMIT);
-            break;
-        }
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (stop_level_loop(p, it, L)) break;
+        if (leader()) {
             ring_prepare(c, qi);
             c->total_queued += L;
+            log_level_start(p, qi, L);
         }
         tp_contract<THREADS, MP>(p, it, qi, L, sm);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         qi++;
         L = ld_cg(&c->qlen[qi & 3]);
         if (L == 0u) break;
-        if (blockIdx.x == 0 && threadIdx.x == 0) ring_prepare(c, qi);
+        if (leader()) {
+            ring_prepare(c, qi);
+            log_level_start(p, qi, L);
+        }
         tp_expand<THREADS, MP>(p, qi, L, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
-        unsigned nbig = ld_cg(&c->big[qi & 3]);
-        if (nbig) {
-            edges_big<THREADS, MP>(p, (qi + 1) & 1, nbig, pol);
+        const unsigned nch = ld_cg(&c->big[qi & 3]);
+        if (leader()) log_level_tiles(p, qi, nch);
+        if (nch) {
+            edge_chunks<THREADS, MP>(p, (qi + 1) & 1, nch, pol);
             if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         }
         qi++;
         it++;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        c->iteration = it;
-        atomicOr(&c->sticky, ld_relaxed_gpu(&c->error));
-    }
+    finish_search(p, it, qi + 1);
 }
 
 // ---- per-level kernels for the graph-driven (iterative) variants ----------------
@@ -603,20 +737,22 @@ template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS) ec_level_kernel(BfsParams p) {
     __shared__ Smem<THREADS, MP> sm;
     init_hist(sm, p.cull_flags);
-    const int it = *(volatile int *)&p.ctr->cur_it;
+    const int it = p.ctr->cur_it;
     const unsigned L = p.ctr->qlen[it & 3];
     if (L == 0u || p.ctr->error) return;
+    if (leader()) log_level_start(p, it, L);
     ec_level<THREADS, MP>(p, it, L, sm, policy_evict_first());
 }
 
 template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS) ec_big_kernel(BfsParams p) {
+__global__ void __launch_bounds__(THREADS) ec_chunks_kernel(BfsParams p) {
     __shared__ Smem<THREADS, MP> sm;
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it;
-    const unsigned nbig = p.ctr->big[it & 3];
-    if (nbig == 0u || p.ctr->error) return;
-    ec_big<THREADS, MP>(p, it, nbig, sm, policy_evict_first());
+    const unsigned n = p.ctr->big[it & 3];
+    if (leader()) log_level_tiles(p, it, n);
+    if (n == 0u || p.ctr->error) return;
+    ec_chunks<THREADS, MP>(p, it, n, sm, policy_evict_first());
 }
 
 template <int THREADS, bool MP>
@@ -626,18 +762,19 @@ __global__ void __launch_bounds__(THREADS) ce_level_kernel(BfsParams p) {
     const int it = p.ctr->cur_it;
     const unsigned L = p.ctr->qlen[it & 3];
     if (L == 0u || p.ctr->error) return;
+    if (leader()) log_level_start(p, it, L);
     ce_level<THREADS, MP>(p, it, L, sm, policy_evict_first());
 }
 
-// Grid-wide big-list pass after a level that writes an edge frontier; `phase`
-// is the ring index of that level (iteration for contract-expand, qi+1 for the
-// two-phase expand).
+// Chunk pass after a per-level kernel that wrote an edge frontier: ring index
+// q = iteration (contract-expand) or 2 * iteration + 1 (two-phase expand).
 template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS) edges_big_kernel(BfsParams p, int two_phase) {
+__global__ void __launch_bounds__(THREADS) edge_chunks_kernel(BfsParams p, int two_phase) {
     const int q = two_phase ? p.ctr->cur_it * 2 + 1 : p.ctr->cur_it;
-    const unsigned nbig = p.ctr->big[q & 3];
-    if (nbig == 0u || p.ctr->error) return;
-    edges_big<THREADS, MP>(p, (q + 1) & 1, nbig, policy_evict_first());
+    const unsigned n = p.ctr->big[q & 3];
+    if (leader()) log_level_tiles(p, q, n);
+    if (n == 0u || p.ctr->error) return;
+    edge_chunks<THREADS, MP>(p, (q + 1) & 1, n, policy_evict_first());
 }
 
 // Two-phase per-level: qi = 2 * it (contract) and 2 * it + 1 (expand).
@@ -648,6 +785,7 @@ __global__ void __launch_bounds__(THREADS) tp_contract_kernel(BfsParams p) {
     const int it = p.ctr->cur_it, qi = 2 * it;
     const unsigned L = p.ctr->qlen[qi & 3];
     if (L == 0u || p.ctr->error) return;
+    if (leader()) log_level_start(p, qi, L);
     tp_contract<THREADS, MP>(p, it, qi, L, sm);
 }
 
@@ -658,6 +796,7 @@ __global__ void __launch_bounds__(THREADS) tp_expand_kernel(BfsParams p) {
     const int it = p.ctr->cur_it, qi = 2 * it + 1;
     const unsigned L = p.ctr->qlen[qi & 3];
     if (L == 0u || p.ctr->error) return;
+    if (leader()) log_level_start(p, qi, L);
     tp_expand<THREADS, MP>(p, qi, L, sm, policy_evict_first());
 }
 
@@ -674,7 +813,7 @@ __global__ void level_control_kernel(BfsParams p, int strategy) {
         const unsigned eq = c->qlen[(qi + 2) & 3];  // expand output
         c->total_queued += c->qlen[qi & 3];
         if (vq == 0u) {
-            c->iteration = it;  // reference breaks after contract without ++
+            c->iteration = it;  // the reference leaves after contract without ++
             more = false;
         } else {
             c->iteration = it + 1;
@@ -686,6 +825,7 @@ __global__ void level_control_kernel(BfsParams p, int strategy) {
         c->qlen[(qi + 3) & 3] = 0u;
         c->qlen[(qi + 4) & 3] = 0u;
         c->big[(qi + 3) & 3] = 0u;
+        if (!more) log_level_start(p, vq == 0u ? qi + 1 : qi + 2, 0u);
     } else {
         const unsigned next = c->qlen[(it + 1) & 3];
         c->total_queued += c->qlen[it & 3];
@@ -694,6 +834,7 @@ __global__ void level_control_kernel(BfsParams p, int strategy) {
         c->steal[(it + 1) & 3] = 0u;
         c->big[(it + 1) & 3] = 0u;
         c->qlen[(it + 2) & 3] = 0u;
+        if (!more) log_level_start(p, it + 1, 0u);
     }
     if (more && level_limit_hit(it + 1, p.nodes)) {
         c->error |= ERR_LEVEL_LIMIT;
@@ -740,24 +881,23 @@ static KernelFn fused_fn_t(int threads, int strategy) {
 }
 
 static KernelFn pick_fused(const KernelConfig &kc) {
-    return kc.mark_pred ? fused_fn_t<true>(kc.threads, kc.strategy)
-                        : fused_fn_t<false>(kc.threads, kc.strategy);
+    return kc.mark_pred ? fused_fn_t<true>(kc.threads, kc.strategy) : fused_fn_t<false>(kc.threads, kc.strategy);
 }
 
 struct LevelFns {
     KernelFn level_a;  // ec_level / ce_level / tp_contract
-    KernelFn level_b;  // ec_big / (none) / tp_expand
-    void (*edges_big)(BfsParams, int);
+    KernelFn level_b;  // ec_chunks / (none) / tp_expand
+    void (*edge_chunks)(BfsParams, int);
 };
 
 template <int THREADS, bool MP>
 static LevelFns level_fns(int strategy) {
     LevelFns f{};
-    f.edges_big = edges_big_kernel<THREADS, MP>;
+    f.edge_chunks = edge_chunks_kernel<THREADS, MP>;
     switch (strategy) {
     case STRATEGY_EXPAND_CONTRACT:
         f.level_a = ec_level_kernel<THREADS, MP>;
-        f.level_b = ec_big_kernel<THREADS, MP>;
+        f.level_b = ec_chunks_kernel<THREADS, MP>;
         break;
     case STRATEGY_CONTRACT_EXPAND:
         f.level_a = ce_level_kernel<THREADS, MP>;
@@ -781,8 +921,7 @@ static LevelFns level_fns_t(int threads, int strategy) {
 }
 
 static LevelFns pick_level(const KernelConfig &kc) {
-    return kc.mark_pred ? level_fns_t<true>(kc.threads, kc.strategy)
-                        : level_fns_t<false>(kc.threads, kc.strategy);
+    return kc.mark_pred ? level_fns_t<true>(kc.threads, kc.strategy) : level_fns_t<false>(kc.threads, kc.strategy);
 }
 
 static cudaError_t grid_for(const void *fn, int threads, int *grid) {
@@ -839,8 +978,7 @@ cudaError_t build_level_graph(BfsParams &p, const KernelConfig &kc, int grid, cu
         cudaGraph_t body = np.conditional.phGraph_out[0];
 
         if ((e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking))) break;
-        if ((e = cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0,
-                                               cudaStreamCaptureModeThreadLocal)))
+        if ((e = cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)))
             break;
         LevelFns f = pick_level(kc);
         const int T = kc.threads;
@@ -848,10 +986,10 @@ cudaError_t build_level_graph(BfsParams &p, const KernelConfig &kc, int grid, cu
         if (kc.strategy == STRATEGY_EXPAND_CONTRACT) {
             f.level_b<<<grid, T, 0, cap>>>(p);
         } else if (kc.strategy == STRATEGY_CONTRACT_EXPAND) {
-            f.edges_big<<<grid, T, 0, cap>>>(p, 0);
+            f.edge_chunks<<<grid, T, 0, cap>>>(p, 0);
         } else {
             f.level_b<<<grid, T, 0, cap>>>(p);
-            f.edges_big<<<grid, T, 0, cap>>>(p, 1);
+            f.edge_chunks<<<grid, T, 0, cap>>>(p, 1);
         }
         level_control_kernel<<<1, 32, 0, cap>>>(p, kc.strategy);
         cudaError_t le = cudaGetLastError();
@@ -877,8 +1015,8 @@ cudaError_t run_barrier_timeout_probe(int grid, unsigned long long wait_ns, unsi
     do {
         if ((e = cudaMemset(c, 0, sizeof(Counters)))) break;
         void *args[] = {&c, &wait_ns};
-        if ((e = cudaLaunchCooperativeKernel((const void *)barrier_timeout_probe_kernel, dim3(grid),
-                                             dim3(32), args, 0, nullptr)))
+        if ((e = cudaLaunchCooperativeKernel((const void *)barrier_timeout_probe_kernel, dim3(grid), dim3(32), args, 0,
+                                             nullptr)))
             break;
         if ((e = cudaDeviceSynchronize())) break;
         Counters h;

@@ -19,6 +19,16 @@ enum CullFlags : unsigned {
     CULL_HISTORY = 2u,  // per-CTA shared-memory history hash
 };
 
+// One record per BFS level, written by one thread of the kernel that runs it:
+// %globaltimer at the level start and after its tile phase, the input
+// frontier length and the number of grid-wide chunks it produced.
+struct LevelRecord {
+    unsigned long long t_start;
+    unsigned long long t_tiles;
+    unsigned frontier;
+    unsigned chunks;
+};
+
 // Everything a BFS kernel needs, passed by value.
 struct BfsParams {
     const int *row_offsets;  // nodes + 1
@@ -27,20 +37,26 @@ struct BfsParams {
     unsigned *mask;          // visited bitmask, bit (v & 31) of word v >> 5
     int *queue[2];           // frontier ping-pong
     int *pred_queue[2];      // predecessor ping-pong (edge frontiers, mark_pred)
-    int4 *big_items;         // lists gathered grid-wide: {start, len, pred, out}
+    int4 *chunks;            // grid-wide gather chunks: {start, len, pred, out}
+    LevelRecord *levels;     // per-level log (level_cap records)
     Counters *ctr;
     unsigned long long wait_ns;      // grid-barrier spin limit
     unsigned long long cond_handle;  // cudaGraphConditionalHandle (per-level graphs)
     long long qcap;                  // elements per frontier queue
-    int big_cap;                     // entries of big_items
+    int chunk_cap;                   // entries of chunks
+    int level_cap;                   // entries of levels
     int vec_end;                     // 16-byte loads of col are safe below this index
     int nodes;
     int src;
     int warp_th;  // lists >= warp_th are gathered by a warp
     int cta_th;   // lists >= cta_th are gathered by the whole CTA
-    int big_th;   // lists >= big_th are gathered by every CTA of the grid
+    int big_th;   // lists >= big_th are cut into chunks gathered by the whole grid
     unsigned cull_flags;
 };
+
+// Edges per grid-wide chunk: one 16-byte load per thread of a CTA.
+template <int THREADS>
+__host__ __device__ constexpr int chunk_edges() { return THREADS * 4; }
 
 struct KernelConfig {
     int strategy;

@@ -134,8 +134,8 @@ EDGE_CASES = {
     "directed_chain": lambda: _graph(list(range(999)), list(range(1, 1000)), 1000),
     "path_5000": lambda: _graph(list(range(4999)) + list(range(1, 5000)),
                                 list(range(1, 5000)) + list(range(4999)), 5000),
-    "star_200k": lambda: _graph([0] * 200000 + list(range(1, 200001)),
-                                list(range(1, 200001)) + [0] * 200000, 200001),
+    "star_20k": lambda: _graph([0] * 20000 + list(range(1, 20001)),
+                                list(range(1, 20001)) + [0] * 20000, 20001),
 }
 
 
@@ -254,3 +254,23 @@ def test_problem_reused_across_strategies(cuda_device, oracle, rmat16):
         for strategy in [0, 1, 2, 0]:
             labels, _ = run_search(g, strategy, 1, s, problem=prob)
             assert oracle.first_mismatch(labels, ref) == -1
+
+
+def test_level_log_matches_oracle_levels(cuda_device, oracle, rmat16):
+    """The per-level log's frontier lengths equal the oracle's level sizes
+    (expand-contract: vertex frontier of depth d at level d)."""
+    b = bfs_mod()
+    g = rmat16
+    s = int(g.sample_sources(1, 3)[0])
+    ref, _ = oracle.bfs(g, s)
+    prob = b.CsrProblem(False).from_graph(g)
+    for variant in VARIANTS:
+        en = b.EnactorExpandContract()
+        en.set_level_log(True)
+        b.check(prob.Reset(en.GetFrontierType(), 1.3))
+        b.check(en.EnactFusedSearch(prob, s) if variant == 1 else en.EnactIterativeSearch(prob, s))
+        log = en.level_log()
+        sizes = [int((ref == d).sum()) for d in range(int(ref.max()) + 1)]
+        assert [r["frontier"] for r in log[:-1]] == sizes
+        assert log[-1]["frontier"] == 0
+        assert all(log[i]["start_ns"] <= log[i + 1]["start_ns"] for i in range(len(log) - 1))
