@@ -42,7 +42,7 @@ SIGNATURES = {
     "b40c_enactor_get_statistics": (c_int, [c_void_p, POINTER(c_longlong), POINTER(c_int), POINTER(c_double)]),
     "b40c_enactor_last_elapsed_ms": (c_int, [c_void_p, POINTER(c_float)]),
     "b40c_enactor_set_stream": (c_int, [c_void_p, c_void_p]),
-    "b40c_enactor_set_policy": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int]),
+    "b40c_enactor_set_policy": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
     "b40c_enactor_set_level_log": (c_int, [c_void_p, c_int]),
     "b40c_enactor_level_log": (c_int, [c_void_p, c_int, POINTER(c_int64), POINTER(c_int64), POINTER(c_int),
                                        POINTER(c_int), POINTER(c_int)]),

@@ -35,9 +35,9 @@ __device__ __forceinline__ bool level_limit_hit(int it, int nodes) { return it >
 
 // Per-search device counters.  ring[x][it & 3] as CtaWorkProgress does.
 struct alignas(128) Counters {
-    unsigned qlen[4];    // qlen[it&3]: length of the input frontier of iteration it
-    unsigned steal[4];   // steal[it&3]: next tile to hand out in iteration it
-    unsigned big[4];     // big[it&3]: big-list items pushed in iteration it
+    unsigned qlen[4];    // qlen[q&3]: length of the input frontier queue of phase q
+    unsigned steal[4];   // steal[q&3]: next warp tile to hand out in phase q
+    unsigned big[4];     // big[q&3]: grid-wide chunks of neighbour lists input to phase q
     unsigned error;      // ERR_* bits
     int iteration;       // iteration counter at exit (reference d_iteration)
     int cur_it;          // current iteration for per-level (graph-driven) kernels

@@ -4,7 +4,7 @@
 // (b40c/graph/bfs/csr_problem.cuh:68-751) for one GPU: it owns the device CSR,
 // labels, visited mask and frontier queues.  b40c_enactor mirrors the
 // Enactor{ExpandContract,ContractExpand,TwoPhase} classes: it owns the search
-// counters, the grid-wide chunk table, its stream, timing events, the cached
+// counters, the two grid-wide chunk tables, its stream, timing events, the cached
 // per-level CUDA graph.  Each entry point returns a cudaError_t value and
 // records a message in the thread's error slot (B40CPerror,
 // b40c/util/error_utils.cuh:44-103).
@@ -78,15 +78,15 @@ struct b40c_enactor {
     int strategy = B40C_EXPAND_CONTRACT;
     bool instrument = false, debug = false;
     int threads = 256;
-    int warp_th = 32, cta_th = 256, big_th = 1024;
+    int warp_th = 32, cta_th = 1024;
     unsigned cull_flags = 0;
     unsigned long long wait_ns = 5000000000ull;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     Counters *d_ctr = nullptr;
     Counters *h_ctr = nullptr;  // pinned
-    int4 *d_chunks = nullptr;
-    int chunk_cap = 0;
+    int4 *d_chunks[2] = {nullptr, nullptr};
+    int chunk_cap = 0;  // entries per table
     LevelRecord *d_levels = nullptr;  // per-level log, when enabled
     bool log_levels = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -229,15 +229,18 @@ int ensure_enactor_buffers(b40c_enactor *e, b40c_problem *p) {
         std::memset(e->h_ctr, 0, sizeof(Counters));
     }
     // Chunks per level: each vertex expands once per search, and a list of
-    // len >= big_th edges takes at most len / CH + 2 chunks (CH >= 512 edges).
-    const long long bt = std::max(1, std::max(e->big_th, std::max(e->cta_th, e->warp_th)));
+    // len >= cta_th edges takes at most len / CH + 2 chunks (CH >= 2048 edges).
+    const long long bt = std::max(1, std::max(e->cta_th, e->warp_th));
     long long need = p->edges / chunk_edges<128>() + 2 * (p->edges / bt) + 64;
     if (need > (1ll << 30)) need = 1ll << 30;
     if (e->chunk_cap < need) {
-        cudaFree(e->d_chunks);
-        e->d_chunks = nullptr;
+        for (int i = 0; i < 2; i++) {
+            cudaFree(e->d_chunks[i]);
+            e->d_chunks[i] = nullptr;
+        }
         e->chunk_cap = 0;
-        CUDA_TRY(cudaMalloc(&e->d_chunks, sizeof(int4) * size_t(need)), "Enactor cudaMalloc chunk table");
+        for (int i = 0; i < 2; i++)
+            CUDA_TRY(cudaMalloc(&e->d_chunks[i], sizeof(int4) * size_t(need)), "Enactor cudaMalloc chunk table");
         e->chunk_cap = int(need);
     }
     if (e->log_levels && !e->d_levels)
@@ -255,7 +258,8 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
         bp.queue[i] = p->d_queue[i];
         bp.pred_queue[i] = p->d_pred[i];
     }
-    bp.chunks = e->d_chunks;
+    bp.chunks[0] = e->d_chunks[0];
+    bp.chunks[1] = e->d_chunks[1];
     bp.levels = e->log_levels ? e->d_levels : nullptr;
     bp.level_cap = LEVEL_LOG_CAP;
     bp.ctr = e->d_ctr;
@@ -271,7 +275,6 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
     bp.src = src;
     bp.warp_th = e->warp_th;
     bp.cta_th = std::max(e->cta_th, e->warp_th);
-    bp.big_th = std::max(e->big_th, bp.cta_th);
     bp.cull_flags = e->cull_flags;
     if (qcap < 1) return set_error(B40C_ERR_ILLEGAL_STATE, "frontier queues not allocated: call Reset first");
     if (p->mark_pred && e->strategy != B40C_EXPAND_CONTRACT && (!p->d_pred[0] || !p->d_pred[1]))
@@ -595,7 +598,8 @@ extern "C" int b40c_enactor_destroy(b40c_enactor_t *e) {
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
     if (e->graph) cudaGraphDestroy(e->graph);
     cudaFree(e->d_ctr);
-    cudaFree(e->d_chunks);
+    cudaFree(e->d_chunks[0]);
+    cudaFree(e->d_chunks[1]);
     cudaFree(e->d_levels);
     if (e->h_ctr) cudaFreeHost(e->h_ctr);
     cudaEventDestroy(e->ev0);
@@ -684,18 +688,17 @@ extern "C" int b40c_enactor_set_stream(b40c_enactor_t *e, void *stream) {
     return B40C_SUCCESS;
 }
 
-extern "C" int b40c_enactor_set_policy(b40c_enactor_t *e, int cta_threads, int warp_th, int cta_th, int big_th,
+extern "C" int b40c_enactor_set_policy(b40c_enactor_t *e, int cta_threads, int warp_th, int cta_th,
                                        int cull_flags) {
     clear_error();
     if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
     if (cta_threads && cta_threads != 128 && cta_threads != 256 && cta_threads != 512)
         return set_error(B40C_ERR_INVALID_VALUE, "cta_threads must be 128, 256 or 512");
-    if (warp_th < 0 || cta_th < 0 || big_th < 0 || cull_flags < 0 || cull_flags > 3)
+    if (warp_th < 0 || cta_th < 0 || cull_flags < 0 || cull_flags > 3)
         return set_error(B40C_ERR_INVALID_VALUE, "invalid policy field");
     if (cta_threads) e->threads = cta_threads;
     if (warp_th) e->warp_th = warp_th;
     if (cta_th) e->cta_th = cta_th;
-    if (big_th) e->big_th = big_th;
     e->cull_flags = unsigned(cull_flags);
     return B40C_SUCCESS;
 }
@@ -720,11 +723,11 @@ extern "C" int b40c_enactor_level_log(b40c_enactor_t *e, int max_records, int64_
     std::vector<LevelRecord> h(LEVEL_LOG_CAP);
     CUDA_TRY(cudaMemcpy(h.data(), e->d_levels, sizeof(LevelRecord) * LEVEL_LOG_CAP, cudaMemcpyDeviceToHost),
              "level log copy");
-    // Records run up to the end-of-search marker (frontier 0).
+    // Records run up to the end-of-search marker (no frontier, no chunks).
     int n = 0;
     while (n < LEVEL_LOG_CAP && h[n].t_start != 0) {
         n++;
-        if (h[n - 1].frontier == 0u) break;
+        if (h[n - 1].frontier == 0u && h[n - 1].chunks == 0u) break;
     }
     n = std::min(n, max_records);
     for (int i = 0; i < n; i++) {

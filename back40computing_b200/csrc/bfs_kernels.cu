@@ -9,23 +9,29 @@
 // 416-516, enactor_two_phase.cuh:465-598), which keeps the level loop on the
 // device instead of polling a host-mapped "done" word.
 //
-// Neighbour-list gather follows the reference's split by list length
-// (two_phase/expand_atomic/cta.cuh:215-423): lists >= cta_th are streamed by the
-// whole CTA, lists >= warp_th by one warp, and shorter lists are packed into a
-// shared-memory gather-offset scratch by a block-wide prefix sum and read by the
-// CTA together.  A fourth tier takes lists >= big_th: they are cut into
-// fixed-size chunks (one 16-byte load per thread of a CTA) that every CTA of
-// the grid takes in turn after the tile phase, so a hub vertex never
-// serialises a level behind one CTA.  Tiles shrink when the frontier is small
-// so that every CTA gets work.  CTA and warp lists are read with 16-byte loads
-// carrying an L2 evict_first policy, one pass ahead of use.
+// Work is organised by warps; no level body waits on a CTA-wide barrier.
+// Neighbour lists are gathered by the reference's strategies chosen by list
+// length (two_phase/expand_atomic/cta.cuh:215-423):
+//   * lists >= cta_th are cut, when their vertex is discovered, into chunks of
+//     16 * THREADS edges for the NEXT level; there every CTA of the grid takes
+//     chunks in turn and streams each with all its threads (CTA-based gather,
+//     spread over the grid so a hub never serialises a level);
+//   * lists >= warp_th are streamed by one warp (warp-based gather);
+//   * shorter lists are packed by a warp prefix sum into a per-warp shared
+//     memory window of gather offsets that the warp reads together
+//     (scan-based gather).
+// CTA and warp gathers use 16-byte loads of column indices with an L2
+// evict_first policy, issued one pass ahead of use.  Contract-expand and
+// two-phase contract the chunks straight from the column array instead of
+// copying hub lists through the edge-frontier queue.
 //
 // Culling: the visited bitmask is the authority and is updated with atomicOr
 // (exact), so each vertex is labelled and expanded once.  Each thread tests 4
 // elements at a time: 4 mask loads in flight, then at most 4 atomicOr, then one
-// warp-aggregated queue reservation.  Optional warp-level (__match_any_sync)
-// and per-CTA history-hash culls drop repeats first (contract_atomic/cta.cuh:
-// 276-327).
+// warp-aggregated queue reservation (the reference reserves with one atomic
+// per CTA tile, util/scan/cooperative_scan.cuh:173-195).  Optional warp-level
+// (__match_any_sync) and per-CTA history-hash culls drop repeats first
+// (two_phase/contract_atomic/cta.cuh:276-327).
 
 #include <cuda_runtime.h>
 
@@ -37,22 +43,24 @@ namespace b40c_b200 {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int HIST_SIZE = 1024;  // history-hash entries per CTA
-constexpr unsigned NO_SPACE = 0xffffffffu;
+constexpr int WINDOW = 128;      // per-warp scan-gather window (4 per lane)
+
+// Resident CTAs per SM requested from ptxas: 40 warps per SM (48 registers
+// per thread); the kernels are bound by memory latency, so resident warps
+// matter more than registers.
+#define MIN_BLOCKS(threads) (1280 / (threads))
+
+template <bool MP>
+struct WarpSmem {
+    int gofs[WINDOW];
+    int gpred[MP ? WINDOW : 1];
+    int surv[WINDOW];
+};
 
 template <int THREADS, bool MP>
 struct Smem {
-    static constexpr int SCRATCH = THREADS * 4;  // gather-offset scratch entries
-    static constexpr int CTILE = THREADS * 4;    // edge-frontier elements per contract tile
-    int2 warp_tot[THREADS / 32 + 1];
-    int gofs[SCRATCH];
-    int gpred[MP ? SCRATCH : 1];
+    WarpSmem<MP> w[THREADS / 32];
     int hist[HIST_SIZE];
-    int surv[CTILE];
-    int owner;
-    int c_start, c_len, c_pred;
-    unsigned c_out;
-    unsigned tile;
-    unsigned out_base;
     unsigned flag;
 };
 
@@ -141,49 +149,34 @@ __device__ __forceinline__ void enqueue4(unsigned flags, const int (&u)[4], int 
     }
 }
 
-// ---------------------------------------------------------------------------------------
-// Sinks: what happens to each gathered neighbour.  Called by every lane of a
-// warp together with up to 4 elements per lane; bit j of valid marks u[j];
-// output positions are out0 + j.
-// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void row_range(const BfsParams &p, int v, int &start, int &len) {
+    start = __ldg(p.row_offsets + v);
+    len = __ldg(p.row_offsets + v + 1) - start;
+}
 
-// Expand-contract: mark and label each neighbour at discovery (label it+1,
-// expand_contract_atomic/cta.cuh:181-218), enqueue the discovered ones.
-template <int THREADS, bool MP>
-struct DiscoverSink {
-    const BfsParams &p;
-    Smem<THREADS, MP> &sm;
-    int *q_out;
-    unsigned *qlen_out;
-    int label;
-
-    __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
-                                               unsigned) const {
-        unsigned disc = cull4<THREADS, MP>(p, sm, valid, u);
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-            if ((disc >> j) & 1u) p.labels[u[j]] = MP ? pred[j] : label;
-        enqueue4(disc, u, q_out, qlen_out, p.qcap, &p.ctr->error);
-    }
-};
-
-// Contract-expand / two-phase expand: neighbours are written at positions
-// reserved beforehand by a block-wide scan (edge frontier, duplicates kept).
-template <bool MP>
-struct PositionSink {
-    int *q_out;
-    int *pq_out;
-    __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
-                                               unsigned out0) const {
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if ((valid >> j) & 1u) {
-                q_out[out0 + j] = u[j];
-                if (MP) pq_out[out0 + j] = pred[j];
-            }
+// Cuts list [start, start+len) of vertex pred into chunks of CH edges aligned
+// to CH-element windows from the 4-aligned start, appended to table.  Returns
+// false when the table is full; the entries it reserved are then written empty
+// and the caller gathers the list another way.  Called by one thread.
+template <int THREADS>
+__device__ __forceinline__ bool push_chunks(const BfsParams &p, int4 *table, unsigned *count, int start, int len,
+                                            int pred) {
+    constexpr int CH = chunk_edges<THREADS>();
+    const int a0 = start & ~3, end = start + len;
+    const unsigned nch = unsigned((end - a0 + CH - 1) / CH);
+    const unsigned base = atomicAdd(count, nch);
+    const unsigned cap = (unsigned)p.chunk_cap;
+    if (base + nch <= cap) {
+        for (unsigned c = 0; c < nch; c++) {
+            const int ws = a0 + int(c) * CH;
+            const int cs = max(ws, start), ce = min(ws + CH, end);
+            table[base + c] = make_int4(cs, ce - cs, pred, 0);
         }
+        return true;
     }
-};
+    for (unsigned c = base; c < cap && c < base + nch; c++) table[c] = make_int4(0, 0, 0, 0);
+    return false;
+}
 
 // ---------------------------------------------------------------------------------------
 // Gather strategies
@@ -205,17 +198,18 @@ __device__ __forceinline__ int4 load_col4(const int *col, int vec_end, int e, in
 }
 
 // The calling group (CTA of THREADS, or one warp with GROUP = 32) streams the
-// list [s, s+l) with 16-byte loads starting from the 4-aligned index a0 <= s;
+// list [s, s+l) with 16-byte loads starting from the 4-aligned index s & ~3;
 // each pass covers GROUP*4 elements; the next pass's load is issued before the
 // current elements are processed.  Elements outside [s, s+l) are masked off.
+// No group-wide barrier: every warp of the group proceeds on its own.
 template <int GROUP, class Sink>
-__device__ __forceinline__ void gather_list(const int *col, int vec_end, int a0, int s, int l, int pred,
-                                            unsigned out, int rank, const Sink &sink, uint64_t pol) {
+__device__ __forceinline__ void gather_list(const int *col, int vec_end, int s, int l, int pred, unsigned out,
+                                            int rank, const Sink &sink, uint64_t pol) {
     const int end = s + l;
-    int e = a0 + rank * 4;
+    int e = (s & ~3) + rank * 4;
     int4 cur = load_col4(col, vec_end, e, end, pol);
     const int pv[4] = {pred, pred, pred, pred};
-    for (int base = a0; base < end; base += GROUP * 4) {
+    for (int base = s & ~3; base < end; base += GROUP * 4) {
         const int en = e + GROUP * 4;
         int4 nxt = load_col4(col, vec_end, en, end, pol);
         unsigned valid = 0;
@@ -229,35 +223,55 @@ __device__ __forceinline__ void gather_list(const int *col, int vec_end, int a0,
     }
 }
 
-// CTA-, warp- and scan-based gather of the lists held by the CTA's threads
-// (one list per thread: start, len, owner vertex pred, output position out).
-// small_off / small_total: block exclusive scan of the lengths of lists shorter
-// than warp_th, whose outputs are contiguous from small_base.
-template <int THREADS, bool MP, class Sink>
-__device__ __forceinline__ void expand_lists(const BfsParams &p, Smem<THREADS, MP> &sm, const Sink &sink,
-                                             uint64_t pol, int start, int len, int pred, unsigned out,
-                                             int small_off, int small_total, unsigned small_base) {
-    const bool small = len < p.warp_th;
-    // (1) whole-CTA gather of lists >= cta_th, one list at a time
-    for (;;) {
-        if (threadIdx.x == 0) sm.owner = -1;
-        __syncthreads();
-        if (len >= p.cta_th) sm.owner = threadIdx.x;
-        __syncthreads();
-        const int owner = sm.owner;
-        if (owner < 0) break;
-        if (owner == (int)threadIdx.x) {
-            sm.c_start = start;
-            sm.c_len = len;
-            sm.c_pred = pred;
-            sm.c_out = out;
-            len = 0;
-        }
-        __syncthreads();
-        const int s = sm.c_start;
-        gather_list<THREADS>(p.col, p.vec_end, s & ~3, s, sm.c_len, sm.c_pred, sm.c_out, threadIdx.x, sink, pol);
+// Grid-wide chunk phase: CTA b streams chunks b, b + G, b + 2G, ... of table.
+template <int THREADS, class Sink>
+__device__ __forceinline__ void gather_chunks(const BfsParams &p, const int4 *table, unsigned n, const Sink &sink,
+                                              uint64_t pol) {
+    if (n > (unsigned)p.chunk_cap) n = p.chunk_cap;
+    const unsigned G = gridDim.x;
+    unsigned k = blockIdx.x;
+    int4 cur = k < n ? __ldcg(table + k) : make_int4(0, 0, 0, 0);
+    for (; k < n; k += G) {
+        int4 nxt = (k + G < n) ? __ldcg(table + k + G) : make_int4(0, 0, 0, 0);
+        if (cur.y > 0) gather_list<THREADS>(p.col, p.vec_end, cur.x, cur.y, cur.z, 0u, threadIdx.x, sink, pol);
+        cur = nxt;
     }
-    // (2) warp gather of lists >= warp_th
+}
+
+// Warp- and scan-based gather of one list per lane (start, len, owner pred).
+// With POSITIONAL the warp first reserves room for all its lists in the output
+// queue with one atomicAdd on qlen_out (short lists first, then the others) and
+// the sink receives each element's position.
+template <bool MP, bool POSITIONAL, class Sink>
+__device__ __forceinline__ void warp_lists(const BfsParams &p, WarpSmem<MP> &ws, const Sink &sink, uint64_t pol,
+                                           int start, int len, int pred, unsigned *qlen_out) {
+    const int lane = lane_id();
+    const bool small = len < p.warp_th;
+    const int sl = small ? len : 0;
+    const int si = warp_inclusive_scan(sl);
+    const int small_total = __shfl_sync(FULL, si, 31);
+    const int small_excl = si - sl;
+    unsigned out = 0, small_base = 0;
+    if (POSITIONAL) {
+        const int ml = small ? 0 : len;
+        const int mi = warp_inclusive_scan(ml);
+        const unsigned need = unsigned(small_total) + unsigned(__shfl_sync(FULL, mi, 31));
+        unsigned base = 0;
+        if (need) {
+            if (lane == 0) {
+                base = atomicAdd(qlen_out, need);
+                if ((unsigned long long)base + need > (unsigned long long)p.qcap) {
+                    atomicOr(&p.ctr->error, ERR_OVERFLOW);
+                    base = 0xffffffffu;
+                }
+            }
+            base = __shfl_sync(FULL, base, 0);
+            if (base == 0xffffffffu) return;  // warp-uniform: output dropped on overflow
+        }
+        small_base = base;
+        out = small ? base + unsigned(small_excl) : base + unsigned(small_total) + unsigned(mi - ml);
+    }
+    // warp-based gather of lists >= warp_th
     unsigned wm;
     while ((wm = __ballot_sync(FULL, len >= p.warp_th)) != 0u) {
         const int leader = __ffs(wm) - 1;
@@ -265,21 +279,19 @@ __device__ __forceinline__ void expand_lists(const BfsParams &p, Smem<THREADS, M
         const int l = __shfl_sync(FULL, len, leader);
         const int pv = __shfl_sync(FULL, pred, leader);
         const unsigned o = __shfl_sync(FULL, out, leader);
-        if ((int)lane_id() == leader) len = 0;
-        gather_list<32>(p.col, p.vec_end, s & ~3, s, l, pv, o, lane_id(), sink, pol);
+        if (lane == leader) len = 0;
+        gather_list<32>(p.col, p.vec_end, s, l, pv, o, lane, sink, pol);
     }
-    // (3) scan-based gather of the short lists through shared memory
-    constexpr int SCRATCH = Smem<THREADS, MP>::SCRATCH;
-    const int my_len = small ? len : 0;
-    for (int round = 0; round < small_total; round += SCRATCH) {
-        const int lo = max(small_off, round), hi = min(small_off + my_len, round + SCRATCH);
+    // scan-based gather of the short lists through the warp's window
+    for (int base = 0; base < small_total; base += WINDOW) {
+        const int lo = max(small_excl, base), hi = min(small_excl + sl, base + WINDOW);
         for (int j = lo; j < hi; j++) {
-            sm.gofs[j - round] = start + (j - small_off);
-            if (MP) sm.gpred[j - round] = pred;
+            ws.gofs[j - base] = start + (j - small_excl);
+            if (MP) ws.gpred[j - base] = pred;
         }
-        __syncthreads();
-        const int cnt = min(SCRATCH, small_total - round);
-        const int k = threadIdx.x * 4;  // SCRATCH = 4 * THREADS: one pass
+        __syncwarp();
+        const int cnt = min(WINDOW, small_total - base);
+        const int k = lane * 4;
         unsigned valid = 0;
         int u[4], pv[4];
 #pragma unroll
@@ -288,302 +300,272 @@ __device__ __forceinline__ void expand_lists(const BfsParams &p, Smem<THREADS, M
             pv[j] = 0;
             if (k + j < cnt) {
                 valid |= 1u << j;
-                u[j] = __ldg(p.col + sm.gofs[k + j]);
-                if (MP) pv[j] = sm.gpred[k + j];
+                u[j] = __ldg(p.col + ws.gofs[k + j]);
+                if (MP) pv[j] = ws.gpred[k + j];
             }
         }
-        sink(valid, u, pv, small_base + unsigned(round + k));
-        __syncthreads();
+        sink(valid, u, pv, small_base + unsigned(base + k));
+        __syncwarp();
     }
 }
 
-// Cuts list [start, start+len) into grid-wide chunks aligned to CHUNK-element
-// windows from the 4-aligned start.  Returns false when the chunk table is
-// full; the entries it reserved are then written empty and the caller's CTA
-// gathers the list itself.
-template <int THREADS>
-__device__ __forceinline__ bool push_chunks(const BfsParams &p, unsigned *chunk_count, int start, int len, int pred,
-                                            unsigned out) {
-    constexpr int CH = chunk_edges<THREADS>();
-    const int a0 = start & ~3, end = start + len;
-    const unsigned nch = unsigned((end - a0 + CH - 1) / CH);
-    const unsigned base = atomicAdd(chunk_count, nch);
-    const unsigned cap = (unsigned)p.chunk_cap;
-    if (base + nch <= cap) {
-        for (unsigned c = 0; c < nch; c++) {
-            const int ws = a0 + int(c) * CH;
-            const int cs = max(ws, start), ce = min(ws + CH, end);
-            p.chunks[base + c] = make_int4(cs, ce - cs, pred, int(out + unsigned(cs - start)));
+__device__ __forceinline__ unsigned warp_next_tile(unsigned *steal) {
+    unsigned t = 0;
+    if (lane_id() == 0) t = atomicAdd(steal, 1u);
+    return __shfl_sync(FULL, t, 0);
+}
+
+// ---------------------------------------------------------------------------------------
+// Sinks: what happens to each gathered element.  Called by every lane of a
+// warp together with up to 4 elements per lane; bit j of valid marks u[j];
+// output positions (edge-frontier queues) are out0 + j.
+// ---------------------------------------------------------------------------------------
+
+// Expand-contract: mark and label each neighbour at discovery (label it+1,
+// expand_contract_atomic/cta.cuh:181-218).  A discovered vertex whose list is
+// >= cta_th becomes chunks of the next level; the others go to the next
+// vertex frontier.
+template <int THREADS, bool MP>
+struct DiscoverSink {
+    const BfsParams &p;
+    Smem<THREADS, MP> &sm;
+    int *q_out;
+    unsigned *qlen_out;
+    int4 *chunk_out;
+    unsigned *chunk_count;
+    int label;
+
+    __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
+                                               unsigned) const {
+        const unsigned disc = cull4<THREADS, MP>(p, sm, valid, u);
+        int st[4], ln[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            st[j] = 0;
+            ln[j] = 0;
+            if ((disc >> j) & 1u) {
+                p.labels[u[j]] = MP ? pred[j] : label;
+                row_range(p, u[j], st[j], ln[j]);
+            }
         }
-        return true;
+        unsigned enq = disc;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (((disc >> j) & 1u) && ln[j] >= p.cta_th &&
+                push_chunks<THREADS>(p, chunk_out, chunk_count, st[j], ln[j], u[j]))
+                enq &= ~(1u << j);
+        enqueue4(enq, u, q_out, qlen_out, p.qcap, &p.ctr->error);
     }
-    for (unsigned c = base; c < cap && c < base + nch; c++) p.chunks[c] = make_int4(0, 0, 0, 0);
-    return false;
-}
+};
 
-// Grid-wide phase: CTA b gathers chunks b, b + G, b + 2G, ...
-template <int THREADS, class Sink>
-__device__ __forceinline__ void gather_chunks(const BfsParams &p, unsigned n, const Sink &sink, uint64_t pol) {
-    if (n > (unsigned)p.chunk_cap) n = p.chunk_cap;
-    const unsigned G = gridDim.x;
-    unsigned k = blockIdx.x;
-    int4 cur = k < n ? __ldcg(p.chunks + k) : make_int4(0, 0, 0, 0);
-    for (; k < n; k += G) {
-        int4 nxt = (k + G < n) ? __ldcg(p.chunks + k + G) : make_int4(0, 0, 0, 0);
-        if (cur.y > 0)
-            gather_list<THREADS>(p.col, p.vec_end, cur.x & ~3, cur.x, cur.y, cur.z, unsigned(cur.w), threadIdx.x,
-                                 sink, pol);
-        cur = nxt;
+// Edge-frontier output (contract-expand / two-phase expand): neighbours are
+// written at reserved positions, duplicates kept.
+template <bool MP>
+struct PositionSink {
+    int *q_out;
+    int *pq_out;
+    __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
+                                               unsigned out0) const {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if ((valid >> j) & 1u) {
+                q_out[out0 + j] = u[j];
+                if (MP) pq_out[out0 + j] = pred[j];
+            }
+        }
     }
-}
+};
 
-// Hands out tiles of the input frontier to CTAs with one atomic each.
+// Contract-expand: cull and label the edge-frontier elements (label it,
+// contract_expand_atomic/cta.cuh:264-304), then expand the survivors at once:
+// lists >= cta_th become chunks of the next level, the rest are copied into
+// the next edge frontier by warp- and scan-based gathers.
 template <int THREADS, bool MP>
-__device__ __forceinline__ unsigned next_tile(unsigned *steal, Smem<THREADS, MP> &sm) {
-    __syncthreads();
-    if (threadIdx.x == 0) sm.tile = atomicAdd(steal, 1u);
-    __syncthreads();
-    return sm.tile;
-}
+struct ContractExpandSink {
+    const BfsParams &p;
+    Smem<THREADS, MP> &sm;
+    int it;
+    uint64_t pol;
 
-// Tile size for a frontier of L elements: at most `most`, small enough that
-// there are about two tiles per CTA when the frontier is short.
-__device__ __forceinline__ unsigned tile_size(unsigned L, unsigned most) {
-    const unsigned G2 = 2u * gridDim.x;
-    unsigned t = (L + G2 - 1) / G2;
-    return t < 1u ? 1u : (t > most ? most : t);
-}
+    __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
+                                               unsigned) const {
+        const unsigned surv = cull4<THREADS, MP>(p, sm, valid, u);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if ((surv >> j) & 1u) p.labels[u[j]] = MP ? pred[j] : it;
+        // Compact the warp's survivors into its window.
+        WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
+        const unsigned lt = lanemask_lt();
+        unsigned total = 0, pre[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            unsigned b = __ballot_sync(FULL, (surv >> j) & 1u);
+            pre[j] = total + __popc(b & lt);
+            total += __popc(b);
+        }
+        if (total == 0u) return;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if ((surv >> j) & 1u) ws.surv[pre[j]] = u[j];
+        __syncwarp();
+        const int nq = (it + 1) & 1;
+        PositionSink<MP> out{p.queue[nq], p.pred_queue[nq]};
+        for (unsigned g = 0; g < total; g += 32) {
+            int v = -1, start = 0, len = 0;
+            if (g + lane_id() < total) {
+                v = ws.surv[g + lane_id()];
+                row_range(p, v, start, len);
+                if (len >= p.cta_th && push_chunks<THREADS>(p, p.chunks[nq], &p.ctr->big[(it + 1) & 3], start, len, v))
+                    len = 0;
+            }
+            warp_lists<MP, true>(p, ws, out, pol, start, len, v, &p.ctr->qlen[(it + 1) & 3]);
+        }
+        __syncwarp();
+    }
+};
 
-__device__ __forceinline__ void row_range(const BfsParams &p, int v, int &start, int &len) {
-    start = __ldg(p.row_offsets + v);
-    len = __ldg(p.row_offsets + v + 1) - start;
-}
+// Two-phase contract: cull and label (iteration it), then append the survivors
+// to the vertex frontier (two_phase/contract_atomic/cta.cuh:494-572).
+template <int THREADS, bool MP>
+struct ContractSink {
+    const BfsParams &p;
+    Smem<THREADS, MP> &sm;
+    int *q_out;
+    unsigned *qlen_out;
+    int it;
+
+    __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
+                                               unsigned) const {
+        const unsigned surv = cull4<THREADS, MP>(p, sm, valid, u);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if ((surv >> j) & 1u) p.labels[u[j]] = MP ? pred[j] : it;
+        enqueue4(surv, u, q_out, qlen_out, p.qcap, &p.ctr->error);
+    }
+};
 
 // ---------------------------------------------------------------------------------------
-// Level bodies
+// Phase bodies.  Phase q reads queue[q&1] (qlen[q&3] entries) and chunks[q&1]
+// (big[q&3] entries) and writes queue[(q+1)&1] / chunks[(q+1)&1].
 // ---------------------------------------------------------------------------------------
 
-// Expand-contract tile phase of level `it`: vertex frontier queue[it&1] ->
-// discovered vertices in queue[(it+1)&1]; lists >= big_th become chunks counted
-// in big[it&3].
+__device__ __forceinline__ int global_warp() { return int(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)); }
+__device__ __forceinline__ int grid_warps() { return int(gridDim.x * (blockDim.x >> 5)); }
+
+// Expand-contract level it: vertex frontier -> discovered vertices labelled it+1.
 template <int THREADS, bool MP>
-__device__ void ec_level(const BfsParams &p, int it, unsigned L, Smem<THREADS, MP> &sm, uint64_t pol) {
+__device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, Smem<THREADS, MP> &sm, uint64_t pol) {
     Counters *c = p.ctr;
+    const int nq = (it + 1) & 1;
+    DiscoverSink<THREADS, MP> sink{p, sm, p.queue[nq], &c->qlen[(it + 1) & 3], p.chunks[nq], &c->big[(it + 1) & 3],
+                                   it + 1};
+    gather_chunks<THREADS>(p, p.chunks[it & 1], nch, sink, pol);
+    WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
     const int *q_in = p.queue[it & 1];
-    DiscoverSink<THREADS, MP> sink{p, sm, p.queue[(it + 1) & 1], &c->qlen[(it + 1) & 3], it + 1};
-    const unsigned tv = tile_size(L, THREADS);
-    const unsigned ntiles = (L + tv - 1) / tv;
+    const unsigned ntiles = (L + 31) / 32;
     for (;;) {
-        const unsigned tile = next_tile<THREADS, MP>(&c->steal[it & 3], sm);
-        if (tile >= ntiles) break;
-        const unsigned idx = tile * tv + threadIdx.x;
+        const unsigned t = warp_next_tile(&c->steal[it & 3]);
+        if (t >= ntiles) break;
+        const unsigned idx = t * 32 + lane_id();
         int v = -1, start = 0, len = 0;
-        if (threadIdx.x < tv && idx < L) {
+        if (idx < L) {
             v = ld_cg(q_in + idx);
             row_range(p, v, start, len);
-            if (len >= p.big_th && push_chunks<THREADS>(p, &c->big[it & 3], start, len, v, 0u)) len = 0;
         }
-        int small_total;
-        const int small_off = block_exclusive_scan<THREADS>(len < p.warp_th ? len : 0, small_total, sm.warp_tot);
-        expand_lists<THREADS, MP>(p, sm, sink, pol, start, len, v, 0u, small_off, small_total, 0u);
+        warp_lists<MP, false>(p, ws, sink, pol, start, len, v, nullptr);
     }
 }
 
-template <int THREADS, bool MP>
-__device__ void ec_chunks(const BfsParams &p, int it, unsigned n, Smem<THREADS, MP> &sm, uint64_t pol) {
-    DiscoverSink<THREADS, MP> sink{p, sm, p.queue[(it + 1) & 1], &p.ctr->qlen[(it + 1) & 3], it + 1};
-    gather_chunks<THREADS>(p, n, sink, pol);
-}
-
-// Expands one list per thread into the edge-frontier queue q_out: a
-// two-component block scan sizes the short and the long lists, thread 0
-// reserves the tile's output with one atomicAdd (ScanTileWithEnqueue,
-// util/scan/cooperative_scan.cuh:173-195), lists >= big_th become chunks with
-// their reserved output positions.
-template <int THREADS, bool MP>
-__device__ __forceinline__ void expand_tile_to_edges(const BfsParams &p, Smem<THREADS, MP> &sm, uint64_t pol,
-                                                     int start, int len, int pred, int *q_out, int *pq_out,
-                                                     unsigned *qlen_out, unsigned *chunk_count) {
-    const bool small = len < p.warp_th;
-    int2 total;
-    const int2 off =
-        block_exclusive_scan2<THREADS>(make_int2(small ? len : 0, small ? 0 : len), total, sm.warp_tot);
-    if (threadIdx.x == 0) {
-        const unsigned need = unsigned(total.x + total.y);
-        unsigned base = 0;
-        if (need) {
-            base = atomicAdd(qlen_out, need);
-            if ((unsigned long long)base + need > (unsigned long long)p.qcap) {
-                atomicOr(&p.ctr->error, ERR_OVERFLOW);
-                base = NO_SPACE;
-            }
-        }
-        sm.out_base = base;
-    }
-    __syncthreads();
-    const unsigned base = sm.out_base;
-    if (base == NO_SPACE) return;  // uniform: the tile's output is dropped on overflow
-    const unsigned out = small ? base + off.x : base + unsigned(total.x) + off.y;
-    if (len >= p.big_th && push_chunks<THREADS>(p, chunk_count, start, len, pred, out)) len = 0;
-    PositionSink<MP> sink{q_out, pq_out};
-    expand_lists<THREADS, MP>(p, sm, sink, pol, start, len, pred, out, off.x, total.x, base);
-}
-
-// Loads up to 4 edge-frontier elements of tile `tile` (tile size te) per
-// thread, strided by THREADS, and culls them.  Returns the survivors' bits.
-template <int THREADS, bool MP>
-__device__ __forceinline__ unsigned contract_tile_load(const BfsParams &p, Smem<THREADS, MP> &sm, const int *q_in,
-                                                       const int *pq_in, unsigned L, unsigned tile, unsigned te,
-                                                       int (&u)[4], int (&pr)[4]) {
-    unsigned valid = 0;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        const unsigned r = j * THREADS + threadIdx.x;
-        const unsigned idx = tile * te + r;
-        u[j] = -1;
-        pr[j] = 0;
-        if (r < te && idx < L) {
-            valid |= 1u << j;
-            u[j] = ld_cg(q_in + idx);
-            if (MP) pr[j] = ld_cg(pq_in + idx);
-        }
-    }
-    return cull4<THREADS, MP>(p, sm, valid, u);
-}
-
-// Contract-expand level `it` (contract_expand_atomic/cta.cuh:573-709): edge
-// frontier queue[it&1] -> cull, label it -> survivors compacted in shared
-// memory -> expanded into queue[(it+1)&1].
-template <int THREADS, bool MP>
-__device__ void ce_level(const BfsParams &p, int it, unsigned L, Smem<THREADS, MP> &sm, uint64_t pol) {
-    Counters *c = p.ctr;
-    const int *q_in = p.queue[it & 1];
-    const int *pq_in = p.pred_queue[it & 1];
-    const unsigned te = tile_size(L, Smem<THREADS, MP>::CTILE);
-    const unsigned ntiles = (L + te - 1) / te;
-    for (;;) {
-        const unsigned tile = next_tile<THREADS, MP>(&c->steal[it & 3], sm);
-        if (tile >= ntiles) break;
+// Edge-frontier phase input: warp tiles of 128 elements (4 per lane,
+// coalesced), statically interleaved over the grid's warps.
+template <bool MP, class Sink>
+__device__ __forceinline__ void edge_tiles(const int *q_in, const int *pq_in, unsigned L, const Sink &sink) {
+    const unsigned ntiles = (L + WINDOW - 1) / WINDOW;
+    const unsigned W = grid_warps();
+    for (unsigned t = global_warp(); t < ntiles; t += W) {
+        unsigned valid = 0;
         int u[4], pr[4];
-        const unsigned surv = contract_tile_load<THREADS, MP>(p, sm, q_in, pq_in, L, tile, te, u, pr);
 #pragma unroll
-        for (int j = 0; j < 4; j++)
-            if ((surv >> j) & 1u) p.labels[u[j]] = MP ? pr[j] : it;
-        int nsurv;
-        int off = block_exclusive_scan<THREADS>(__popc(surv), nsurv, sm.warp_tot);
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-            if ((surv >> j) & 1u) sm.surv[off++] = u[j];
-        __syncthreads();
-        for (int r0 = 0; r0 < nsurv; r0 += THREADS) {
-            int v = -1, start = 0, len = 0;
-            if (r0 + (int)threadIdx.x < nsurv) {
-                v = sm.surv[r0 + threadIdx.x];
-                row_range(p, v, start, len);
+        for (int j = 0; j < 4; j++) {
+            const unsigned idx = t * WINDOW + j * 32 + lane_id();
+            u[j] = -1;
+            pr[j] = 0;
+            if (idx < L) {
+                valid |= 1u << j;
+                u[j] = ld_cg(q_in + idx);
+                if (MP) pr[j] = ld_cg(pq_in + idx);
             }
-            expand_tile_to_edges<THREADS, MP>(p, sm, pol, start, len, v, p.queue[(it + 1) & 1],
-                                              p.pred_queue[(it + 1) & 1], &c->qlen[(it + 1) & 3], &c->big[it & 3]);
         }
+        sink(valid, u, pr, 0u);
     }
 }
 
-// Chunk phase after a level that wrote an edge frontier to queue[out_sel].
+// Contract-expand level it (contract_expand_atomic/cta.cuh:573-709).
 template <int THREADS, bool MP>
-__device__ void edge_chunks(const BfsParams &p, int out_sel, unsigned n, uint64_t pol) {
-    PositionSink<MP> sink{p.queue[out_sel], p.pred_queue[out_sel]};
-    gather_chunks<THREADS>(p, n, sink, pol);
+__device__ void ce_level(const BfsParams &p, int it, unsigned L, unsigned nch, Smem<THREADS, MP> &sm, uint64_t pol) {
+    ContractExpandSink<THREADS, MP> sink{p, sm, it, pol};
+    gather_chunks<THREADS>(p, p.chunks[it & 1], nch, sink, pol);
+    edge_tiles<MP>(p.queue[it & 1], p.pred_queue[it & 1], L, sink);
 }
 
-// Two-phase contract (two_phase/contract_atomic/cta.cuh:494-572): edge frontier
-// queue[qi&1] -> cull, label `it` -> compacted vertex frontier queue[(qi+1)&1],
-// allocated by a block scan and one atomicAdd per tile.
+// Two-phase contract, phase qi = 2 * it.
 template <int THREADS, bool MP>
-__device__ void tp_contract(const BfsParams &p, int it, int qi, unsigned L, Smem<THREADS, MP> &sm) {
-    Counters *c = p.ctr;
-    const int *q_in = p.queue[qi & 1];
-    const int *pq_in = p.pred_queue[qi & 1];
-    int *q_out = p.queue[(qi + 1) & 1];
-    const unsigned te = tile_size(L, Smem<THREADS, MP>::CTILE);
-    const unsigned ntiles = (L + te - 1) / te;
-    for (;;) {
-        const unsigned tile = next_tile<THREADS, MP>(&c->steal[qi & 3], sm);
-        if (tile >= ntiles) break;
-        int u[4], pr[4];
-        const unsigned surv = contract_tile_load<THREADS, MP>(p, sm, q_in, pq_in, L, tile, te, u, pr);
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-            if ((surv >> j) & 1u) p.labels[u[j]] = MP ? pr[j] : it;
-        int total;
-        int off = block_exclusive_scan<THREADS>(__popc(surv), total, sm.warp_tot);
-        if (threadIdx.x == 0) {
-            unsigned base = total ? atomicAdd(&c->qlen[(qi + 1) & 3], (unsigned)total) : 0u;
-            if ((unsigned long long)base + total > (unsigned long long)p.qcap) {
-                atomicOr(&c->error, ERR_OVERFLOW);
-                base = NO_SPACE;
-            }
-            sm.out_base = base;
-        }
-        __syncthreads();
-        const unsigned base = sm.out_base;
-        if (base != NO_SPACE) {
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if ((surv >> j) & 1u) q_out[base + off++] = u[j];
-        }
-    }
+__device__ void tp_contract(const BfsParams &p, int it, int qi, unsigned L, unsigned nch, Smem<THREADS, MP> &sm,
+                            uint64_t pol) {
+    ContractSink<THREADS, MP> sink{p, sm, p.queue[(qi + 1) & 1], &p.ctr->qlen[(qi + 1) & 3], it};
+    gather_chunks<THREADS>(p, p.chunks[qi & 1], nch, sink, pol);
+    edge_tiles<MP>(p.queue[qi & 1], p.pred_queue[qi & 1], L, sink);
 }
 
-// Two-phase expand (two_phase/expand_atomic/cta.cuh:606-719): vertex frontier
-// queue[qi&1] -> edge frontier queue[(qi+1)&1] with predecessors.
+// Two-phase expand, phase qi = 2 * it + 1 (two_phase/expand_atomic/cta.cuh:606-719).
 template <int THREADS, bool MP>
 __device__ void tp_expand(const BfsParams &p, int qi, unsigned L, Smem<THREADS, MP> &sm, uint64_t pol) {
     Counters *c = p.ctr;
+    const int nq = (qi + 1) & 1;
+    PositionSink<MP> out{p.queue[nq], p.pred_queue[nq]};
+    WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
     const int *q_in = p.queue[qi & 1];
-    const unsigned tv = tile_size(L, THREADS);
-    const unsigned ntiles = (L + tv - 1) / tv;
+    const unsigned ntiles = (L + 31) / 32;
     for (;;) {
-        const unsigned tile = next_tile<THREADS, MP>(&c->steal[qi & 3], sm);
-        if (tile >= ntiles) break;
-        const unsigned idx = tile * tv + threadIdx.x;
+        const unsigned t = warp_next_tile(&c->steal[qi & 3]);
+        if (t >= ntiles) break;
+        const unsigned idx = t * 32 + lane_id();
         int v = -1, start = 0, len = 0;
-        if (threadIdx.x < tv && idx < L) {
+        if (idx < L) {
             v = ld_cg(q_in + idx);
             row_range(p, v, start, len);
+            if (len >= p.cta_th && push_chunks<THREADS>(p, p.chunks[nq], &c->big[(qi + 1) & 3], start, len, v))
+                len = 0;
         }
-        expand_tile_to_edges<THREADS, MP>(p, sm, pol, start, len, v, p.queue[(qi + 1) & 1],
-                                          p.pred_queue[(qi + 1) & 1], &c->qlen[(qi + 1) & 3], &c->big[qi & 3]);
+        warp_lists<MP, true>(p, ws, out, pol, start, len, v, &c->qlen[(qi + 1) & 3]);
     }
 }
 
-// Ring housekeeping for phase index q: entries that phase q+1 will use start
-// from zero.  Done by one thread while no CTA touches them.
+// Ring housekeeping for phase q: the entries phase q+1 writes start at zero.
+// Done by one thread while no CTA touches them.
 __device__ __forceinline__ void ring_prepare(Counters *c, int q) {
     c->qlen[(q + 2) & 3] = 0u;
+    c->big[(q + 2) & 3] = 0u;
     c->steal[(q + 1) & 3] = 0u;
-    c->big[(q + 1) & 3] = 0u;
 }
 
-__device__ __forceinline__ void log_level_start(const BfsParams &p, int idx, unsigned frontier) {
+__device__ __forceinline__ void log_phase(const BfsParams &p, int idx, unsigned frontier, unsigned chunks) {
     if (p.levels && idx < p.level_cap) {
         LevelRecord r;
         r.t_start = globaltimer_ns();
         r.t_tiles = 0;
         r.frontier = frontier;
-        r.chunks = 0;
+        r.chunks = chunks;
         p.levels[idx] = r;
-    }
-}
-__device__ __forceinline__ void log_level_tiles(const BfsParams &p, int idx, unsigned chunks) {
-    if (p.levels && idx < p.level_cap) {
-        p.levels[idx].t_tiles = globaltimer_ns();
-        p.levels[idx].chunks = chunks;
     }
 }
 
 template <int THREADS, bool MP>
 __device__ __forceinline__ void init_hist(Smem<THREADS, MP> &sm, unsigned flags) {
-    if (flags & CULL_HISTORY)
+    if (flags & CULL_HISTORY) {
         for (int i = threadIdx.x; i < HIST_SIZE; i += THREADS) sm.hist[i] = -1;
+        __syncthreads();
+    }
 }
 
 __device__ __forceinline__ bool leader() { return blockIdx.x == 0 && threadIdx.x == 0; }
@@ -614,10 +596,10 @@ __global__ void search_init_kernel(BfsParams p, int strategy, int mark_pred) {
     }
 }
 
-// Leaves the loop of a fused kernel (every CTA decides alike: L and the level
-// index are the same everywhere after a barrier).
-__device__ __forceinline__ bool stop_level_loop(const BfsParams &p, int level, unsigned L) {
-    if (L == 0u) return true;
+// Whether a fused kernel's level loop ends (every CTA decides alike: the
+// counters and the level index are the same everywhere after a barrier).
+__device__ __forceinline__ bool stop_level_loop(const BfsParams &p, int level, unsigned work) {
+    if (work == 0u) return true;
     if (level_limit_hit(level, p.nodes)) {
         if (leader()) atomicOr(&p.ctr->error, ERR_LEVEL_LIMIT);
         return true;
@@ -628,62 +610,50 @@ __device__ __forceinline__ bool stop_level_loop(const BfsParams &p, int level, u
 __device__ __forceinline__ void finish_search(const BfsParams &p, int iteration, int log_idx) {
     if (leader()) {
         p.ctr->iteration = iteration;
-        log_level_start(p, log_idx, 0u);  // end-of-search timestamp
+        log_phase(p, log_idx, 0u, 0u);  // end-of-search marker
         atomicOr(&p.ctr->sticky, ld_relaxed_gpu(&p.ctr->error));
     }
 }
 
 template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS) ec_fused_kernel(BfsParams p) {
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(BfsParams p) {
     __shared__ Smem<THREADS, MP> sm;
     init_hist(sm, p.cull_flags);
     const uint64_t pol = policy_evict_first();
     Counters *c = p.ctr;
     int it = 0;
     for (;;) {
-        const unsigned L = ld_cg(&c->qlen[it & 3]);
-        if (stop_level_loop(p, it, L)) break;
+        const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]);
+        if (stop_level_loop(p, it, L + nch)) break;
         if (leader()) {
             ring_prepare(c, it);
             c->total_queued += L;
-            log_level_start(p, it, L);
+            log_phase(p, it, L, nch);
         }
-        ec_level<THREADS, MP>(p, it, L, sm, pol);
+        ec_level<THREADS, MP>(p, it, L, nch, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
-        const unsigned nch = ld_cg(&c->big[it & 3]);
-        if (leader()) log_level_tiles(p, it, nch);
-        if (nch) {
-            ec_chunks<THREADS, MP>(p, it, nch, sm, pol);
-            if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
-        }
         it++;
     }
     finish_search(p, it, it);
 }
 
 template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS) ce_fused_kernel(BfsParams p) {
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(BfsParams p) {
     __shared__ Smem<THREADS, MP> sm;
     init_hist(sm, p.cull_flags);
     const uint64_t pol = policy_evict_first();
     Counters *c = p.ctr;
     int it = 0;
     for (;;) {
-        const unsigned L = ld_cg(&c->qlen[it & 3]);
-        if (stop_level_loop(p, it, L)) break;
+        const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]);
+        if (stop_level_loop(p, it, L + nch)) break;
         if (leader()) {
             ring_prepare(c, it);
             c->total_queued += L;
-            log_level_start(p, it, L);
+            log_phase(p, it, L, nch);
         }
-        ce_level<THREADS, MP>(p, it, L, sm, pol);
+        ce_level<THREADS, MP>(p, it, L, nch, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
-        const unsigned nch = ld_cg(&c->big[it & 3]);
-        if (leader()) log_level_tiles(p, it, nch);
-        if (nch) {
-            edge_chunks<THREADS, MP>(p, (it + 1) & 1, nch, pol);
-            if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
-        }
         it++;
     }
     finish_search(p, it, it);
@@ -694,7 +664,7 @@ __global__ void __launch_bounds__(THREADS) ce_fused_kernel(BfsParams p) {
 // its enactor cannot instantiate, enactor_two_phase.cuh:302).  The level log is
 // indexed by phase (2 * iteration for contract, + 1 for expand).
 template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS) tp_fused_kernel(BfsParams p) {
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(BfsParams p) {
     __shared__ Smem<THREADS, MP> sm;
     init_hist(sm, p.cull_flags);
     const uint64_t pol = policy_evict_first();
@@ -702,29 +672,24 @@ __global__ void __launch_bounds__(THREADS) tp_fused_kernel(BfsParams p) {
     int it = 0, qi = 0;
     for (;;) {
         unsigned L = ld_cg(&c->qlen[qi & 3]);
-        if (stop_level_loop(p, it, L)) break;
+        const unsigned nch = ld_cg(&c->big[qi & 3]);
+        if (stop_level_loop(p, it, L + nch)) break;
         if (leader()) {
             ring_prepare(c, qi);
             c->total_queued += L;
-            log_level_start(p, qi, L);
+            log_phase(p, qi, L, nch);
         }
-        tp_contract<THREADS, MP>(p, it, qi, L, sm);
+        tp_contract<THREADS, MP>(p, it, qi, L, nch, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         qi++;
         L = ld_cg(&c->qlen[qi & 3]);
-        if (L == 0u) break;
+        if (L == 0u) break;  // no vertex discovered: the reference stops without ++
         if (leader()) {
             ring_prepare(c, qi);
-            log_level_start(p, qi, L);
+            log_phase(p, qi, L, 0u);
         }
         tp_expand<THREADS, MP>(p, qi, L, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
-        const unsigned nch = ld_cg(&c->big[qi & 3]);
-        if (leader()) log_level_tiles(p, qi, nch);
-        if (nch) {
-            edge_chunks<THREADS, MP>(p, (qi + 1) & 1, nch, pol);
-            if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
-        }
         qi++;
         it++;
     }
@@ -734,69 +699,47 @@ __global__ void __launch_bounds__(THREADS) tp_fused_kernel(BfsParams p) {
 // ---- per-level kernels for the graph-driven (iterative) variants ----------------
 
 template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS) ec_level_kernel(BfsParams p) {
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_level_kernel(BfsParams p) {
     __shared__ Smem<THREADS, MP> sm;
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it;
-    const unsigned L = p.ctr->qlen[it & 3];
-    if (L == 0u || p.ctr->error) return;
-    if (leader()) log_level_start(p, it, L);
-    ec_level<THREADS, MP>(p, it, L, sm, policy_evict_first());
+    const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3];
+    if (L + nch == 0u || p.ctr->error) return;
+    if (leader()) log_phase(p, it, L, nch);
+    ec_level<THREADS, MP>(p, it, L, nch, sm, policy_evict_first());
 }
 
 template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS) ec_chunks_kernel(BfsParams p) {
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_level_kernel(BfsParams p) {
     __shared__ Smem<THREADS, MP> sm;
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it;
-    const unsigned n = p.ctr->big[it & 3];
-    if (leader()) log_level_tiles(p, it, n);
-    if (n == 0u || p.ctr->error) return;
-    ec_chunks<THREADS, MP>(p, it, n, sm, policy_evict_first());
-}
-
-template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS) ce_level_kernel(BfsParams p) {
-    __shared__ Smem<THREADS, MP> sm;
-    init_hist(sm, p.cull_flags);
-    const int it = p.ctr->cur_it;
-    const unsigned L = p.ctr->qlen[it & 3];
-    if (L == 0u || p.ctr->error) return;
-    if (leader()) log_level_start(p, it, L);
-    ce_level<THREADS, MP>(p, it, L, sm, policy_evict_first());
-}
-
-// Chunk pass after a per-level kernel that wrote an edge frontier: ring index
-// q = iteration (contract-expand) or 2 * iteration + 1 (two-phase expand).
-template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS) edge_chunks_kernel(BfsParams p, int two_phase) {
-    const int q = two_phase ? p.ctr->cur_it * 2 + 1 : p.ctr->cur_it;
-    const unsigned n = p.ctr->big[q & 3];
-    if (leader()) log_level_tiles(p, q, n);
-    if (n == 0u || p.ctr->error) return;
-    edge_chunks<THREADS, MP>(p, (q + 1) & 1, n, policy_evict_first());
+    const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3];
+    if (L + nch == 0u || p.ctr->error) return;
+    if (leader()) log_phase(p, it, L, nch);
+    ce_level<THREADS, MP>(p, it, L, nch, sm, policy_evict_first());
 }
 
 // Two-phase per-level: qi = 2 * it (contract) and 2 * it + 1 (expand).
 template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS) tp_contract_kernel(BfsParams p) {
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_contract_kernel(BfsParams p) {
     __shared__ Smem<THREADS, MP> sm;
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it, qi = 2 * it;
-    const unsigned L = p.ctr->qlen[qi & 3];
-    if (L == 0u || p.ctr->error) return;
-    if (leader()) log_level_start(p, qi, L);
-    tp_contract<THREADS, MP>(p, it, qi, L, sm);
+    const unsigned L = p.ctr->qlen[qi & 3], nch = p.ctr->big[qi & 3];
+    if (L + nch == 0u || p.ctr->error) return;
+    if (leader()) log_phase(p, qi, L, nch);
+    tp_contract<THREADS, MP>(p, it, qi, L, nch, sm, policy_evict_first());
 }
 
 template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS) tp_expand_kernel(BfsParams p) {
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_expand_kernel(BfsParams p) {
     __shared__ Smem<THREADS, MP> sm;
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it, qi = 2 * it + 1;
     const unsigned L = p.ctr->qlen[qi & 3];
     if (L == 0u || p.ctr->error) return;
-    if (leader()) log_level_start(p, qi, L);
+    if (leader()) log_phase(p, qi, L, 0u);
     tp_expand<THREADS, MP>(p, qi, L, sm, policy_evict_first());
 }
 
@@ -809,8 +752,8 @@ __global__ void level_control_kernel(BfsParams p, int strategy) {
     bool more;
     if (strategy == STRATEGY_TWO_PHASE) {
         const int qi = 2 * it;
-        const unsigned vq = c->qlen[(qi + 1) & 3];  // contract output
-        const unsigned eq = c->qlen[(qi + 2) & 3];  // expand output
+        const unsigned vq = c->qlen[(qi + 1) & 3];                        // contract output
+        const unsigned eq = c->qlen[(qi + 2) & 3] + c->big[(qi + 2) & 3];  // expand output
         c->total_queued += c->qlen[qi & 3];
         if (vq == 0u) {
             c->iteration = it;  // the reference leaves after contract without ++
@@ -819,22 +762,23 @@ __global__ void level_control_kernel(BfsParams p, int strategy) {
             c->iteration = it + 1;
             more = eq != 0u;
         }
-        // next body runs phases qi+2 (contract) and qi+3 (expand)
+        // the next body runs phases qi+2 (contract) and qi+3 (expand)
         c->steal[(qi + 2) & 3] = 0u;
         c->steal[(qi + 3) & 3] = 0u;
         c->qlen[(qi + 3) & 3] = 0u;
         c->qlen[(qi + 4) & 3] = 0u;
         c->big[(qi + 3) & 3] = 0u;
-        if (!more) log_level_start(p, vq == 0u ? qi + 1 : qi + 2, 0u);
+        c->big[(qi + 4) & 3] = 0u;
+        if (!more) log_phase(p, vq == 0u ? qi + 1 : qi + 2, 0u, 0u);
     } else {
-        const unsigned next = c->qlen[(it + 1) & 3];
+        const unsigned next = c->qlen[(it + 1) & 3] + c->big[(it + 1) & 3];
         c->total_queued += c->qlen[it & 3];
         c->iteration = it + 1;
         more = next != 0u;
         c->steal[(it + 1) & 3] = 0u;
-        c->big[(it + 1) & 3] = 0u;
         c->qlen[(it + 2) & 3] = 0u;
-        if (!more) log_level_start(p, it + 1, 0u);
+        c->big[(it + 2) & 3] = 0u;
+        if (!more) log_phase(p, it + 1, 0u, 0u);
     }
     if (more && level_limit_hit(it + 1, p.nodes)) {
         c->error |= ERR_LEVEL_LIMIT;
@@ -886,23 +830,15 @@ static KernelFn pick_fused(const KernelConfig &kc) {
 
 struct LevelFns {
     KernelFn level_a;  // ec_level / ce_level / tp_contract
-    KernelFn level_b;  // ec_chunks / (none) / tp_expand
-    void (*edge_chunks)(BfsParams, int);
+    KernelFn level_b;  // tp_expand for two-phase
 };
 
 template <int THREADS, bool MP>
 static LevelFns level_fns(int strategy) {
     LevelFns f{};
-    f.edge_chunks = edge_chunks_kernel<THREADS, MP>;
     switch (strategy) {
-    case STRATEGY_EXPAND_CONTRACT:
-        f.level_a = ec_level_kernel<THREADS, MP>;
-        f.level_b = ec_chunks_kernel<THREADS, MP>;
-        break;
-    case STRATEGY_CONTRACT_EXPAND:
-        f.level_a = ce_level_kernel<THREADS, MP>;
-        f.level_b = nullptr;
-        break;
+    case STRATEGY_EXPAND_CONTRACT: f.level_a = ec_level_kernel<THREADS, MP>; break;
+    case STRATEGY_CONTRACT_EXPAND: f.level_a = ce_level_kernel<THREADS, MP>; break;
     default:
         f.level_a = tp_contract_kernel<THREADS, MP>;
         f.level_b = tp_expand_kernel<THREADS, MP>;
@@ -983,14 +919,7 @@ cudaError_t build_level_graph(BfsParams &p, const KernelConfig &kc, int grid, cu
         LevelFns f = pick_level(kc);
         const int T = kc.threads;
         f.level_a<<<grid, T, 0, cap>>>(p);
-        if (kc.strategy == STRATEGY_EXPAND_CONTRACT) {
-            f.level_b<<<grid, T, 0, cap>>>(p);
-        } else if (kc.strategy == STRATEGY_CONTRACT_EXPAND) {
-            f.edge_chunks<<<grid, T, 0, cap>>>(p, 0);
-        } else {
-            f.level_b<<<grid, T, 0, cap>>>(p);
-            f.edge_chunks<<<grid, T, 0, cap>>>(p, 1);
-        }
+        if (f.level_b) f.level_b<<<grid, T, 0, cap>>>(p);
         level_control_kernel<<<1, 32, 0, cap>>>(p, kc.strategy);
         cudaError_t le = cudaGetLastError();
         cudaGraph_t captured = nullptr;

@@ -37,26 +37,25 @@ struct BfsParams {
     unsigned *mask;          // visited bitmask, bit (v & 31) of word v >> 5
     int *queue[2];           // frontier ping-pong
     int *pred_queue[2];      // predecessor ping-pong (edge frontiers, mark_pred)
-    int4 *chunks;            // grid-wide gather chunks: {start, len, pred, out}
+    int4 *chunks[2];         // grid-wide chunks of neighbour lists, ping-pong by phase: {start, len, pred, 0}
     LevelRecord *levels;     // per-level log (level_cap records)
     Counters *ctr;
     unsigned long long wait_ns;      // grid-barrier spin limit
     unsigned long long cond_handle;  // cudaGraphConditionalHandle (per-level graphs)
     long long qcap;                  // elements per frontier queue
-    int chunk_cap;                   // entries of chunks
+    int chunk_cap;                   // entries of each chunk table
     int level_cap;                   // entries of levels
     int vec_end;                     // 16-byte loads of col are safe below this index
     int nodes;
     int src;
-    int warp_th;  // lists >= warp_th are gathered by a warp
-    int cta_th;   // lists >= cta_th are gathered by the whole CTA
-    int big_th;   // lists >= big_th are cut into chunks gathered by the whole grid
+    int warp_th;  // lists >= warp_th are gathered by one warp; shorter ones by a warp scan
+    int cta_th;   // lists >= cta_th are cut into CTA-sized chunks that the whole grid shares
     unsigned cull_flags;
 };
 
-// Edges per grid-wide chunk: one 16-byte load per thread of a CTA.
+// Edges per grid-wide chunk: four passes of one 16-byte load per thread of a CTA.
 template <int THREADS>
-__host__ __device__ constexpr int chunk_edges() { return THREADS * 4; }
+__host__ __device__ constexpr int chunk_edges() { return THREADS * 16; }
 
 struct KernelConfig {
     int strategy;

@@ -119,14 +119,16 @@ int b40c_enactor_get_statistics(b40c_enactor_t *enactor, long long *total_queued
 int b40c_enactor_last_elapsed_ms(b40c_enactor_t *enactor, float *ms);
 /* Stream (a cudaStream_t) for later searches; NULL = the enactor's own stream. */
 int b40c_enactor_set_stream(b40c_enactor_t *enactor, void *stream);
-/* Tuning policy (the reference's compile-time KernelPolicy, kernel_policy.cuh:61-87):
- * cta_threads in {128,256,512}; warp/cta/grid gather thresholds in edges
- * (defaults 32 / 256 / 1024: lists of at least grid_gather_threshold edges
- * are cut into chunks that every CTA of the grid shares); flags: bit0
- * warp-level cull, bit1 history-hash cull.  0 keeps a field (flags always set). */
+/* Tuning policy (the reference's compile-time KernelPolicy, kernel_policy.cuh:61-87,
+ * WARP_GATHER_THRESHOLD / CTA_GATHER_THRESHOLD): cta_threads in {128,256,512};
+ * lists of at least warp_gather_threshold edges (default 32) are gathered by a
+ * warp, shorter ones by a warp prefix sum; lists of at least
+ * cta_gather_threshold edges (default 1024) are cut into chunks of
+ * 16 * cta_threads edges that every CTA of the grid shares, each chunk
+ * gathered by a whole CTA.  cull_flags: bit0 warp-level cull, bit1
+ * history-hash cull.  A 0 keeps a threshold; cull_flags is always set. */
 int b40c_enactor_set_policy(b40c_enactor_t *enactor, int cta_threads,
-                            int warp_gather_threshold, int cta_gather_threshold,
-                            int grid_gather_threshold, int cull_flags);
+                            int warp_gather_threshold, int cta_gather_threshold, int cull_flags);
 /* Per-level log (the reference's DEBUG per-level queue lengths,
  * enactor_two_phase.cuh:496-499, with device timestamps): when enabled, each
  * later search records per level its %globaltimer start, the end of its tile
@@ -134,7 +136,9 @@ int b40c_enactor_set_policy(b40c_enactor_t *enactor, int cta_threads,
 int b40c_enactor_set_level_log(b40c_enactor_t *enactor, int enable);
 /* Copies up to max_records records of the last search (any out pointer may be
  * NULL); *count gets the number copied, the last one being the end marker
- * (frontier 0).  Levels of the two-phase strategy are its phases. */
+ * (frontier 0, chunks 0).  frontier counts queued vertices (or edges for the
+ * edge-frontier strategies); vertices whose lists went to grid-wide chunks are
+ * counted in chunks instead.  Levels of the two-phase strategy are its phases. */
 int b40c_enactor_level_log(b40c_enactor_t *enactor, int max_records, int64_t *t_start_ns,
                            int64_t *t_tiles_ns, int *frontier, int *chunks, int *count);
 /* Spin limit of every device-side wait (grid barrier), in microseconds. */

@@ -100,12 +100,13 @@ def test_rmat16_vs_oracle(cuda_device, oracle, rmat16, strategy, variant):
 POLICIES = [
     dict(cta_threads=128),
     dict(cta_threads=512),
-    dict(warp_gather_threshold=4, cta_gather_threshold=16, grid_gather_threshold=64),
-    dict(warp_gather_threshold=1, cta_gather_threshold=1, grid_gather_threshold=1),
-    dict(cta_threads=512, warp_gather_threshold=8, cta_gather_threshold=512, grid_gather_threshold=600),
+    dict(warp_gather_threshold=4, cta_gather_threshold=16),
+    dict(warp_gather_threshold=1, cta_gather_threshold=1),
+    dict(warp_gather_threshold=1000000, cta_gather_threshold=1000000),
+    dict(cta_threads=512, warp_gather_threshold=8, cta_gather_threshold=600),
     dict(cull_flags=1),
     dict(cull_flags=2),
-    dict(cull_flags=3, cta_threads=128, grid_gather_threshold=100),
+    dict(cull_flags=3, cta_threads=128, cta_gather_threshold=100),
 ]
 
 
@@ -271,6 +272,11 @@ def test_level_log_matches_oracle_levels(cuda_device, oracle, rmat16):
         b.check(en.EnactFusedSearch(prob, s) if variant == 1 else en.EnactIterativeSearch(prob, s))
         log = en.level_log()
         sizes = [int((ref == d).sum()) for d in range(int(ref.max()) + 1)]
-        assert [r["frontier"] for r in log[:-1]] == sizes
-        assert log[-1]["frontier"] == 0
+        # one record per level (depths 0..d) plus the end marker
+        assert len(log) == len(sizes) + 1
+        assert log[0]["frontier"] == 1
+        # vertices of a level are queued or, with long lists, turned into chunks
+        for r, n in zip(log[:-1], sizes):
+            assert r["frontier"] <= n and (r["frontier"] == n or r["chunks"] > 0)
+        assert log[-1]["frontier"] == 0 and log[-1]["chunks"] == 0
         assert all(log[i]["start_ns"] <= log[i + 1]["start_ns"] for i in range(len(log) - 1))
