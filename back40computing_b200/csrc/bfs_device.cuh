@@ -34,20 +34,25 @@ enum : unsigned {
 __device__ __forceinline__ bool level_limit_hit(int it, int nodes) { return it > nodes + 2; }
 
 // Per-search device counters.  ring[x][it & 3] as CtaWorkProgress does.
-struct alignas(128) Counters {
+// Every group of counters that takes atomics lives in its own 256-byte block,
+// so that their atomics are served by different L2 slices instead of queueing
+// at one.
+struct alignas(256) Counters {
     unsigned qlen[4];    // qlen[q&3]: length of the input frontier queue of phase q
+    unsigned pad_q[60];
     unsigned steal[4];   // steal[q&3]: next warp tile to hand out in phase q
+    unsigned pad_s[60];
     unsigned big[4];     // big[q&3]: grid-wide chunks of neighbour lists input to phase q
+    unsigned pad_b[60];
     unsigned error;      // ERR_* bits
     int iteration;       // iteration counter at exit (reference d_iteration)
     int cur_it;          // current iteration for per-level (graph-driven) kernels
     unsigned done;       // 1 once the search has finished (per-level variants)
     unsigned long long total_queued;  // sum of frontier lengths (instrumented)
-    unsigned pad0[8];
-    // Grid barrier in its own 128-byte line.
-    alignas(128) unsigned bar_count;
+    unsigned pad_e[58];
+    unsigned bar_count;  // grid barrier
     unsigned bar_gen;
-    unsigned pad1[29];
+    unsigned pad_g[61];
     unsigned sticky;  // OR of error over searches since the host last read it (not reset per search)
 };
 

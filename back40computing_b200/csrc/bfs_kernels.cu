@@ -50,11 +50,16 @@ constexpr int WINDOW = 128;      // per-warp scan-gather window (4 per lane)
 // matter more than registers.
 #define MIN_BLOCKS(threads) (1280 / (threads))
 
+constexpr int OBUF = 256;        // per-warp staging of vertex-queue appends
+constexpr int TILE_GRAB = 4;     // warp tiles handed out per atomic
+
 template <bool MP>
 struct WarpSmem {
     int gofs[WINDOW];
     int gpred[MP ? WINDOW : 1];
     int surv[WINDOW];
+    int obuf[OBUF];
+    unsigned nbuf;
 };
 
 template <int THREADS, bool MP>
@@ -123,10 +128,30 @@ __device__ __forceinline__ unsigned cull4(const BfsParams &p, Smem<THREADS, MP> 
     return claimed;
 }
 
-// Appends the flagged elements of every lane to queue q with one atomicAdd
-// per warp.  Called by all lanes together.
-__device__ __forceinline__ void enqueue4(unsigned flags, const int (&u)[4], int *q, unsigned *qlen, long long qcap,
-                                         unsigned *err) {
+// Writes the warp's staged appends to queue q with one atomicAdd (coalesced
+// stores).  Called by all lanes together.
+template <bool MP>
+__device__ __forceinline__ void warp_flush(WarpSmem<MP> &ws, unsigned n, int *q, unsigned *qlen, long long qcap,
+                                           unsigned *err) {
+    unsigned base = 0;
+    if (lane_id() == 0) base = atomicAdd(qlen, n);
+    base = __shfl_sync(FULL, base, 0);
+    for (unsigned i = lane_id(); i < n; i += 32) {
+        const unsigned long long pos = (unsigned long long)base + i;
+        if (pos < (unsigned long long)qcap) q[pos] = ws.obuf[i];
+        else atomicOr(err, ERR_OVERFLOW);
+    }
+    __syncwarp();
+}
+
+// Stages the flagged elements of every lane (bit j of flags marks u[j]) in the
+// warp's buffer; flushes it to queue q when fewer than 128 slots stay free.
+// The reference reserves queue space with one atomic per CTA tile
+// (util/scan/cooperative_scan.cuh:173-195); here it is one per <= 256
+// appends of a warp.  Called by all lanes together.
+template <bool MP>
+__device__ __forceinline__ void stage4(WarpSmem<MP> &ws, unsigned flags, const int (&u)[4], int *q, unsigned *qlen,
+                                       long long qcap, unsigned *err) {
     const unsigned lt = lanemask_lt();
     unsigned total = 0, pre[4];
 #pragma unroll
@@ -136,17 +161,27 @@ __device__ __forceinline__ void enqueue4(unsigned flags, const int (&u)[4], int 
         total += __popc(b);
     }
     if (total == 0u) return;  // warp-uniform
-    unsigned base = 0;
-    if (lane_id() == 0) base = atomicAdd(qlen, total);
-    base = __shfl_sync(FULL, base, 0);
+    unsigned n = ws.nbuf;
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-        if ((flags >> j) & 1u) {
-            unsigned long long pos = (unsigned long long)base + pre[j];
-            if (pos < (unsigned long long)qcap) q[pos] = u[j];
-            else atomicOr(err, ERR_OVERFLOW);
-        }
+    for (int j = 0; j < 4; j++)
+        if ((flags >> j) & 1u) ws.obuf[n + pre[j]] = u[j];
+    n += total;
+    __syncwarp();
+    if (n > unsigned(OBUF - WINDOW)) {
+        warp_flush(ws, n, q, qlen, qcap, err);
+        n = 0;
     }
+    if (lane_id() == 0) ws.nbuf = n;
+    __syncwarp();
+}
+
+// Flushes what the warp still holds; every warp calls it at the end of a phase.
+template <bool MP>
+__device__ __forceinline__ void stage_drain(WarpSmem<MP> &ws, int *q, unsigned *qlen, long long qcap, unsigned *err) {
+    const unsigned n = ws.nbuf;
+    if (n) warp_flush(ws, n, q, qlen, qcap, err);
+    if (lane_id() == 0) ws.nbuf = 0;
+    __syncwarp();
 }
 
 __device__ __forceinline__ void row_range(const BfsParams &p, int v, int &start, int &len) {
@@ -354,7 +389,10 @@ struct DiscoverSink {
             if (((disc >> j) & 1u) && ln[j] >= p.cta_th &&
                 push_chunks<THREADS>(p, chunk_out, chunk_count, st[j], ln[j], u[j]))
                 enq &= ~(1u << j);
-        enqueue4(enq, u, q_out, qlen_out, p.qcap, &p.ctr->error);
+        stage4(sm.w[threadIdx.x >> 5], enq, u, q_out, qlen_out, p.qcap, &p.ctr->error);
+    }
+    __device__ __forceinline__ void drain() const {
+        stage_drain(sm.w[threadIdx.x >> 5], q_out, qlen_out, p.qcap, &p.ctr->error);
     }
 };
 
@@ -440,7 +478,10 @@ struct ContractSink {
 #pragma unroll
         for (int j = 0; j < 4; j++)
             if ((surv >> j) & 1u) p.labels[u[j]] = MP ? pred[j] : it;
-        enqueue4(surv, u, q_out, qlen_out, p.qcap, &p.ctr->error);
+        stage4(sm.w[threadIdx.x >> 5], surv, u, q_out, qlen_out, p.qcap, &p.ctr->error);
+    }
+    __device__ __forceinline__ void drain() const {
+        stage_drain(sm.w[threadIdx.x >> 5], q_out, qlen_out, p.qcap, &p.ctr->error);
     }
 };
 
@@ -464,16 +505,19 @@ __device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, S
     const int *q_in = p.queue[it & 1];
     const unsigned ntiles = (L + 31) / 32;
     for (;;) {
-        const unsigned t = warp_next_tile(&c->steal[it & 3]);
-        if (t >= ntiles) break;
-        const unsigned idx = t * 32 + lane_id();
-        int v = -1, start = 0, len = 0;
-        if (idx < L) {
-            v = ld_cg(q_in + idx);
-            row_range(p, v, start, len);
+        const unsigned t0 = warp_next_tile(&c->steal[it & 3]) * TILE_GRAB;
+        if (t0 >= ntiles) break;
+        for (unsigned t = t0; t < t0 + TILE_GRAB && t < ntiles; t++) {
+            const unsigned idx = t * 32 + lane_id();
+            int v = -1, start = 0, len = 0;
+            if (idx < L) {
+                v = ld_cg(q_in + idx);
+                row_range(p, v, start, len);
+            }
+            warp_lists<MP, false>(p, ws, sink, pol, start, len, v, nullptr);
         }
-        warp_lists<MP, false>(p, ws, sink, pol, start, len, v, nullptr);
     }
+    sink.drain();
 }
 
 // Edge-frontier phase input: warp tiles of 128 elements (4 per lane,
@@ -515,6 +559,7 @@ __device__ void tp_contract(const BfsParams &p, int it, int qi, unsigned L, unsi
     ContractSink<THREADS, MP> sink{p, sm, p.queue[(qi + 1) & 1], &p.ctr->qlen[(qi + 1) & 3], it};
     gather_chunks<THREADS>(p, p.chunks[qi & 1], nch, sink, pol);
     edge_tiles<MP>(p.queue[qi & 1], p.pred_queue[qi & 1], L, sink);
+    sink.drain();
 }
 
 // Two-phase expand, phase qi = 2 * it + 1 (two_phase/expand_atomic/cta.cuh:606-719).
@@ -527,17 +572,19 @@ __device__ void tp_expand(const BfsParams &p, int qi, unsigned L, Smem<THREADS, 
     const int *q_in = p.queue[qi & 1];
     const unsigned ntiles = (L + 31) / 32;
     for (;;) {
-        const unsigned t = warp_next_tile(&c->steal[qi & 3]);
-        if (t >= ntiles) break;
-        const unsigned idx = t * 32 + lane_id();
-        int v = -1, start = 0, len = 0;
-        if (idx < L) {
-            v = ld_cg(q_in + idx);
-            row_range(p, v, start, len);
-            if (len >= p.cta_th && push_chunks<THREADS>(p, p.chunks[nq], &c->big[(qi + 1) & 3], start, len, v))
-                len = 0;
+        const unsigned t0 = warp_next_tile(&c->steal[qi & 3]) * TILE_GRAB;
+        if (t0 >= ntiles) break;
+        for (unsigned t = t0; t < t0 + TILE_GRAB && t < ntiles; t++) {
+            const unsigned idx = t * 32 + lane_id();
+            int v = -1, start = 0, len = 0;
+            if (idx < L) {
+                v = ld_cg(q_in + idx);
+                row_range(p, v, start, len);
+                if (len >= p.cta_th && push_chunks<THREADS>(p, p.chunks[nq], &c->big[(qi + 1) & 3], start, len, v))
+                    len = 0;
+            }
+            warp_lists<MP, true>(p, ws, out, pol, start, len, v, &c->qlen[(qi + 1) & 3]);
         }
-        warp_lists<MP, true>(p, ws, out, pol, start, len, v, &c->qlen[(qi + 1) & 3]);
     }
 }
 
@@ -562,6 +609,8 @@ __device__ __forceinline__ void log_phase(const BfsParams &p, int idx, unsigned 
 
 template <int THREADS, bool MP>
 __device__ __forceinline__ void init_hist(Smem<THREADS, MP> &sm, unsigned flags) {
+    if (lane_id() == 0) sm.w[threadIdx.x >> 5].nbuf = 0;
+    __syncwarp();
     if (flags & CULL_HISTORY) {
         for (int i = threadIdx.x; i < HIST_SIZE; i += THREADS) sm.hist[i] = -1;
         __syncthreads();
