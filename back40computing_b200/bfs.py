@@ -215,8 +215,9 @@ class _Enactor:
         check(lib().b40c_enactor_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)))
 
     def set_policy(self, cta_threads: int = 0, warp_gather_threshold: int = 0, cta_gather_threshold: int = 0,
-                   cull_flags: int = 0) -> None:
-        """KernelPolicy knobs: CTA size, warp / CTA gather thresholds (edges), cull flags."""
+                   cull_flags: int = -1) -> None:
+        """KernelPolicy knobs: CTA size, warp / CTA gather thresholds (edges; 0 keeps),
+        cull flags (bit0 warp cull, bit1 history cache; -1 keeps)."""
         check(lib().b40c_enactor_set_policy(self._h, cta_threads, warp_gather_threshold, cta_gather_threshold,
                                             cull_flags))
 

@@ -79,7 +79,7 @@ struct b40c_enactor {
     bool instrument = false, debug = false;
     int threads = 256;
     int warp_th = 32, cta_th = 1024;
-    unsigned cull_flags = 0;
+    unsigned cull_flags = CULL_HISTORY;
     unsigned long long wait_ns = 5000000000ull;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
@@ -694,12 +694,12 @@ extern "C" int b40c_enactor_set_policy(b40c_enactor_t *e, int cta_threads, int w
     if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
     if (cta_threads && cta_threads != 128 && cta_threads != 256 && cta_threads != 512)
         return set_error(B40C_ERR_INVALID_VALUE, "cta_threads must be 128, 256 or 512");
-    if (warp_th < 0 || cta_th < 0 || cull_flags < 0 || cull_flags > 3)
+    if (warp_th < 0 || cta_th < 0 || cull_flags < -1 || cull_flags > 3)
         return set_error(B40C_ERR_INVALID_VALUE, "invalid policy field");
     if (cta_threads) e->threads = cta_threads;
     if (warp_th) e->warp_th = warp_th;
     if (cta_th) e->cta_th = cta_th;
-    e->cull_flags = unsigned(cull_flags);
+    if (cull_flags >= 0) e->cull_flags = unsigned(cull_flags);
     return B40C_SUCCESS;
 }
 

@@ -42,7 +42,7 @@
 namespace b40c_b200 {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int HIST_SIZE = 1024;  // history-hash entries per CTA
+constexpr int VCACHE = 2048;     // history cache: visited-mask words held per CTA
 constexpr int WINDOW = 128;      // per-warp scan-gather window (4 per lane)
 
 // Resident CTAs per SM requested from ptxas: 40 warps per SM (48 registers
@@ -65,7 +65,7 @@ struct WarpSmem {
 template <int THREADS, bool MP>
 struct Smem {
     WarpSmem<MP> w[THREADS / 32];
-    int hist[HIST_SIZE];
+    unsigned long long vcache[VCACHE];  // (mask word index << 32) | word value
     unsigned flag;
 };
 
@@ -73,32 +73,35 @@ struct Smem {
 // Culling and enqueueing, 4 elements per thread
 // ---------------------------------------------------------------------------------------
 
-// Optional culls.  Called by every lane of the warp (match_any needs them all).
-template <int THREADS, bool MP>
-__device__ __forceinline__ bool pre_cull(bool valid, int u, unsigned flags, Smem<THREADS, MP> &sm) {
-    if (flags & CULL_WARP) {
-        // Lanes without an element get distinct negative keys so they never match.
-        int key = valid ? u : int(0x80000000u | lane_id());
-        unsigned peers = __match_any_sync(FULL, key);
-        if (valid && (int)lane_id() != __ffs(peers) - 1) valid = false;
-    }
-    if ((flags & CULL_HISTORY) && valid) {
-        int h = u & (HIST_SIZE - 1);
-        if (sm.hist[h] == u) valid = false;  // seen recently by this CTA
-        else sm.hist[h] = u;                 // racy insert is harmless
-    }
-    return valid;
-}
+// Slot of mask word w in the CTA's history cache (multiplicative hash, so the
+// low-popcount word indices of skewed graphs spread over the slots).
+__device__ __forceinline__ unsigned vcache_slot(unsigned w) { return (w * 2654435761u) >> (32 - 11); }
+static_assert(VCACHE == 2048, "vcache_slot takes 11 bits");
 
 // Exact test-and-set of the visited bits of up to 4 vertices (bit j of valid
 // marks u[j]).  Returns the bits of the vertices this thread claimed first.
+//
+// The history cull (the reference's per-CTA history hash of recently seen
+// ids, two_phase/contract_atomic/cta.cuh:276-297) is kept here as a
+// shared-memory cache of visited-mask words.  Bits are only ever set during a
+// search, so a cached word is a lower bound of the true one: a bit set there
+// culls the vertex with no global access, a clear bit falls through to the L2
+// probe, whose result refreshes the entry.  Hub vertices' words stay cached,
+// which keeps their mask lines from becoming L2 hot spots.  The optional warp
+// cull (__match_any_sync) drops repeats inside a warp first.
 template <int THREADS, bool MP>
 __device__ __forceinline__ unsigned cull4(const BfsParams &p, Smem<THREADS, MP> &sm, unsigned valid,
                                           const int (&u)[4]) {
-    if (p.cull_flags) {
+    const bool history = p.cull_flags & CULL_HISTORY;
+    if (p.cull_flags & CULL_WARP) {
 #pragma unroll
-        for (int j = 0; j < 4; j++)
-            if (!pre_cull<THREADS, MP>((valid >> j) & 1u, u[j], p.cull_flags, sm)) valid &= ~(1u << j);
+        for (int j = 0; j < 4; j++) {
+            // Lanes without an element get distinct negative keys so they never match.
+            const bool ok = (valid >> j) & 1u;
+            const int key = ok ? u[j] : int(0x80000000u | lane_id());
+            const unsigned peers = __match_any_sync(FULL, key);
+            if (ok && (int)lane_id() != __ffs(peers) - 1) valid &= ~(1u << j);
+        }
     }
     unsigned w[4], bit[4], m[4];
 #pragma unroll
@@ -111,20 +114,29 @@ __device__ __forceinline__ unsigned cull4(const BfsParams &p, Smem<THREADS, MP> 
         }
         w[j] = ok ? (unsigned)u[j] >> 5 : 0u;
         bit[j] = 1u << ((unsigned)u[j] & 31u);
+        if (ok && history) {
+            const unsigned long long e = sm.vcache[vcache_slot(w[j])];
+            if (unsigned(e >> 32) == w[j] && (unsigned(e) & bit[j])) valid &= ~(1u << j);
+        }
     }
 #pragma unroll
-    for (int j = 0; j < 4; j++) m[j] = ld_cg(p.mask + w[j]);  // 4 probes in flight
+    for (int j = 0; j < 4; j++) m[j] = ((valid >> j) & 1u) ? ld_cg(p.mask + w[j]) : 0u;  // probes in flight
     unsigned need = 0;
 #pragma unroll
     for (int j = 0; j < 4; j++)
         if (((valid >> j) & 1u) && !(m[j] & bit[j])) need |= 1u << j;
     unsigned old[4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) old[j] = ((need >> j) & 1u) ? atomicOr(p.mask + w[j], bit[j]) : bit[j];
+    for (int j = 0; j < 4; j++) old[j] = ((need >> j) & 1u) ? atomicOr(p.mask + w[j], bit[j]) : m[j];
     unsigned claimed = 0;
 #pragma unroll
-    for (int j = 0; j < 4; j++)
-        if (!(old[j] & bit[j])) claimed |= 1u << j;
+    for (int j = 0; j < 4; j++) {
+        if ((valid >> j) & 1u) {
+            if (!(old[j] & bit[j])) claimed |= 1u << j;
+            if (history)
+                sm.vcache[vcache_slot(w[j])] = ((unsigned long long)w[j] << 32) | (old[j] | bit[j]);
+        }
+    }
     return claimed;
 }
 
@@ -612,7 +624,8 @@ __device__ __forceinline__ void init_hist(Smem<THREADS, MP> &sm, unsigned flags)
     if (lane_id() == 0) sm.w[threadIdx.x >> 5].nbuf = 0;
     __syncwarp();
     if (flags & CULL_HISTORY) {
-        for (int i = threadIdx.x; i < HIST_SIZE; i += THREADS) sm.hist[i] = -1;
+        // Tag 0xffffffff matches no mask word (word indices stay below 2^27).
+        for (int i = threadIdx.x; i < VCACHE; i += THREADS) sm.vcache[i] = ~0ull << 32;
         __syncthreads();
     }
 }

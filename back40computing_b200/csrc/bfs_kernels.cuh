@@ -16,7 +16,7 @@ enum Strategy : int {
 
 enum CullFlags : unsigned {
     CULL_WARP = 1u,     // __match_any_sync duplicate cull inside a warp
-    CULL_HISTORY = 2u,  // per-CTA shared-memory history hash
+    CULL_HISTORY = 2u,  // per-CTA shared-memory history cache of visited-mask words
 };
 
 // One record per BFS level, written by one thread of the kernel that runs it:

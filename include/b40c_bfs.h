@@ -125,8 +125,10 @@ int b40c_enactor_set_stream(b40c_enactor_t *enactor, void *stream);
  * warp, shorter ones by a warp prefix sum; lists of at least
  * cta_gather_threshold edges (default 1024) are cut into chunks of
  * 16 * cta_threads edges that every CTA of the grid shares, each chunk
- * gathered by a whole CTA.  cull_flags: bit0 warp-level cull, bit1
- * history-hash cull.  A 0 keeps a threshold; cull_flags is always set. */
+ * gathered by a whole CTA.  cull_flags: bit0 warp-level cull
+ * (__match_any_sync), bit1 history cull through a per-CTA shared-memory cache
+ * of visited-mask words (default: bit1 only).  A 0 keeps a threshold, a -1
+ * keeps the cull flags. */
 int b40c_enactor_set_policy(b40c_enactor_t *enactor, int cta_threads,
                             int warp_gather_threshold, int cta_gather_threshold, int cull_flags);
 /* Per-level log (the reference's DEBUG per-level queue lengths,

@@ -104,6 +104,7 @@ POLICIES = [
     dict(warp_gather_threshold=1, cta_gather_threshold=1),
     dict(warp_gather_threshold=1000000, cta_gather_threshold=1000000),
     dict(cta_threads=512, warp_gather_threshold=8, cta_gather_threshold=600),
+    dict(cull_flags=0),
     dict(cull_flags=1),
     dict(cull_flags=2),
     dict(cull_flags=3, cta_threads=128, cta_gather_threshold=100),
