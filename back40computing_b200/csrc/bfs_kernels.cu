@@ -632,6 +632,14 @@ __device__ __forceinline__ void init_hist(Smem<THREADS, MP> &sm, unsigned flags)
 
 __device__ __forceinline__ bool leader() { return blockIdx.x == 0 && threadIdx.x == 0; }
 
+// The kernels keep Smem in dynamic shared memory (it can exceed the 48 KB
+// static limit at 512 threads); launches pass sizeof(Smem<THREADS, MP>).
+template <int THREADS, bool MP>
+__device__ __forceinline__ Smem<THREADS, MP> &kernel_smem() {
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
+    return *reinterpret_cast<Smem<THREADS, MP> *>(dyn_smem);
+}
+
 // ---------------------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------------------
@@ -679,7 +687,7 @@ __device__ __forceinline__ void finish_search(const BfsParams &p, int iteration,
 
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(BfsParams p) {
-    __shared__ Smem<THREADS, MP> sm;
+    Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const uint64_t pol = policy_evict_first();
     Counters *c = p.ctr;
@@ -701,7 +709,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
 
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(BfsParams p) {
-    __shared__ Smem<THREADS, MP> sm;
+    Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const uint64_t pol = policy_evict_first();
     Counters *c = p.ctr;
@@ -727,7 +735,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
 // indexed by phase (2 * iteration for contract, + 1 for expand).
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(BfsParams p) {
-    __shared__ Smem<THREADS, MP> sm;
+    Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const uint64_t pol = policy_evict_first();
     Counters *c = p.ctr;
@@ -762,7 +770,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
 
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_level_kernel(BfsParams p) {
-    __shared__ Smem<THREADS, MP> sm;
+    Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it;
     const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3];
@@ -773,7 +781,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_level_kernel(
 
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_level_kernel(BfsParams p) {
-    __shared__ Smem<THREADS, MP> sm;
+    Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it;
     const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3];
@@ -785,7 +793,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_level_kernel(
 // Two-phase per-level: qi = 2 * it (contract) and 2 * it + 1 (expand).
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_contract_kernel(BfsParams p) {
-    __shared__ Smem<THREADS, MP> sm;
+    Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it, qi = 2 * it;
     const unsigned L = p.ctr->qlen[qi & 3], nch = p.ctr->big[qi & 3];
@@ -796,7 +804,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_contract_kern
 
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_expand_kernel(BfsParams p) {
-    __shared__ Smem<THREADS, MP> sm;
+    Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it, qi = 2 * it + 1;
     const unsigned L = p.ctr->qlen[qi & 3];
@@ -886,6 +894,24 @@ static KernelFn fused_fn_t(int threads, int strategy) {
     }
 }
 
+template <bool MP>
+static size_t smem_bytes_t(int threads) {
+    switch (threads) {
+    case 128: return sizeof(Smem<128, MP>);
+    case 512: return sizeof(Smem<512, MP>);
+    default: return sizeof(Smem<256, MP>);
+    }
+}
+
+static size_t smem_bytes(const KernelConfig &kc) {
+    return kc.mark_pred ? smem_bytes_t<true>(kc.threads) : smem_bytes_t<false>(kc.threads);
+}
+
+// Opts a kernel in to its dynamic shared memory size (beyond 48 KB needs it).
+static cudaError_t allow_smem(const void *fn, size_t bytes) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+}
+
 static KernelFn pick_fused(const KernelConfig &kc) {
     return kc.mark_pred ? fused_fn_t<true>(kc.threads, kc.strategy) : fused_fn_t<false>(kc.threads, kc.strategy);
 }
@@ -922,13 +948,14 @@ static LevelFns pick_level(const KernelConfig &kc) {
     return kc.mark_pred ? level_fns_t<true>(kc.threads, kc.strategy) : level_fns_t<false>(kc.threads, kc.strategy);
 }
 
-static cudaError_t grid_for(const void *fn, int threads, int *grid) {
+static cudaError_t grid_for(const void *fn, int threads, size_t smem, int *grid) {
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, 0);
+    if ((e = allow_smem(fn, smem))) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem);
     if (e) return e;
     if (occ < 1) return cudaErrorInvalidConfiguration;
     *grid = sms * occ;
@@ -941,18 +968,26 @@ cudaError_t launch_search_init(const BfsParams &p, const KernelConfig &kc, cudaS
 }
 
 cudaError_t fused_grid_limit(const KernelConfig &kc, int *grid) {
-    return grid_for((const void *)pick_fused(kc), kc.threads, grid);
+    return grid_for((const void *)pick_fused(kc), kc.threads, smem_bytes(kc), grid);
 }
 
 cudaError_t level_grid_limit(const KernelConfig &kc, int *grid) {
-    return grid_for((const void *)pick_level(kc).level_a, kc.threads, grid);
+    LevelFns f = pick_level(kc);
+    if (f.level_b) {
+        cudaError_t e = allow_smem((const void *)f.level_b, smem_bytes(kc));
+        if (e) return e;
+    }
+    return grid_for((const void *)f.level_a, kc.threads, smem_bytes(kc), grid);
 }
 
 cudaError_t launch_fused(const BfsParams &p, const KernelConfig &kc, int grid, cudaStream_t stream) {
     KernelFn fn = pick_fused(kc);
+    const size_t smem = smem_bytes(kc);
+    cudaError_t e = allow_smem((const void *)fn, smem);
+    if (e) return e;
     BfsParams arg = p;
     void *args[] = {&arg};
-    return cudaLaunchCooperativeKernel((const void *)fn, dim3(grid), dim3(kc.threads), args, 0, stream);
+    return cudaLaunchCooperativeKernel((const void *)fn, dim3(grid), dim3(kc.threads), args, smem, stream);
 }
 
 cudaError_t build_level_graph(BfsParams &p, const KernelConfig &kc, int grid, cudaGraphExec_t *exec,
@@ -980,8 +1015,11 @@ cudaError_t build_level_graph(BfsParams &p, const KernelConfig &kc, int grid, cu
             break;
         LevelFns f = pick_level(kc);
         const int T = kc.threads;
-        f.level_a<<<grid, T, 0, cap>>>(p);
-        if (f.level_b) f.level_b<<<grid, T, 0, cap>>>(p);
+        const size_t smem = smem_bytes(kc);
+        if ((e = allow_smem((const void *)f.level_a, smem))) break;
+        if (f.level_b && (e = allow_smem((const void *)f.level_b, smem))) break;
+        f.level_a<<<grid, T, smem, cap>>>(p);
+        if (f.level_b) f.level_b<<<grid, T, smem, cap>>>(p);
         level_control_kernel<<<1, 32, 0, cap>>>(p, kc.strategy);
         cudaError_t le = cudaGetLastError();
         cudaGraph_t captured = nullptr;

@@ -55,3 +55,12 @@ def test_product_never_imports_the_oracle():
     for path in (ROOT / "back40computing_b200").rglob("*.py"):
         src = path.read_text()
         assert "oracle" not in re.sub(r"#.*", "", src).replace("oracle/", ""), path
+
+
+def test_library_is_not_older_than_its_sources():
+    """A failed build keeps the previous .so; this catches running it stale."""
+    from back40computing_b200 import build
+    lib = build.LIB
+    assert lib.exists(), "libb40c_bfs.so not built"
+    newest = max(p.stat().st_mtime for p in list(build.CSRC.iterdir()) + [build.INCLUDE / "b40c_bfs.h"])
+    assert lib.stat().st_mtime >= newest, "libb40c_bfs.so is older than csrc/: rebuild"
