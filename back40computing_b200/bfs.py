@@ -225,22 +225,19 @@ class _Enactor:
         check(lib().b40c_enactor_set_level_log(self._h, int(enable)))
 
     def level_log(self, max_records: int = 4096) -> list:
-        """Per-level records of the last search: start/tile-phase-end times (ns,
-        relative to the search start), input frontier length, grid-wide chunks."""
+        """Per-level records of the last search: start time (ns, relative to the
+        first level), input frontier queue length, input CTA and warp chunks."""
         ts = (ctypes.c_int64 * max_records)()
-        tt = (ctypes.c_int64 * max_records)()
         fr = (ctypes.c_int * max_records)()
         ch = (ctypes.c_int * max_records)()
+        wc = (ctypes.c_int * max_records)()
         n = ctypes.c_int()
-        check(lib().b40c_enactor_level_log(self._h, max_records, ts, tt, fr, ch, ctypes.byref(n)))
+        check(lib().b40c_enactor_level_log(self._h, max_records, ts, fr, ch, wc, ctypes.byref(n)))
         if n.value == 0:
             return []
         t0 = ts[0]
-        out = []
-        for i in range(n.value):
-            out.append({"level": i, "start_ns": ts[i] - t0, "tiles_done_ns": (tt[i] - t0) if tt[i] else None,
-                        "frontier": fr[i], "chunks": ch[i]})
-        return out
+        return [{"level": i, "start_ns": ts[i] - t0, "frontier": fr[i], "chunks": ch[i], "wchunks": wc[i]}
+                for i in range(n.value)]
 
     def set_wait_limit_us(self, us: int) -> None:
         check(lib().b40c_enactor_set_wait_limit_us(self._h, int(us)))

@@ -42,8 +42,10 @@ struct alignas(256) Counters {
     unsigned pad_q[60];
     unsigned steal[4];   // steal[q&3]: next warp tile to hand out in phase q
     unsigned pad_s[60];
-    unsigned big[4];     // big[q&3]: grid-wide chunks of neighbour lists input to phase q
+    unsigned big[4];     // big[q&3]: CTA chunks of neighbour lists input to phase q
     unsigned pad_b[60];
+    unsigned wch[4];     // wch[q&3]: warp chunks of neighbour lists input to phase q
+    unsigned pad_w[60];
     unsigned error;      // ERR_* bits
     int iteration;       // iteration counter at exit (reference d_iteration)
     int cur_it;          // current iteration for per-level (graph-driven) kernels

@@ -78,15 +78,17 @@ struct b40c_enactor {
     int strategy = B40C_EXPAND_CONTRACT;
     bool instrument = false, debug = false;
     int threads = 256;
-    int warp_th = 32, cta_th = 1024;
+    int warp_th = 64, cta_th = 1024;
     unsigned cull_flags = CULL_HISTORY;
     unsigned long long wait_ns = 5000000000ull;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     Counters *d_ctr = nullptr;
     Counters *h_ctr = nullptr;  // pinned
-    int4 *d_chunks[2] = {nullptr, nullptr};
-    int chunk_cap = 0;  // entries per table
+    int4 *d_chunks[2] = {nullptr, nullptr};   // CTA chunks
+    int4 *d_wchunks[2] = {nullptr, nullptr};  // warp chunks
+    int chunk_cap = 0;   // entries per CTA chunk table
+    int wchunk_cap = 0;  // entries per warp chunk table
     LevelRecord *d_levels = nullptr;  // per-level log, when enabled
     bool log_levels = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -228,11 +230,14 @@ int ensure_enactor_buffers(b40c_enactor *e, b40c_problem *p) {
         CUDA_TRY(cudaHostAlloc(&e->h_ctr, sizeof(Counters), cudaHostAllocDefault), "Enactor cudaHostAlloc");
         std::memset(e->h_ctr, 0, sizeof(Counters));
     }
-    // Chunks per level: each vertex expands once per search, and a list of
-    // len >= cta_th edges takes at most len / CH + 2 chunks (CH >= 2048 edges).
-    const long long bt = std::max(1, std::max(e->cta_th, e->warp_th));
-    long long need = p->edges / chunk_edges<128>() + 2 * (p->edges / bt) + 64;
-    if (need > (1ll << 30)) need = 1ll << 30;
+    // Chunks per phase: each vertex expands once per search, and a list of len
+    // edges placed in a table of CH-edge chunks takes at most len / CH + 2
+    // entries (CH >= 2048 for CTA chunks, 512 for warp chunks).
+    const long long ct = std::max(1, std::max(e->cta_th, e->warp_th)), wt = std::max(1, e->warp_th);
+    long long need = p->edges / chunk_edges<128>() + 2 * (p->edges / ct) + 64;
+    long long wneed = p->edges / WARP_CHUNK + 2 * (p->edges / wt) + 64;
+    need = std::min(need, 1ll << 30);
+    wneed = std::min(wneed, 1ll << 30);
     if (e->chunk_cap < need) {
         for (int i = 0; i < 2; i++) {
             cudaFree(e->d_chunks[i]);
@@ -240,8 +245,18 @@ int ensure_enactor_buffers(b40c_enactor *e, b40c_problem *p) {
         }
         e->chunk_cap = 0;
         for (int i = 0; i < 2; i++)
-            CUDA_TRY(cudaMalloc(&e->d_chunks[i], sizeof(int4) * size_t(need)), "Enactor cudaMalloc chunk table");
+            CUDA_TRY(cudaMalloc(&e->d_chunks[i], sizeof(int4) * size_t(need)), "Enactor cudaMalloc CTA chunk table");
         e->chunk_cap = int(need);
+    }
+    if (e->wchunk_cap < wneed) {
+        for (int i = 0; i < 2; i++) {
+            cudaFree(e->d_wchunks[i]);
+            e->d_wchunks[i] = nullptr;
+        }
+        e->wchunk_cap = 0;
+        for (int i = 0; i < 2; i++)
+            CUDA_TRY(cudaMalloc(&e->d_wchunks[i], sizeof(int4) * size_t(wneed)), "Enactor cudaMalloc warp chunk table");
+        e->wchunk_cap = int(wneed);
     }
     if (e->log_levels && !e->d_levels)
         CUDA_TRY(cudaMalloc(&e->d_levels, sizeof(LevelRecord) * LEVEL_LOG_CAP), "Enactor cudaMalloc level log");
@@ -260,6 +275,8 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
     }
     bp.chunks[0] = e->d_chunks[0];
     bp.chunks[1] = e->d_chunks[1];
+    bp.wchunks[0] = e->d_wchunks[0];
+    bp.wchunks[1] = e->d_wchunks[1];
     bp.levels = e->log_levels ? e->d_levels : nullptr;
     bp.level_cap = LEVEL_LOG_CAP;
     bp.ctr = e->d_ctr;
@@ -270,6 +287,7 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
     if (qcap > 0xffffffffll) qcap = 0xffffffffll;
     bp.qcap = qcap;
     bp.chunk_cap = e->chunk_cap;
+    bp.wchunk_cap = e->wchunk_cap;
     bp.vec_end = p->mapped ? int(p->edges & ~int64_t(3)) : int(p->edges + 4);
     bp.nodes = int(p->nodes);
     bp.src = src;
@@ -600,6 +618,8 @@ extern "C" int b40c_enactor_destroy(b40c_enactor_t *e) {
     cudaFree(e->d_ctr);
     cudaFree(e->d_chunks[0]);
     cudaFree(e->d_chunks[1]);
+    cudaFree(e->d_wchunks[0]);
+    cudaFree(e->d_wchunks[1]);
     cudaFree(e->d_levels);
     if (e->h_ctr) cudaFreeHost(e->h_ctr);
     cudaEventDestroy(e->ev0);
@@ -710,8 +730,8 @@ extern "C" int b40c_enactor_set_level_log(b40c_enactor_t *e, int enable) {
     return B40C_SUCCESS;
 }
 
-extern "C" int b40c_enactor_level_log(b40c_enactor_t *e, int max_records, int64_t *t_start_ns, int64_t *t_tiles_ns,
-                                      int *frontier, int *chunks, int *count) {
+extern "C" int b40c_enactor_level_log(b40c_enactor_t *e, int max_records, int64_t *t_start_ns, int *frontier,
+                                      int *chunks, int *wchunks, int *count) {
     clear_error();
     if (!e || !count || max_records < 0) return set_error(B40C_ERR_INVALID_VALUE, "invalid argument");
     *count = 0;
@@ -727,14 +747,14 @@ extern "C" int b40c_enactor_level_log(b40c_enactor_t *e, int max_records, int64_
     int n = 0;
     while (n < LEVEL_LOG_CAP && h[n].t_start != 0) {
         n++;
-        if (h[n - 1].frontier == 0u && h[n - 1].chunks == 0u) break;
+        if (h[n - 1].frontier == 0u && h[n - 1].chunks == 0u && h[n - 1].wchunks == 0u) break;
     }
     n = std::min(n, max_records);
     for (int i = 0; i < n; i++) {
         if (t_start_ns) t_start_ns[i] = (int64_t)h[i].t_start;
-        if (t_tiles_ns) t_tiles_ns[i] = (int64_t)h[i].t_tiles;
         if (frontier) frontier[i] = (int)h[i].frontier;
         if (chunks) chunks[i] = (int)h[i].chunks;
+        if (wchunks) wchunks[i] = (int)h[i].wchunks;
     }
     *count = n;
     return B40C_SUCCESS;

@@ -201,28 +201,80 @@ __device__ __forceinline__ void row_range(const BfsParams &p, int v, int &start,
     len = __ldg(p.row_offsets + v + 1) - start;
 }
 
-// Cuts list [start, start+len) of vertex pred into chunks of CH edges aligned
-// to CH-element windows from the 4-aligned start, appended to table.  Returns
-// false when the table is full; the entries it reserved are then written empty
-// and the caller gathers the list another way.  Called by one thread.
-template <int THREADS>
-__device__ __forceinline__ bool push_chunks(const BfsParams &p, int4 *table, unsigned *count, int start, int len,
-                                            int pred) {
-    constexpr int CH = chunk_edges<THREADS>();
-    const int a0 = start & ~3, end = start + len;
-    const unsigned nch = unsigned((end - a0 + CH - 1) / CH);
-    const unsigned base = atomicAdd(count, nch);
-    const unsigned cap = (unsigned)p.chunk_cap;
-    if (base + nch <= cap) {
-        for (unsigned c = 0; c < nch; c++) {
-            const int ws = a0 + int(c) * CH;
-            const int cs = max(ws, start), ce = min(ws + CH, end);
-            table[base + c] = make_int4(cs, ce - cs, pred, 0);
+// Reserves, with one atomicAdd for the whole warp, chunk-table entries for the
+// lists flagged in sel (nc[j] chunks of CH edges for list j of this lane, n in
+// all) and writes their descriptors: windows of CH elements from the list's
+// 4-aligned start, clipped to the list.  Returns sel, or 0 when the table
+// would overflow (the reserved entries are then written empty and the lists
+// stay with their lanes).  Called by all lanes together.
+template <int CH>
+__device__ __forceinline__ unsigned place_tier(int4 *table, unsigned *count, int cap, unsigned sel, int n,
+                                               const int (&nc)[4], const int (&st)[4], const int (&ln)[4],
+                                               const int (&pr)[4]) {
+    const int incl = warp_inclusive_scan(n);
+    const unsigned total = (unsigned)__shfl_sync(FULL, incl, 31);
+    if (total == 0u) return 0u;  // warp-uniform
+    unsigned base = 0;
+    if (lane_id() == 0) base = atomicAdd(count, total);
+    base = __shfl_sync(FULL, base, 0);
+    unsigned my = base + unsigned(incl - n);
+    if ((unsigned long long)base + total <= (unsigned long long)cap) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if ((sel >> j) & 1u) {
+                const int a0 = st[j] & ~3, end = st[j] + ln[j];
+                for (int c = 0; c < nc[j]; c++) {
+                    const int ws = a0 + c * CH;
+                    const int cs = max(ws, st[j]), ce = min(ws + CH, end);
+                    table[my++] = make_int4(cs, ce - cs, pr[j], 0);
+                }
+            }
         }
-        return true;
+        return sel;
     }
-    for (unsigned c = base; c < cap && c < base + nch; c++) table[c] = make_int4(0, 0, 0, 0);
-    return false;
+    for (unsigned c = my; c < (unsigned)cap && c < my + unsigned(n); c++) table[c] = make_int4(0, 0, 0, 0);
+    return 0u;
+}
+
+// Places up to 4 lists per lane (bit j of has marks list j: start st[j],
+// length ln[j], owner pr[j]) for phase q_next by length: lists >= cta_th are
+// cut into CTA chunks, lists >= warp_th into warp chunks; shorter lists stay
+// with their lanes.  Returns the bits of the lists placed in a chunk table.
+// Called by all lanes together.
+template <int THREADS>
+__device__ __forceinline__ unsigned place4(const BfsParams &p, int q_next, unsigned has, const int (&st)[4],
+                                           const int (&ln)[4], const int (&pr)[4]) {
+    constexpr int CH = chunk_edges<THREADS>();
+    unsigned cta = 0, wrp = 0;
+    int ncta = 0, nw = 0, nc[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        nc[j] = 0;
+        if ((has >> j) & 1u) {
+            const int span = st[j] + ln[j] - (st[j] & ~3);
+            if (ln[j] >= p.cta_th) {
+                cta |= 1u << j;
+                nc[j] = (span + CH - 1) / CH;
+                ncta += nc[j];
+            } else if (ln[j] >= p.warp_th) {
+                wrp |= 1u << j;
+                nc[j] = (span + WARP_CHUNK - 1) / WARP_CHUNK;
+                nw += nc[j];
+            }
+        }
+    }
+    if (!__any_sync(FULL, (cta | wrp) != 0u)) return 0u;
+    const int nq = q_next & 1;
+    unsigned placed = place_tier<CH>(p.chunks[nq], &p.ctr->big[q_next & 3], p.chunk_cap, cta, ncta, nc, st, ln, pr);
+    placed |= place_tier<WARP_CHUNK>(p.wchunks[nq], &p.ctr->wch[q_next & 3], p.wchunk_cap, wrp, nw, nc, st, ln, pr);
+    return placed;
+}
+
+// One list per lane: place4 with list 0 only.
+template <int THREADS>
+__device__ __forceinline__ bool place1(const BfsParams &p, int q_next, bool has, int start, int len, int pred) {
+    const int st[4] = {start, 0, 0, 0}, ln[4] = {len, 0, 0, 0}, pr[4] = {pred, 0, 0, 0};
+    return place4<THREADS>(p, q_next, has ? 1u : 0u, st, ln, pr) & 1u;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -281,6 +333,24 @@ __device__ __forceinline__ void gather_chunks(const BfsParams &p, const int4 *ta
     for (; k < n; k += G) {
         int4 nxt = (k + G < n) ? __ldcg(table + k + G) : make_int4(0, 0, 0, 0);
         if (cur.y > 0) gather_list<THREADS>(p.col, p.vec_end, cur.x, cur.y, cur.z, 0u, threadIdx.x, sink, pol);
+        cur = nxt;
+    }
+}
+
+__device__ __forceinline__ int global_warp() { return int(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)); }
+__device__ __forceinline__ int grid_warps() { return int(gridDim.x * (blockDim.x >> 5)); }
+
+// Warp chunk phase: warp w of the grid streams warp chunks w, w + W, ...
+template <class Sink>
+__device__ __forceinline__ void gather_wchunks(const BfsParams &p, const int4 *table, unsigned n, const Sink &sink,
+                                               uint64_t pol) {
+    if (n > (unsigned)p.wchunk_cap) n = p.wchunk_cap;
+    const unsigned W = grid_warps();
+    unsigned k = global_warp();
+    int4 cur = k < n ? __ldcg(table + k) : make_int4(0, 0, 0, 0);
+    for (; k < n; k += W) {
+        int4 nxt = (k + W < n) ? __ldcg(table + k + W) : make_int4(0, 0, 0, 0);
+        if (cur.y > 0) gather_list<32>(p.col, p.vec_end, cur.x, cur.y, cur.z, 0u, lane_id(), sink, pol);
         cur = nxt;
     }
 }
@@ -356,6 +426,11 @@ __device__ __forceinline__ void warp_lists(const BfsParams &p, WarpSmem<MP> &ws,
     }
 }
 
+// Warp tiles handed out per atomic: several when there are many per warp.
+__device__ __forceinline__ unsigned tile_grab(unsigned ntiles) {
+    return ntiles >= unsigned(grid_warps()) * 16u ? TILE_GRAB : 1u;
+}
+
 __device__ __forceinline__ unsigned warp_next_tile(unsigned *steal) {
     unsigned t = 0;
     if (lane_id() == 0) t = atomicAdd(steal, 1u);
@@ -369,18 +444,16 @@ __device__ __forceinline__ unsigned warp_next_tile(unsigned *steal) {
 // ---------------------------------------------------------------------------------------
 
 // Expand-contract: mark and label each neighbour at discovery (label it+1,
-// expand_contract_atomic/cta.cuh:181-218).  A discovered vertex whose list is
-// >= cta_th becomes chunks of the next level; the others go to the next
-// vertex frontier.
+// expand_contract_atomic/cta.cuh:181-218).  A discovered vertex's list becomes
+// CTA or warp chunks of the next level when it is long enough; the other
+// vertices go to the next vertex frontier.
 template <int THREADS, bool MP>
 struct DiscoverSink {
     const BfsParams &p;
     Smem<THREADS, MP> &sm;
     int *q_out;
     unsigned *qlen_out;
-    int4 *chunk_out;
-    unsigned *chunk_count;
-    int label;
+    int label;  // it + 1; also the phase whose inputs the discovered lists become
 
     __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
                                                unsigned) const {
@@ -395,12 +468,7 @@ struct DiscoverSink {
                 row_range(p, u[j], st[j], ln[j]);
             }
         }
-        unsigned enq = disc;
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-            if (((disc >> j) & 1u) && ln[j] >= p.cta_th &&
-                push_chunks<THREADS>(p, chunk_out, chunk_count, st[j], ln[j], u[j]))
-                enq &= ~(1u << j);
+        const unsigned enq = disc & ~place4<THREADS>(p, label, disc, st, ln, u);
         stage4(sm.w[threadIdx.x >> 5], enq, u, q_out, qlen_out, p.qcap, &p.ctr->error);
     }
     __device__ __forceinline__ void drain() const {
@@ -428,8 +496,9 @@ struct PositionSink {
 
 // Contract-expand: cull and label the edge-frontier elements (label it,
 // contract_expand_atomic/cta.cuh:264-304), then expand the survivors at once:
-// lists >= cta_th become chunks of the next level, the rest are copied into
-// the next edge frontier by warp- and scan-based gathers.
+// long lists become CTA or warp chunks of the next level (contracted from the
+// column array there), short ones are copied into the next edge frontier by a
+// scan-based gather.
 template <int THREADS, bool MP>
 struct ContractExpandSink {
     const BfsParams &p;
@@ -465,9 +534,8 @@ struct ContractExpandSink {
             if (g + lane_id() < total) {
                 v = ws.surv[g + lane_id()];
                 row_range(p, v, start, len);
-                if (len >= p.cta_th && push_chunks<THREADS>(p, p.chunks[nq], &p.ctr->big[(it + 1) & 3], start, len, v))
-                    len = 0;
             }
+            if (place1<THREADS>(p, it + 1, len > 0, start, len, v)) len = 0;
             warp_lists<MP, true>(p, ws, out, pol, start, len, v, &p.ctr->qlen[(it + 1) & 3]);
         }
         __syncwarp();
@@ -502,24 +570,23 @@ struct ContractSink {
 // (big[q&3] entries) and writes queue[(q+1)&1] / chunks[(q+1)&1].
 // ---------------------------------------------------------------------------------------
 
-__device__ __forceinline__ int global_warp() { return int(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)); }
-__device__ __forceinline__ int grid_warps() { return int(gridDim.x * (blockDim.x >> 5)); }
-
 // Expand-contract level it: vertex frontier -> discovered vertices labelled it+1.
 template <int THREADS, bool MP>
-__device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, Smem<THREADS, MP> &sm, uint64_t pol) {
+__device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, unsigned nwch, Smem<THREADS, MP> &sm,
+                         uint64_t pol) {
     Counters *c = p.ctr;
     const int nq = (it + 1) & 1;
-    DiscoverSink<THREADS, MP> sink{p, sm, p.queue[nq], &c->qlen[(it + 1) & 3], p.chunks[nq], &c->big[(it + 1) & 3],
-                                   it + 1};
+    DiscoverSink<THREADS, MP> sink{p, sm, p.queue[nq], &c->qlen[(it + 1) & 3], it + 1};
     gather_chunks<THREADS>(p, p.chunks[it & 1], nch, sink, pol);
+    gather_wchunks(p, p.wchunks[it & 1], nwch, sink, pol);
     WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
     const int *q_in = p.queue[it & 1];
     const unsigned ntiles = (L + 31) / 32;
+    const unsigned grab = tile_grab(ntiles);
     for (;;) {
-        const unsigned t0 = warp_next_tile(&c->steal[it & 3]) * TILE_GRAB;
+        const unsigned t0 = warp_next_tile(&c->steal[it & 3]) * grab;
         if (t0 >= ntiles) break;
-        for (unsigned t = t0; t < t0 + TILE_GRAB && t < ntiles; t++) {
+        for (unsigned t = t0; t < t0 + grab && t < ntiles; t++) {
             const unsigned idx = t * 32 + lane_id();
             int v = -1, start = 0, len = 0;
             if (idx < L) {
@@ -558,18 +625,21 @@ __device__ __forceinline__ void edge_tiles(const int *q_in, const int *pq_in, un
 
 // Contract-expand level it (contract_expand_atomic/cta.cuh:573-709).
 template <int THREADS, bool MP>
-__device__ void ce_level(const BfsParams &p, int it, unsigned L, unsigned nch, Smem<THREADS, MP> &sm, uint64_t pol) {
+__device__ void ce_level(const BfsParams &p, int it, unsigned L, unsigned nch, unsigned nwch, Smem<THREADS, MP> &sm,
+                         uint64_t pol) {
     ContractExpandSink<THREADS, MP> sink{p, sm, it, pol};
     gather_chunks<THREADS>(p, p.chunks[it & 1], nch, sink, pol);
+    gather_wchunks(p, p.wchunks[it & 1], nwch, sink, pol);
     edge_tiles<MP>(p.queue[it & 1], p.pred_queue[it & 1], L, sink);
 }
 
 // Two-phase contract, phase qi = 2 * it.
 template <int THREADS, bool MP>
-__device__ void tp_contract(const BfsParams &p, int it, int qi, unsigned L, unsigned nch, Smem<THREADS, MP> &sm,
-                            uint64_t pol) {
+__device__ void tp_contract(const BfsParams &p, int it, int qi, unsigned L, unsigned nch, unsigned nwch,
+                            Smem<THREADS, MP> &sm, uint64_t pol) {
     ContractSink<THREADS, MP> sink{p, sm, p.queue[(qi + 1) & 1], &p.ctr->qlen[(qi + 1) & 3], it};
     gather_chunks<THREADS>(p, p.chunks[qi & 1], nch, sink, pol);
+    gather_wchunks(p, p.wchunks[qi & 1], nwch, sink, pol);
     edge_tiles<MP>(p.queue[qi & 1], p.pred_queue[qi & 1], L, sink);
     sink.drain();
 }
@@ -583,18 +653,18 @@ __device__ void tp_expand(const BfsParams &p, int qi, unsigned L, Smem<THREADS, 
     WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
     const int *q_in = p.queue[qi & 1];
     const unsigned ntiles = (L + 31) / 32;
+    const unsigned grab = tile_grab(ntiles);
     for (;;) {
-        const unsigned t0 = warp_next_tile(&c->steal[qi & 3]) * TILE_GRAB;
+        const unsigned t0 = warp_next_tile(&c->steal[qi & 3]) * grab;
         if (t0 >= ntiles) break;
-        for (unsigned t = t0; t < t0 + TILE_GRAB && t < ntiles; t++) {
+        for (unsigned t = t0; t < t0 + grab && t < ntiles; t++) {
             const unsigned idx = t * 32 + lane_id();
             int v = -1, start = 0, len = 0;
             if (idx < L) {
                 v = ld_cg(q_in + idx);
                 row_range(p, v, start, len);
-                if (len >= p.cta_th && push_chunks<THREADS>(p, p.chunks[nq], &c->big[(qi + 1) & 3], start, len, v))
-                    len = 0;
             }
+            if (place1<THREADS>(p, qi + 1, len > 0, start, len, v)) len = 0;
             warp_lists<MP, true>(p, ws, out, pol, start, len, v, &c->qlen[(qi + 1) & 3]);
         }
     }
@@ -605,16 +675,19 @@ __device__ void tp_expand(const BfsParams &p, int qi, unsigned L, Smem<THREADS, 
 __device__ __forceinline__ void ring_prepare(Counters *c, int q) {
     c->qlen[(q + 2) & 3] = 0u;
     c->big[(q + 2) & 3] = 0u;
+    c->wch[(q + 2) & 3] = 0u;
     c->steal[(q + 1) & 3] = 0u;
 }
 
-__device__ __forceinline__ void log_phase(const BfsParams &p, int idx, unsigned frontier, unsigned chunks) {
+__device__ __forceinline__ void log_phase(const BfsParams &p, int idx, unsigned frontier, unsigned chunks,
+                                          unsigned wchunks) {
     if (p.levels && idx < p.level_cap) {
         LevelRecord r;
         r.t_start = globaltimer_ns();
-        r.t_tiles = 0;
         r.frontier = frontier;
         r.chunks = chunks;
+        r.wchunks = wchunks;
+        r.pad = 0;
         p.levels[idx] = r;
     }
 }
@@ -648,22 +721,40 @@ __device__ __forceinline__ Smem<THREADS, MP> &kernel_smem() {
 // first frontier.  Expand-contract labels and marks the source here (as
 // expand_contract_atomic/kernel.cuh:291-326); the edge-frontier strategies
 // label it when they contract it at iteration 0, with predecessor -2.
-__global__ void search_init_kernel(BfsParams p, int strategy, int mark_pred) {
+__global__ void search_init_kernel(BfsParams p, int strategy, int mark_pred, int cta_chunk) {
     Counters *c = p.ctr;
     unsigned *w = reinterpret_cast<unsigned *>(c);
     constexpr int WORDS = int(offsetof(Counters, sticky) / 4);  // everything but the sticky error
     for (int i = threadIdx.x; i < WORDS; i += blockDim.x) w[i] = 0u;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        c->qlen[0] = 1u;
-        p.queue[0][0] = p.src;
-        if (strategy == STRATEGY_EXPAND_CONTRACT) {
-            p.labels[p.src] = mark_pred ? -2 : 0;
-            p.mask[unsigned(p.src) >> 5] |= 1u << (unsigned(p.src) & 31u);
-        } else if (mark_pred) {
-            p.pred_queue[0][0] = -2;
+    if (threadIdx.x != 0) return;
+    if (strategy == STRATEGY_EXPAND_CONTRACT) {
+        p.labels[p.src] = mark_pred ? -2 : 0;
+        p.mask[unsigned(p.src) >> 5] |= 1u << (unsigned(p.src) & 31u);
+        // The source's list is level 0's input, placed by length like any
+        // discovered vertex's list.
+        int start, len;
+        row_range(p, p.src, start, len);
+        const int a0 = start & ~3, span = start + len - a0;
+        const bool cta = len >= p.cta_th, wrp = !cta && len >= p.warp_th;
+        const int CH = cta ? cta_chunk : WARP_CHUNK;
+        const int nch = (span + CH - 1) / CH;
+        if ((cta || wrp) && nch <= (cta ? p.chunk_cap : p.wchunk_cap)) {
+            int4 *table = cta ? p.chunks[0] : p.wchunks[0];
+            for (int k = 0; k < nch; k++) {
+                const int ws = a0 + k * CH;
+                const int cs = max(ws, start), ce = min(ws + CH, start + len);
+                table[k] = make_int4(cs, ce - cs, p.src, 0);
+            }
+            if (cta) c->big[0] = unsigned(nch);
+            else c->wch[0] = unsigned(nch);
+            return;
         }
+    } else if (mark_pred) {
+        p.pred_queue[0][0] = -2;
     }
+    c->qlen[0] = 1u;
+    p.queue[0][0] = p.src;
 }
 
 // Whether a fused kernel's level loop ends (every CTA decides alike: the
@@ -680,7 +771,7 @@ __device__ __forceinline__ bool stop_level_loop(const BfsParams &p, int level, u
 __device__ __forceinline__ void finish_search(const BfsParams &p, int iteration, int log_idx) {
     if (leader()) {
         p.ctr->iteration = iteration;
-        log_phase(p, log_idx, 0u, 0u);  // end-of-search marker
+        log_phase(p, log_idx, 0u, 0u, 0u);  // end-of-search marker
         atomicOr(&p.ctr->sticky, ld_relaxed_gpu(&p.ctr->error));
     }
 }
@@ -693,14 +784,14 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
     Counters *c = p.ctr;
     int it = 0;
     for (;;) {
-        const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]);
-        if (stop_level_loop(p, it, L + nch)) break;
+        const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]), nw = ld_cg(&c->wch[it & 3]);
+        if (stop_level_loop(p, it, L + nch + nw)) break;
         if (leader()) {
             ring_prepare(c, it);
             c->total_queued += L;
-            log_phase(p, it, L, nch);
+            log_phase(p, it, L, nch, nw);
         }
-        ec_level<THREADS, MP>(p, it, L, nch, sm, pol);
+        ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         it++;
     }
@@ -715,14 +806,14 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
     Counters *c = p.ctr;
     int it = 0;
     for (;;) {
-        const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]);
-        if (stop_level_loop(p, it, L + nch)) break;
+        const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]), nw = ld_cg(&c->wch[it & 3]);
+        if (stop_level_loop(p, it, L + nch + nw)) break;
         if (leader()) {
             ring_prepare(c, it);
             c->total_queued += L;
-            log_phase(p, it, L, nch);
+            log_phase(p, it, L, nch, nw);
         }
-        ce_level<THREADS, MP>(p, it, L, nch, sm, pol);
+        ce_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         it++;
     }
@@ -742,21 +833,21 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
     int it = 0, qi = 0;
     for (;;) {
         unsigned L = ld_cg(&c->qlen[qi & 3]);
-        const unsigned nch = ld_cg(&c->big[qi & 3]);
-        if (stop_level_loop(p, it, L + nch)) break;
+        const unsigned nch = ld_cg(&c->big[qi & 3]), nw = ld_cg(&c->wch[qi & 3]);
+        if (stop_level_loop(p, it, L + nch + nw)) break;
         if (leader()) {
             ring_prepare(c, qi);
             c->total_queued += L;
-            log_phase(p, qi, L, nch);
+            log_phase(p, qi, L, nch, nw);
         }
-        tp_contract<THREADS, MP>(p, it, qi, L, nch, sm, pol);
+        tp_contract<THREADS, MP>(p, it, qi, L, nch, nw, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         qi++;
         L = ld_cg(&c->qlen[qi & 3]);
         if (L == 0u) break;  // no vertex discovered: the reference stops without ++
         if (leader()) {
             ring_prepare(c, qi);
-            log_phase(p, qi, L, 0u);
+            log_phase(p, qi, L, 0u, 0u);
         }
         tp_expand<THREADS, MP>(p, qi, L, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
@@ -773,10 +864,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_level_kernel(
     Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it;
-    const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3];
-    if (L + nch == 0u || p.ctr->error) return;
-    if (leader()) log_phase(p, it, L, nch);
-    ec_level<THREADS, MP>(p, it, L, nch, sm, policy_evict_first());
+    const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3], nw = p.ctr->wch[it & 3];
+    if (L + nch + nw == 0u || p.ctr->error) return;
+    if (leader()) log_phase(p, it, L, nch, nw);
+    ec_level<THREADS, MP>(p, it, L, nch, nw, sm, policy_evict_first());
 }
 
 template <int THREADS, bool MP>
@@ -784,10 +875,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_level_kernel(
     Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it;
-    const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3];
-    if (L + nch == 0u || p.ctr->error) return;
-    if (leader()) log_phase(p, it, L, nch);
-    ce_level<THREADS, MP>(p, it, L, nch, sm, policy_evict_first());
+    const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3], nw = p.ctr->wch[it & 3];
+    if (L + nch + nw == 0u || p.ctr->error) return;
+    if (leader()) log_phase(p, it, L, nch, nw);
+    ce_level<THREADS, MP>(p, it, L, nch, nw, sm, policy_evict_first());
 }
 
 // Two-phase per-level: qi = 2 * it (contract) and 2 * it + 1 (expand).
@@ -796,10 +887,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_contract_kern
     Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it, qi = 2 * it;
-    const unsigned L = p.ctr->qlen[qi & 3], nch = p.ctr->big[qi & 3];
-    if (L + nch == 0u || p.ctr->error) return;
-    if (leader()) log_phase(p, qi, L, nch);
-    tp_contract<THREADS, MP>(p, it, qi, L, nch, sm, policy_evict_first());
+    const unsigned L = p.ctr->qlen[qi & 3], nch = p.ctr->big[qi & 3], nw = p.ctr->wch[qi & 3];
+    if (L + nch + nw == 0u || p.ctr->error) return;
+    if (leader()) log_phase(p, qi, L, nch, nw);
+    tp_contract<THREADS, MP>(p, it, qi, L, nch, nw, sm, policy_evict_first());
 }
 
 template <int THREADS, bool MP>
@@ -809,7 +900,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_expand_kernel
     const int it = p.ctr->cur_it, qi = 2 * it + 1;
     const unsigned L = p.ctr->qlen[qi & 3];
     if (L == 0u || p.ctr->error) return;
-    if (leader()) log_phase(p, qi, L, 0u);
+    if (leader()) log_phase(p, qi, L, 0u, 0u);
     tp_expand<THREADS, MP>(p, qi, L, sm, policy_evict_first());
 }
 
@@ -823,7 +914,7 @@ __global__ void level_control_kernel(BfsParams p, int strategy) {
     if (strategy == STRATEGY_TWO_PHASE) {
         const int qi = 2 * it;
         const unsigned vq = c->qlen[(qi + 1) & 3];                        // contract output
-        const unsigned eq = c->qlen[(qi + 2) & 3] + c->big[(qi + 2) & 3];  // expand output
+        const unsigned eq = c->qlen[(qi + 2) & 3] + c->big[(qi + 2) & 3] + c->wch[(qi + 2) & 3];  // expand output
         c->total_queued += c->qlen[qi & 3];
         if (vq == 0u) {
             c->iteration = it;  // the reference leaves after contract without ++
@@ -839,16 +930,19 @@ __global__ void level_control_kernel(BfsParams p, int strategy) {
         c->qlen[(qi + 4) & 3] = 0u;
         c->big[(qi + 3) & 3] = 0u;
         c->big[(qi + 4) & 3] = 0u;
-        if (!more) log_phase(p, vq == 0u ? qi + 1 : qi + 2, 0u, 0u);
+        c->wch[(qi + 3) & 3] = 0u;
+        c->wch[(qi + 4) & 3] = 0u;
+        if (!more) log_phase(p, vq == 0u ? qi + 1 : qi + 2, 0u, 0u, 0u);
     } else {
-        const unsigned next = c->qlen[(it + 1) & 3] + c->big[(it + 1) & 3];
+        const unsigned next = c->qlen[(it + 1) & 3] + c->big[(it + 1) & 3] + c->wch[(it + 1) & 3];
         c->total_queued += c->qlen[it & 3];
         c->iteration = it + 1;
         more = next != 0u;
         c->steal[(it + 1) & 3] = 0u;
         c->qlen[(it + 2) & 3] = 0u;
         c->big[(it + 2) & 3] = 0u;
-        if (!more) log_phase(p, it + 1, 0u, 0u);
+        c->wch[(it + 2) & 3] = 0u;
+        if (!more) log_phase(p, it + 1, 0u, 0u, 0u);
     }
     if (more && level_limit_hit(it + 1, p.nodes)) {
         c->error |= ERR_LEVEL_LIMIT;
@@ -963,7 +1057,9 @@ static cudaError_t grid_for(const void *fn, int threads, size_t smem, int *grid)
 }
 
 cudaError_t launch_search_init(const BfsParams &p, const KernelConfig &kc, cudaStream_t stream) {
-    search_init_kernel<<<1, 64, 0, stream>>>(p, kc.strategy, kc.mark_pred ? 1 : 0);
+    const int cta_chunk = kc.threads == 128 ? chunk_edges<128>() : kc.threads == 512 ? chunk_edges<512>()
+                                                                                       : chunk_edges<256>();
+    search_init_kernel<<<1, 64, 0, stream>>>(p, kc.strategy, kc.mark_pred ? 1 : 0, cta_chunk);
     return cudaGetLastError();
 }
 

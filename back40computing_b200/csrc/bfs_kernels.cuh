@@ -19,14 +19,15 @@ enum CullFlags : unsigned {
     CULL_HISTORY = 2u,  // per-CTA shared-memory history cache of visited-mask words
 };
 
-// One record per BFS level, written by one thread of the kernel that runs it:
-// %globaltimer at the level start and after its tile phase, the input
-// frontier length and the number of grid-wide chunks it produced.
+// One record per BFS level (per phase for two-phase), written by one thread
+// of the kernel that runs it: %globaltimer at its start, the input frontier
+// queue length and the numbers of CTA and warp chunks it takes as input.
 struct LevelRecord {
     unsigned long long t_start;
-    unsigned long long t_tiles;
     unsigned frontier;
     unsigned chunks;
+    unsigned wchunks;
+    unsigned pad;
 };
 
 // Everything a BFS kernel needs, passed by value.
@@ -37,25 +38,29 @@ struct BfsParams {
     unsigned *mask;          // visited bitmask, bit (v & 31) of word v >> 5
     int *queue[2];           // frontier ping-pong
     int *pred_queue[2];      // predecessor ping-pong (edge frontiers, mark_pred)
-    int4 *chunks[2];         // grid-wide chunks of neighbour lists, ping-pong by phase: {start, len, pred, 0}
+    int4 *chunks[2];         // CTA chunks of neighbour lists, ping-pong by phase: {start, len, pred, 0}
+    int4 *wchunks[2];        // warp chunks of neighbour lists, same layout
     LevelRecord *levels;     // per-level log (level_cap records)
     Counters *ctr;
     unsigned long long wait_ns;      // grid-barrier spin limit
     unsigned long long cond_handle;  // cudaGraphConditionalHandle (per-level graphs)
     long long qcap;                  // elements per frontier queue
-    int chunk_cap;                   // entries of each chunk table
+    int chunk_cap;                   // entries of each CTA chunk table
+    int wchunk_cap;                  // entries of each warp chunk table
     int level_cap;                   // entries of levels
     int vec_end;                     // 16-byte loads of col are safe below this index
     int nodes;
     int src;
-    int warp_th;  // lists >= warp_th are gathered by one warp; shorter ones by a warp scan
-    int cta_th;   // lists >= cta_th are cut into CTA-sized chunks that the whole grid shares
+    int warp_th;  // lists >= warp_th are cut into warp chunks; shorter ones go through a warp scan
+    int cta_th;   // lists >= cta_th are cut into CTA chunks
     unsigned cull_flags;
 };
 
-// Edges per grid-wide chunk: four passes of one 16-byte load per thread of a CTA.
+// Edges per CTA chunk: four passes of one 16-byte load per thread of a CTA.
 template <int THREADS>
 __host__ __device__ constexpr int chunk_edges() { return THREADS * 16; }
+// Edges per warp chunk: four passes of one 16-byte load per lane.
+constexpr int WARP_CHUNK = 512;
 
 struct KernelConfig {
     int strategy;

@@ -121,11 +121,11 @@ int b40c_enactor_last_elapsed_ms(b40c_enactor_t *enactor, float *ms);
 int b40c_enactor_set_stream(b40c_enactor_t *enactor, void *stream);
 /* Tuning policy (the reference's compile-time KernelPolicy, kernel_policy.cuh:61-87,
  * WARP_GATHER_THRESHOLD / CTA_GATHER_THRESHOLD): cta_threads in {128,256,512};
- * lists of at least warp_gather_threshold edges (default 32) are gathered by a
- * warp, shorter ones by a warp prefix sum; lists of at least
- * cta_gather_threshold edges (default 1024) are cut into chunks of
- * 16 * cta_threads edges that every CTA of the grid shares, each chunk
- * gathered by a whole CTA.  cull_flags: bit0 warp-level cull
+ * lists of at least cta_gather_threshold edges (default 1024) are cut into
+ * chunks of 16 * cta_threads edges, each gathered by a whole CTA; lists of at
+ * least warp_gather_threshold edges (default 64) into chunks of 512 edges,
+ * each gathered by one warp; chunks are shared by the whole grid; shorter
+ * lists are gathered by a warp prefix sum.  cull_flags: bit0 warp-level cull
  * (__match_any_sync), bit1 history cull through a per-CTA shared-memory cache
  * of visited-mask words (default: bit1 only).  A 0 keeps a threshold, a -1
  * keeps the cull flags. */
@@ -133,16 +133,16 @@ int b40c_enactor_set_policy(b40c_enactor_t *enactor, int cta_threads,
                             int warp_gather_threshold, int cta_gather_threshold, int cull_flags);
 /* Per-level log (the reference's DEBUG per-level queue lengths,
  * enactor_two_phase.cuh:496-499, with device timestamps): when enabled, each
- * later search records per level its %globaltimer start, the end of its tile
- * phase, the input frontier length and the grid-wide chunk count. */
+ * later search records per level its %globaltimer start, its input frontier
+ * queue length and its input CTA and warp chunk counts. */
 int b40c_enactor_set_level_log(b40c_enactor_t *enactor, int enable);
 /* Copies up to max_records records of the last search (any out pointer may be
  * NULL); *count gets the number copied, the last one being the end marker
- * (frontier 0, chunks 0).  frontier counts queued vertices (or edges for the
- * edge-frontier strategies); vertices whose lists went to grid-wide chunks are
- * counted in chunks instead.  Levels of the two-phase strategy are its phases. */
+ * (all counts 0).  frontier counts queued vertices (edge-frontier strategies:
+ * queued edges); lists long enough to be cut into chunks are counted in
+ * chunks / wchunks instead.  Levels of the two-phase strategy are its phases. */
 int b40c_enactor_level_log(b40c_enactor_t *enactor, int max_records, int64_t *t_start_ns,
-                           int64_t *t_tiles_ns, int *frontier, int *chunks, int *count);
+                           int *frontier, int *chunks, int *wchunks, int *count);
 /* Spin limit of every device-side wait (grid barrier), in microseconds. */
 int b40c_enactor_set_wait_limit_us(b40c_enactor_t *enactor, long long us);
 

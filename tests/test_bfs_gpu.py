@@ -275,9 +275,9 @@ def test_level_log_matches_oracle_levels(cuda_device, oracle, rmat16):
         sizes = [int((ref == d).sum()) for d in range(int(ref.max()) + 1)]
         # one record per level (depths 0..d) plus the end marker
         assert len(log) == len(sizes) + 1
-        assert log[0]["frontier"] == 1
+        assert log[0]["frontier"] + log[0]["chunks"] + log[0]["wchunks"] >= 1
         # vertices of a level are queued or, with long lists, turned into chunks
         for r, n in zip(log[:-1], sizes):
-            assert r["frontier"] <= n and (r["frontier"] == n or r["chunks"] > 0)
-        assert log[-1]["frontier"] == 0 and log[-1]["chunks"] == 0
+            assert r["frontier"] <= n and (r["frontier"] == n or r["chunks"] + r["wchunks"] > 0)
+        assert log[-1]["frontier"] == 0 and log[-1]["chunks"] == 0 and log[-1]["wchunks"] == 0
         assert all(log[i]["start_ns"] <= log[i + 1]["start_ns"] for i in range(len(log) - 1))
