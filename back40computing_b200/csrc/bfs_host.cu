@@ -592,6 +592,9 @@ extern "C" int b40c_enactor_create(int strategy, int instrument, int debug, b40c
     b40c_enactor *e = new (std::nothrow) b40c_enactor();
     if (!e) return set_error(B40C_ERR_MEMORY_ALLOCATION, "enactor allocation");
     e->strategy = strategy;
+    // Measured defaults on R-MAT graphs: expand-contract gathers lists of
+    // 128+ edges with warps, the edge-frontier strategies lists of 64+.
+    if (strategy == B40C_EXPAND_CONTRACT) e->warp_th = 128;
     e->instrument = instrument != 0;
     e->debug = debug != 0;
     cudaError_t ce = cudaGetDevice(&e->device);
