@@ -15,4 +15,5 @@ from .bfs import (  # noqa: F401
     check,
     make_enactor,
 )
-from .graphs import CsrGraph, erdos_renyi, from_coo, grid2d, grid3d, rmat  # noqa: F401
+from .graphs import (CsrGraph, erdos_renyi, from_coo, grid2d, grid3d, read_dimacs, read_market,  # noqa: F401
+                     read_metis, rmat)

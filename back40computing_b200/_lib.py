@@ -32,6 +32,7 @@ SIGNATURES = {
     "b40c_problem_extract_results_async": (c_int, [c_void_p, c_void_p]),
     "b40c_problem_info": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_int64), POINTER(c_void_p),
                                   POINTER(c_void_p), POINTER(c_void_p), POINTER(c_void_p)]),
+    "b40c_problem_device": (c_int, [c_void_p, POINTER(c_int)]),
     "b40c_problem_set_stream": (c_int, [c_void_p, c_void_p]),
     "b40c_enactor_create": (c_int, [c_int, c_int, c_int, POINTER(c_void_p)]),
     "b40c_enactor_destroy": (c_int, [c_void_p]),
@@ -52,6 +53,9 @@ SIGNATURES = {
     "b40c_graph_rmat": (c_int, [c_int, c_int, c_double, c_double, c_double, c_uint64, c_int, POINTER(CsrT)]),
     "b40c_graph_erdos_renyi": (c_int, [c_int, c_double, c_uint64, POINTER(CsrT)]),
     "b40c_graph_from_coo": (c_int, [c_int, c_int64, c_void_p, c_void_p, POINTER(CsrT)]),
+    "b40c_graph_read_market": (c_int, [c_char_p, c_int, POINTER(CsrT)]),
+    "b40c_graph_read_metis": (c_int, [c_char_p, POINTER(CsrT)]),
+    "b40c_graph_read_dimacs": (c_int, [c_char_p, c_int, POINTER(CsrT)]),
     "b40c_csr_free": (c_int, [POINTER(CsrT)]),
     "b40c_graph_sample_sources": (c_int, [POINTER(CsrT), c_int, c_uint64, c_void_p]),
     "b40c_debug_barrier_timeout": (c_int, [c_int, c_longlong]),

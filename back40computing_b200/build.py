@@ -18,7 +18,8 @@ INCLUDE = ROOT / "include"
 LIB = PKG / "libb40c_bfs.so"
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["bfs_kernels.cu", "bfs_host.cu", "graph_gen.cpp"]
+SOURCES = ["bfs_kernels.cu", "bfs_host.cu", "graph_gen.cpp", "graph_io.cpp"]
+DRIVER = PKG / "test_bfs"
 
 
 def _nvcc() -> str:
@@ -40,6 +41,8 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> Path:
     deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [
         INCLUDE / "b40c_bfs.h"]
     if not force and not _stale(LIB, deps):
+        if _stale(DRIVER, [LIB, CSRC / "test_bfs_main.cpp"] + list((INCLUDE / "b40c").rglob("*.hpp"))):
+            build_driver(verbose=verbose)
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [_nvcc(), *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", "--shared",
@@ -50,7 +53,20 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> Path:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True, cwd=str(ROOT))
     os.replace(tmp, LIB)
+    build_driver(verbose=verbose)
     return LIB
+
+
+def build_driver(verbose: bool = False) -> Path:
+    """The test_bfs command-line driver: plain C++ over the C ABI (no nvcc)."""
+    src = CSRC / "test_bfs_main.cpp"
+    cuda_inc = Path(_nvcc()).resolve().parent.parent / "include"
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", f"-I{INCLUDE}", f"-I{cuda_inc}", "-o", str(DRIVER),
+           str(src), f"-L{PKG}", "-lb40c_bfs", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True, cwd=str(ROOT))
+    return DRIVER
 
 
 if __name__ == "__main__":

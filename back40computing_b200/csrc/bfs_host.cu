@@ -575,6 +575,13 @@ extern "C" int b40c_problem_info(b40c_problem_t *p, int64_t *nodes, int64_t *edg
     return B40C_SUCCESS;
 }
 
+extern "C" int b40c_problem_device(b40c_problem_t *p, int *device) {
+    clear_error();
+    if (!p || !device) return set_error(B40C_ERR_INVALID_VALUE, "NULL argument");
+    *device = p->device;
+    return B40C_SUCCESS;
+}
+
 extern "C" int b40c_problem_set_stream(b40c_problem_t *p, void *stream) {
     clear_error();
     if (!p) return set_error(B40C_ERR_INVALID_VALUE, "NULL problem");

@@ -111,3 +111,18 @@ def from_coo(nodes: int, rows, cols) -> CsrGraph:
         raise GraphError("rows and cols differ in length")
     return _call(lib().b40c_graph_from_coo, nodes, r.shape[0], r.ctypes.data_as(ctypes.c_void_p),
                  cc.ctypes.data_as(ctypes.c_void_p), name="coo")
+
+
+def read_market(path, undirected: bool = False) -> CsrGraph:
+    """Matrix Market coordinate file (entry "a b" is the edge b-1 -> a-1)."""
+    return _call(lib().b40c_graph_read_market, str(path).encode(), int(undirected), name=f"market:{path}")
+
+
+def read_metis(path) -> CsrGraph:
+    """METIS adjacency file (1-based neighbour lists, both directions stored)."""
+    return _call(lib().b40c_graph_read_metis, str(path).encode(), name=f"metis:{path}")
+
+
+def read_dimacs(path, undirected: bool = False) -> CsrGraph:
+    """DIMACS shortest-path arc file ("p" line, "a u v w" arcs)."""
+    return _call(lib().b40c_graph_read_dimacs, str(path).encode(), int(undirected), name=f"dimacs:{path}")

@@ -60,6 +60,7 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--verify", type=int, default=2, help="sources checked against the oracle")
+    ap.add_argument("--sources", type=int, default=NUM_SOURCES, help="sources per step (64 for the bench line)")
     return ap.parse_args()
 
 
@@ -79,6 +80,18 @@ def measured_peaks():
         d = json.loads(p.read_text())
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def measured_traffic(scale):
+    """DRAM bytes per launch of the headline kernel from the committed ncu
+    summary (profiles/ec_fused_rmat21_full.md), scaled there to scale 22."""
+    prof = ROOT / "profiles" / "ec_fused_rmat21_full.md"
+    if scale != 22 or not prof.exists():
+        return None
+    for line in prof.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch_rmat22:"):
+            return float(line.split(":", 1)[1])
+    return None
 
 
 class ClockSampler:
@@ -225,7 +238,8 @@ def main():
     dev = torch.device("cuda", local)
 
     g = make_graph(args.scale, args.edge_factor)
-    sources = g.sample_sources(NUM_SOURCES, 2 + 1000 * rank)
+    sources = g.sample_sources(args.sources, 2 + 1000 * rank)
+    nsrc = len(sources)
     deg = g.degrees().astype(np.int64)
     strategies = [int(s) for s in args.strategies.split(",") if s.strip()]
     if HEADLINE not in strategies:
@@ -245,8 +259,8 @@ def main():
         en = b.make_enactor(strat)
         en.set_stream(stream.cuda_stream)
         ft = en.GetFrontierType()
-        E = np.zeros(NUM_SOURCES, np.int64)
-        V = np.zeros(NUM_SOURCES, np.int64)
+        E = np.zeros(nsrc, np.int64)
+        V = np.zeros(nsrc, np.int64)
         # Warm-up steps; the first one also measures E and V per source and checks labels.
         for w in range(max(1, args.warmup)):
             for i, s in enumerate(sources):
@@ -262,8 +276,8 @@ def main():
                         verified.append((strat, int(s), lab))
             b.check(en.Sync())
         # Timed steps.
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps * NUM_SOURCES)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps * NUM_SOURCES)]
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps * nsrc)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps * nsrc)]
         t_start = torch.cuda.Event(enable_timing=True)
         t_end = torch.cuda.Event(enable_timing=True)
         barrier()
@@ -301,7 +315,7 @@ def main():
             "alg_gbs": float(bytes_alg.sum() * args.steps / (np.sum(kern_ms) / 1e3) / 1e9),
             "edges_visited_mean": float(E.mean()),
             "vertices_visited_mean": float(V.mean()),
-            "launches": 2 * args.steps * NUM_SOURCES,
+            "launches": 2 * args.steps * nsrc,
             "clocks": clk,
         }
         del en
@@ -326,7 +340,7 @@ def main():
         en = b.make_enactor(HEADLINE)
         en.set_stream(stream.cuda_stream)
         ft = en.GetFrontierType()
-        E = np.zeros(NUM_SOURCES, np.int64)
+        E = np.zeros(nsrc, np.int64)
 
         def e2e_step(record):
             prob = b.CsrProblem(False)
@@ -354,8 +368,8 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             secs = float(t.item())
         e2e = {"value": float(E.sum()) * args.steps * world / secs / 1e9, "unit": UNIT,
-               "h2d_bytes_per_step": int(4 * (g.nodes + 1) + 4 * g.edges + 4 * NUM_SOURCES),
-               "d2h_bytes_per_step": int(4 * g.nodes * NUM_SOURCES),
+               "h2d_bytes_per_step": int(4 * (g.nodes + 1) + 4 * g.edges + 4 * nsrc),
+               "d2h_bytes_per_step": int(4 * g.nodes * nsrc),
                "ms_per_step": secs / args.steps * 1e3}
         del en
 
@@ -375,16 +389,13 @@ def main():
         return
     peak, peak_kind = measured_peaks()
     head = results[HEADLINE]
-    traffic = None
-    prof = ROOT / "profiles" / "traffic_rmat22.json"
-    if prof.exists():
-        traffic = json.loads(prof.read_text()).get(STRATEGY_NAMES[HEADLINE])
+    traffic = measured_traffic(args.scale)
     line = {
         "metric": METRIC, "value": head["gteps"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded R-MAT, 64 sources)",
         "config": {"workload": f"BFS rmat-s{args.scale}-ef{args.edge_factor} (a=.57 b=.19 c=.19), "
-                               f"64 sources/step, strategy {STRATEGY_NAMES[HEADLINE]} "
+                               f"{nsrc} sources/step, strategy {STRATEGY_NAMES[HEADLINE]} "
                                f"{'fused' if args.variant == 1 else 'iterative'}",
                    "nodes": g.nodes, "edges": g.edges, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (column indices %.0f MB)" % (4 * g.edges / 1e6)},
@@ -393,7 +404,7 @@ def main():
                      "alg_bytes_per_launch": head["alg_bytes_per_search"],
                      "kernel_ms_mean": head["kernel_ms_mean"]},
         "strategies": {STRATEGY_NAMES[s]: {k: v for k, v in r.items() if k != "clocks"} for s, r in results.items()},
-        "gpu_launches": sum(r["launches"] for r in results.values()),
+        "gpu_launches": head["launches"],
         "clocks": head["clocks"],
         "e2e": e2e,
         "cpu_baseline": cpu,

@@ -86,6 +86,8 @@ int b40c_problem_extract_results_async(b40c_problem_t *problem, int *h_labels);
 int b40c_problem_info(b40c_problem_t *problem, int64_t *nodes, int64_t *edges,
                       void **d_row_offsets, void **d_column_indices,
                       void **d_labels, void **d_visited_mask);
+/* CUDA device ordinal the problem lives on (GraphSlice::gpu, :103). */
+int b40c_problem_device(b40c_problem_t *problem, int *device);
 /* Stream (a cudaStream_t) for every later operation on this problem; NULL = the
  * library's own stream for this problem. */
 int b40c_problem_set_stream(b40c_problem_t *problem, void *stream);
@@ -170,6 +172,13 @@ int b40c_graph_erdos_renyi(int nodes, double p, uint64_t seed, b40c_csr_t *out);
 /* CsrGraph::FromCoo (csr_graph.cuh:108-152): stable sort by row. */
 int b40c_graph_from_coo(int nodes, int64_t num_edges, const int *rows,
                         const int *cols, b40c_csr_t *out);
+/* Graph files (b40c/graph/builder/market.cuh, metis.cuh, dimacs.cuh; the
+ * BuildMarketGraph / BuildMetisGraph / BuildDimacsGraph readers used by
+ * test/bfs/test_bfs.cu:981-1036).  Matrix Market entry "a b" is the edge
+ * b-1 -> a-1 as the reference reads it; undirected adds each reverse edge. */
+int b40c_graph_read_market(const char *path, int undirected, b40c_csr_t *out);
+int b40c_graph_read_metis(const char *path, b40c_csr_t *out);
+int b40c_graph_read_dimacs(const char *path, int undirected, b40c_csr_t *out);
 /* Frees the arrays of a b40c_csr_t filled by this library. */
 int b40c_csr_free(b40c_csr_t *csr);
 /* num_sources vertex ids drawn uniformly (with a seeded RNG) among vertices of degree > 0. */

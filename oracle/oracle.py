@@ -106,6 +106,9 @@ class ReferenceBfs:
         L.ref_build_random.argtypes = [c_int, c_int, c_int, c_uint] + gp
         L.ref_build_rmat.argtypes = [c_int, c_int, c_int, c_double, c_double, c_double, c_uint] + gp
         L.ref_from_coo.argtypes = [c_int, c_int, c_void_p, c_void_p] + gp
+        L.ref_read_market.argtypes = [ctypes.c_char_p, c_int] + gp
+        L.ref_read_metis.argtypes = [ctypes.c_char_p] + gp
+        L.ref_read_dimacs.argtypes = [ctypes.c_char_p, c_int] + gp
         L.ref_free.argtypes = [c_void_p]
         L.ref_free.restype = None
 
@@ -152,3 +155,12 @@ class ReferenceBfs:
         r = np.ascontiguousarray(rows, dtype=np.int32)
         cc = np.ascontiguousarray(cols, dtype=np.int32)
         return self._graph(self.lib.ref_from_coo, nodes, r.shape[0], _p(r), _p(cc))
+
+    def read_market(self, path, undirected):
+        return self._graph(self.lib.ref_read_market, str(path).encode(), int(undirected))
+
+    def read_metis(self, path):
+        return self._graph(self.lib.ref_read_metis, str(path).encode())
+
+    def read_dimacs(self, path, undirected):
+        return self._graph(self.lib.ref_read_dimacs, str(path).encode(), int(undirected))

@@ -152,3 +152,29 @@ extern "C" int ref_from_coo(int nodes, int num_edges, const int *rows, const int
 }
 
 extern "C" void ref_free(void *p) { free(p); }
+
+/* The reference's graph-file readers (b40c/graph/builder/market.cuh,
+ * metis.cuh, dimacs.cuh), for pinning this package's readers. */
+extern "C" int ref_read_market(const char *path, int undirected, int64_t *n_out, int64_t *m_out, int **row_offsets,
+                               int **column_indices) {
+    Quiet q;
+    Graph g(false);
+    if (b40c::graph::builder::BuildMarketGraph<false>((char *)path, g, undirected != 0)) return -1;
+    return export_graph(g, n_out, m_out, row_offsets, column_indices);
+}
+
+extern "C" int ref_read_metis(const char *path, int64_t *n_out, int64_t *m_out, int **row_offsets,
+                              int **column_indices) {
+    Quiet q;
+    Graph g(false);
+    if (b40c::graph::builder::BuildMetisGraph<false>((char *)path, g)) return -1;
+    return export_graph(g, n_out, m_out, row_offsets, column_indices);
+}
+
+extern "C" int ref_read_dimacs(const char *path, int undirected, int64_t *n_out, int64_t *m_out, int **row_offsets,
+                               int **column_indices) {
+    Quiet q;
+    Graph g(false);
+    if (b40c::graph::builder::BuildDimacsGraph<false>((char *)path, g, undirected != 0, 0)) return -1;
+    return export_graph(g, n_out, m_out, row_offsets, column_indices);
+}
