@@ -59,6 +59,17 @@ SIGNATURES = {
     "b40c_csr_free": (c_int, [POINTER(CsrT)]),
     "b40c_graph_sample_sources": (c_int, [POINTER(CsrT), c_int, c_uint64, c_void_p]),
     "b40c_debug_barrier_timeout": (c_int, [c_int, c_longlong]),
+    "b40c_batch_create": (c_int, [c_int, POINTER(c_void_p)]),
+    "b40c_batch_destroy": (c_int, [c_void_p]),
+    "b40c_batch_add_graph": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, POINTER(c_int)]),
+    "b40c_batch_set_policy": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
+    "b40c_batch_set_stream": (c_int, [c_void_p, c_void_p]),
+    "b40c_batch_run": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int]),
+    "b40c_batch_run_async": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int]),
+    "b40c_batch_sync": (c_int, [c_void_p]),
+    "b40c_batch_extract": (c_int, [c_void_p, c_int, c_void_p]),
+    "b40c_batch_search_depth": (c_int, [c_void_p, c_int, POINTER(c_int)]),
+    "b40c_batch_last_elapsed_ms": (c_int, [c_void_p, POINTER(c_float)]),
 }
 
 _lib = None

@@ -42,7 +42,6 @@
 namespace b40c_b200 {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int VCACHE = 2048;     // history cache: visited-mask words held per CTA
 constexpr int WINDOW = 128;      // per-warp scan-gather window (4 per lane)
 
 // Resident CTAs per SM requested from ptxas: 40 warps per SM (48 registers
@@ -73,10 +72,6 @@ struct Smem {
 // Culling and enqueueing, 4 elements per thread
 // ---------------------------------------------------------------------------------------
 
-// Slot of mask word w in the CTA's history cache (multiplicative hash, so the
-// low-popcount word indices of skewed graphs spread over the slots).
-__device__ __forceinline__ unsigned vcache_slot(unsigned w) { return (w * 2654435761u) >> (32 - 11); }
-static_assert(VCACHE == 2048, "vcache_slot takes 11 bits");
 
 // Exact test-and-set of the visited bits of up to 4 vertices (bit j of valid
 // marks u[j]).  Returns the bits of the vertices this thread claimed first.
@@ -280,47 +275,6 @@ __device__ __forceinline__ bool place1(const BfsParams &p, int q_next, bool has,
 // ---------------------------------------------------------------------------------------
 // Gather strategies
 // ---------------------------------------------------------------------------------------
-
-__device__ __forceinline__ int4 load_col4(const int *col, int vec_end, int e, int end, uint64_t pol) {
-    int4 c = make_int4(-1, -1, -1, -1);
-    if (e < end) {
-        if (e + 4 <= vec_end) {
-            c = ldg_stream_v4(col + e, pol);
-        } else {  // unpadded (host-mapped) array tail: scalar loads inside the list
-            c.x = __ldg(col + e);
-            if (e + 1 < end) c.y = __ldg(col + e + 1);
-            if (e + 2 < end) c.z = __ldg(col + e + 2);
-            if (e + 3 < end) c.w = __ldg(col + e + 3);
-        }
-    }
-    return c;
-}
-
-// The calling group (CTA of THREADS, or one warp with GROUP = 32) streams the
-// list [s, s+l) with 16-byte loads starting from the 4-aligned index s & ~3;
-// each pass covers GROUP*4 elements; the next pass's load is issued before the
-// current elements are processed.  Elements outside [s, s+l) are masked off.
-// No group-wide barrier: every warp of the group proceeds on its own.
-template <int GROUP, class Sink>
-__device__ __forceinline__ void gather_list(const int *col, int vec_end, int s, int l, int pred, unsigned out,
-                                            int rank, const Sink &sink, uint64_t pol) {
-    const int end = s + l;
-    int e = (s & ~3) + rank * 4;
-    int4 cur = load_col4(col, vec_end, e, end, pol);
-    const int pv[4] = {pred, pred, pred, pred};
-    for (int base = s & ~3; base < end; base += GROUP * 4) {
-        const int en = e + GROUP * 4;
-        int4 nxt = load_col4(col, vec_end, en, end, pol);
-        unsigned valid = 0;
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-            if (e + j >= s && e + j < end) valid |= 1u << j;
-        const int u[4] = {cur.x, cur.y, cur.z, cur.w};
-        sink(valid, u, pv, out + unsigned(e - s));
-        cur = nxt;
-        e = en;
-    }
-}
 
 // Grid-wide chunk phase: CTA b streams chunks b, b + G, b + 2G, ... of table.
 template <int THREADS, class Sink>

@@ -184,6 +184,36 @@ int b40c_csr_free(b40c_csr_t *csr);
 /* num_sources vertex ids drawn uniformly (with a seeded RNG) among vertices of degree > 0. */
 int b40c_graph_sample_sources(const b40c_csr_t *csr, int num_sources, uint64_t seed, int *sources);
 
+/* ---- batched searches (no reference counterpart: the reference runs one
+ * search per EnactSearch) -------------------------------------------------
+ * Many (graph, source) searches over resident graphs run in one persistent
+ * launch (expand-contract); each search has its own labels.  A batch can be
+ * captured into a CUDA graph and replayed when run again unchanged. */
+typedef struct b40c_batch b40c_batch_t;
+int b40c_batch_create(int mark_predecessors, b40c_batch_t **out);
+int b40c_batch_destroy(b40c_batch_t *batch);
+/* Uploads a graph (validated like FromHostProblem); *graph_id names it. */
+int b40c_batch_add_graph(b40c_batch_t *batch, int nodes, int edges, const int *h_column_indices,
+                         const int *h_row_offsets, int *graph_id);
+/* Same knobs as b40c_enactor_set_policy (expand-contract defaults). */
+int b40c_batch_set_policy(b40c_batch_t *batch, int cta_threads, int warp_gather_threshold,
+                          int cta_gather_threshold, int cull_flags);
+int b40c_batch_set_stream(b40c_batch_t *batch, void *stream);
+/* Runs search i from sources[i] on graph graph_ids[i], i < num_searches, and
+ * waits.  use_cuda_graph captures the launch sequence (pool clears, admission
+ * kernel, persistent kernel) once and replays it for identical batches. */
+int b40c_batch_run(b40c_batch_t *batch, int num_searches, const int *graph_ids, const int *sources,
+                   int use_cuda_graph);
+int b40c_batch_run_async(b40c_batch_t *batch, int num_searches, const int *graph_ids,
+                         const int *sources, int use_cuda_graph);
+int b40c_batch_sync(b40c_batch_t *batch);
+/* Labels of search i of the last batch (its graph's node count entries). */
+int b40c_batch_extract(b40c_batch_t *batch, int search, int *h_labels);
+/* search_depth of search i as the expand-contract enactor reports it. */
+int b40c_batch_search_depth(b40c_batch_t *batch, int search, int *depth);
+/* Device time of the last batch, CUDA events around its launch sequence. */
+int b40c_batch_last_elapsed_ms(b40c_batch_t *batch, float *ms);
+
 /* ---- failure detection -------------------------------------------------- */
 /* Runs the bounded grid barrier on a cooperative grid with one arrival that
  * never comes: every block gives up after wait_limit_us and the call returns

@@ -1,0 +1,85 @@
+"""Batched multi-search BFS: every search of a batch must equal its own
+single search (bit-exact depth labels against the oracle)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mixed_graphs():
+    import back40computing_b200 as b
+    return [b.rmat(10, 8, seed=1), b.rmat(13, 16, seed=2), b.erdos_renyi(3000, 16 / 2999, seed=3),
+            b.grid2d(40), b.rmat(14, 24, seed=4), b.grid3d(12)]
+
+
+def _check(oracle, batch, graphs, gids, srcs, mark_pred=False):
+    for i, (g, s) in enumerate(zip(gids, srcs)):
+        ref, _ = oracle.bfs(graphs[g], int(s))
+        got = batch.labels(i)
+        if mark_pred:
+            assert oracle.check_predecessors(graphs[g], got, ref)[0] == -1, i
+        else:
+            assert oracle.first_mismatch(got, ref) == -1, (i, g, s)
+            assert batch.search_depth(i) == int(ref.max())
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_batch_matches_oracle(cuda_device, oracle, mixed_graphs, use_graph):
+    from back40computing_b200.batch import BfsBatch
+    batch = BfsBatch()
+    ids = [batch.add_graph(g) for g in mixed_graphs]
+    gids, srcs = [], []
+    for gid, g in zip(ids, mixed_graphs):
+        for s in g.sample_sources(5, 7 + gid):
+            gids.append(gid)
+            srcs.append(int(s))
+    batch.run(gids, srcs, use_cuda_graph=use_graph)
+    _check(oracle, batch, mixed_graphs, gids, srcs)
+    # replay the same batch, then a different one
+    batch.run(gids, srcs, use_cuda_graph=use_graph)
+    _check(oracle, batch, mixed_graphs, gids, srcs)
+    gids2, srcs2 = gids[::-1], [int(mixed_graphs[g].sample_sources(1, 99 + i)[0]) for i, g in enumerate(gids[::-1])]
+    batch.run(gids2, srcs2, use_cuda_graph=use_graph)
+    _check(oracle, batch, mixed_graphs, gids2, srcs2)
+
+
+def test_batch_predecessors_valid(cuda_device, oracle, mixed_graphs):
+    from back40computing_b200.batch import BfsBatch
+    batch = BfsBatch(mark_predecessors=True)
+    ids = [batch.add_graph(g) for g in mixed_graphs]
+    gids = ids * 3
+    srcs = [int(mixed_graphs[g].sample_sources(1, 5 + k)[0]) for k, g in enumerate(gids)]
+    batch.run(gids, srcs)
+    _check(oracle, batch, mixed_graphs, gids, srcs, mark_pred=True)
+
+
+@pytest.mark.parametrize("policy", [dict(cta_threads=128), dict(cta_threads=512),
+                                    dict(warp_gather_threshold=8, cta_gather_threshold=64),
+                                    dict(warp_gather_threshold=100000, cta_gather_threshold=100000),
+                                    dict(cull_flags=0), dict(cull_flags=3)],
+                         ids=lambda p: ",".join(f"{k}={v}" for k, v in p.items()))
+def test_batch_policies(cuda_device, oracle, mixed_graphs, policy):
+    from back40computing_b200.batch import BfsBatch
+    batch = BfsBatch()
+    batch.set_policy(**policy)
+    ids = [batch.add_graph(g) for g in mixed_graphs]
+    gids = ids * 2
+    srcs = [int(mixed_graphs[g].sample_sources(1, 11 + k)[0]) for k, g in enumerate(gids)]
+    batch.run(gids, srcs)
+    _check(oracle, batch, mixed_graphs, gids, srcs)
+
+
+def test_batch_edge_cases(cuda_device, oracle):
+    import back40computing_b200 as b
+    from back40computing_b200.batch import BfsBatch
+    graphs = [b.from_coo(1, [], []), b.from_coo(5, [1, 2], [2, 1]),
+              b.from_coo(20001, [0] * 20000 + list(range(1, 20001)), list(range(1, 20001)) + [0] * 20000)]
+    batch = BfsBatch()
+    ids = [batch.add_graph(g) for g in graphs]
+    gids = [ids[0], ids[1], ids[1], ids[2], ids[2]]
+    srcs = [0, 0, 1, 0, 777]
+    batch.run(gids, srcs)
+    _check(oracle, batch, graphs, gids, srcs)
