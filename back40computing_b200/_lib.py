@@ -70,6 +70,13 @@ SIGNATURES = {
     "b40c_batch_extract": (c_int, [c_void_p, c_int, c_void_p]),
     "b40c_batch_search_depth": (c_int, [c_void_p, c_int, POINTER(c_int)]),
     "b40c_batch_last_elapsed_ms": (c_int, [c_void_p, POINTER(c_float)]),
+    "b40c_server_create": (c_int, [c_int, c_int, c_longlong, POINTER(c_void_p)]),
+    "b40c_server_destroy": (c_int, [c_void_p]),
+    "b40c_server_add_graph": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, POINTER(c_int)]),
+    "b40c_server_set_policy": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int]),
+    "b40c_server_run_trace": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                      POINTER(c_double)]),
+    "b40c_server_stats": (c_int, [c_void_p, POINTER(c_longlong), POINTER(c_longlong)]),
 }
 
 _lib = None

@@ -51,7 +51,8 @@ struct alignas(256) Counters {
     int cur_it;          // current iteration for per-level (graph-driven) kernels
     unsigned done;       // 1 once the search has finished (per-level variants)
     unsigned long long total_queued;  // sum of frontier lengths (instrumented)
-    unsigned pad_e[58];
+    unsigned retired[4];  // multi-search: searches retired at the start of level q, at [q&3]
+    unsigned pad_e[54];
     unsigned bar_count;  // grid barrier
     unsigned bar_gen;
     unsigned pad_g[61];

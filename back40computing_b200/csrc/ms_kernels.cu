@@ -363,19 +363,24 @@ __device__ void ms_level(const MsParams &p, int L, unsigned nq_in, unsigned nch,
 // One CTA retires the slots without input for level L and clears the alive
 // entries level L+1 will fill.  final_sweep: the batch has no work left, so
 // every active slot ends here.
+// Retired searches are counted in Counters::retired[L&3] (zeroed at level L-1).
 __device__ void ms_bookkeeping(const MsParams &p, int L, bool final_sweep) {
     const unsigned char *in = p.alive + size_t(L & 3) * size_t(p.nslots);
     unsigned char *clear = p.alive + size_t((L + 2) & 3) * size_t(p.nslots);
     const unsigned long long now = globaltimer_ns();
+    unsigned retired = 0;
+    if (threadIdx.x == 0) p.ctr->retired[(L + 1) & 3] = 0u;
     for (int s = threadIdx.x; s < p.nslots; s += blockDim.x) {
         MsSlotState &st = p.state[s];
         if (st.active && (final_sweep || !in[s])) {
             st.active = 0;
             st.done_levels = L - load_slot(p, s).start_level;
             st.done_ns = now;
+            retired++;
         }
         clear[s] = 0;
     }
+    if (retired) atomicAdd(&p.ctr->retired[L & 3], retired);
 }
 
 __device__ __forceinline__ void ms_ring_prepare(Counters *c, int q) {
@@ -396,11 +401,14 @@ __global__ void __launch_bounds__(THREADS, MS_MIN_BLOCKS(THREADS)) ms_fused_kern
     Counters *c = p.ctr;
     int L = c->cur_it;
     const int L_end = p.max_levels > 0 ? L + p.max_levels : 0x7fffffff;
+    const int L_first = L;
     for (;;) {
         const unsigned nq = ld_cg(&c->qlen[L & 3]), nch = ld_cg(&c->big[L & 3]), nw = ld_cg(&c->wch[L & 3]);
+        // Searches retired at the previous level's start (final before the barrier).
+        const bool retired_before = L > L_first && ld_cg(&c->retired[(L - 1) & 3]) != 0u;
         const bool empty = nq + nch + nw == 0u;
         if (blockIdx.x == 0) ms_bookkeeping(p, L, empty);
-        if (empty || L >= L_end) break;
+        if (empty || L >= L_end || (p.stop_on_retire && retired_before)) break;
         if (leader()) {
             ms_ring_prepare(c, L);
             if (p.levels && L < p.level_cap) {
@@ -472,6 +480,17 @@ __global__ void ms_admit_kernel(MsParams p, const int2 *slot_src, int count, int
     else atomicOr(&c->error, ERR_OVERFLOW);
 }
 
+// One CTA per slot: labels := -1 and visited-mask words := 0.
+__global__ void ms_clear_kernel(MsParams p, const int *slots, int count) {
+    if ((int)blockIdx.x >= count) return;
+    const MsSlot d = load_slot(p, slots[blockIdx.x]);
+    int *labels = p.labels + d.label_off;
+    unsigned *mask = p.mask + d.mask_off;
+    const int words = (d.nodes + 31) / 32;
+    for (int i = threadIdx.x; i < d.nodes; i += blockDim.x) labels[i] = -1;
+    for (int i = threadIdx.x; i < words; i += blockDim.x) mask[i] = 0u;
+}
+
 typedef void (*MsKernelFn)(MsParams);
 
 template <bool MP>
@@ -519,6 +538,12 @@ cudaError_t ms_launch(const MsParams &p, const MsKernelConfig &kc, int grid, cud
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, fn, p);
+}
+
+cudaError_t ms_clear_slots(const MsParams &p, const int *d_slots, int count, cudaStream_t stream) {
+    if (count <= 0) return cudaSuccess;
+    ms_clear_kernel<<<count, 512, 0, stream>>>(p, d_slots, count);
+    return cudaGetLastError();
 }
 
 cudaError_t ms_admit(const MsParams &p, const MsKernelConfig &kc, const int2 *d_slot_src, int count,

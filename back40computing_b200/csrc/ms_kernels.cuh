@@ -53,6 +53,7 @@ struct MsParams {
     int cta_th;
     unsigned cull_flags;
     int max_levels;  // levels to run in this launch before returning (<= 0: until no work)
+    int stop_on_retire;  // return at the level after one where a search retired
 };
 
 struct MsKernelConfig {
@@ -65,6 +66,8 @@ cudaError_t ms_grid_limit(const MsKernelConfig &kc, int *grid);
 // Cooperative launch: runs levels from Counters::cur_it until no search has
 // work or max_levels levels ran; leaves the ring ready to continue.
 cudaError_t ms_launch(const MsParams &p, const MsKernelConfig &kc, int grid, cudaStream_t stream);
+// Clears labels (to -1) and visited-mask words (to 0) of the given slots.
+cudaError_t ms_clear_slots(const MsParams &p, const int *d_slots, int count, cudaStream_t stream);
 // Admits searches: for each (slot, source) pair labels and marks the source
 // and places its list as input of level Counters::cur_it.  The slots' labels
 // and masks must be cleared beforehand.

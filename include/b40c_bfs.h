@@ -214,6 +214,30 @@ int b40c_batch_search_depth(b40c_batch_t *batch, int search, int *depth);
 /* Device time of the last batch, CUDA events around its launch sequence. */
 int b40c_batch_last_elapsed_ms(b40c_batch_t *batch, float *ms);
 
+/* ---- serving (no reference counterpart) ----------------------------------
+ * BFS queries over resident graphs with continuous batching: queries are
+ * admitted into up to max_slots concurrent searches while the HBM budget's
+ * label, mask, frontier and chunk pools allow, run together in epochs of the
+ * persistent multi-search kernel, and retire as they finish, freeing room
+ * for the queries that arrived meanwhile. */
+typedef struct b40c_server b40c_server_t;
+int b40c_server_create(int mark_predecessors, int max_slots, long long hbm_budget_bytes, b40c_server_t **out);
+int b40c_server_destroy(b40c_server_t *server);
+int b40c_server_add_graph(b40c_server_t *server, int nodes, int edges, const int *h_column_indices,
+                          const int *h_row_offsets, int *graph_id);
+/* Policy as b40c_batch_set_policy, plus the level cap of one epoch (0 keeps). */
+int b40c_server_set_policy(b40c_server_t *server, int cta_threads, int warp_gather_threshold,
+                           int cta_gather_threshold, int cull_flags, int epoch_levels);
+/* Replays a trace in real time: query i (graph_ids[i], sources[i]) arrives
+ * arrival_us[i] microseconds after the call (non-decreasing).  Returns when
+ * every query finished; latency_us[i] = completion - arrival on the host
+ * clock; labels_out[i], when labels_out and it are non-NULL, receives query
+ * i's labels; *makespan_us (may be NULL) the time of the last completion. */
+int b40c_server_run_trace(b40c_server_t *server, int n, const int *graph_ids, const int *sources,
+                          const double *arrival_us, double *latency_us, int **labels_out, double *makespan_us);
+/* Epochs run and the largest number of concurrent searches in the last trace. */
+int b40c_server_stats(b40c_server_t *server, long long *epochs, long long *max_active);
+
 /* ---- failure detection -------------------------------------------------- */
 /* Runs the bounded grid barrier on a cooperative grid with one arrival that
  * never comes: every block gives up after wait_limit_us and the call returns
