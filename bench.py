@@ -18,6 +18,14 @@ and two-phase are timed the same way and reported under "strategies".
           visited vertex) / the fused kernel's average duration, against the
           measured HBM copy bandwidth.
 
+  batched   1024 searches over 64 graphs (R-MAT scale 12..20, Erdos-Renyi) in
+          one multi-search launch vs the same searches as back-to-back
+          EnactSearch calls; queries/s, every label array checked.
+  served    Poisson traces (1K, 10K, 50K req/s, and all at once) over 32
+          resident graphs through the continuous-batching server; queries/s
+          and p50/p99 latency against sequential EnactSearch serving the
+          same trace.
+
 --impl reference runs the reference's own CPU BFS (SimpleReferenceBfs, built
 into oracle/_ref) on all host cores instead.  With torchrun each rank runs an
 independent replica (its own 64 sources; no collective on the data path) and
@@ -59,6 +67,8 @@ def parse_args():
     ap.add_argument("--variant", type=int, default=1, help="1 fused, 2 iterative (graph-driven)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 1024-search batched leg")
+    ap.add_argument("--no-served", action="store_true", help="skip the Poisson-trace serving leg")
     ap.add_argument("--verify", type=int, default=2, help="sources checked against the oracle")
     ap.add_argument("--sources", type=int, default=NUM_SOURCES, help="sources per step (64 for the bench line)")
     return ap.parse_args()
@@ -218,6 +228,226 @@ def reference_arm(args):
 
 
 # ------------------------------------------------------------------------------------------
+# Batched and served legs (multi-search kernel vs back-to-back single searches)
+# ------------------------------------------------------------------------------------------
+
+def batched_set(seed=4):
+    """64 graphs: R-MAT with scale uniform in 12..20 and edge factor uniform in
+    8..32, every fourth an Erdos-Renyi G(n, 16/(n-1)) of the same n; 16 seeded
+    sources each (1024 searches)."""
+    from back40computing_b200 import graphs
+    rng = np.random.default_rng(seed)
+    gs, desc = [], []
+    for i in range(64):
+        scale = int(rng.integers(12, 21))
+        ef = int(rng.integers(8, 33))
+        n = 1 << scale
+        if i % 4 == 3:
+            gs.append(graphs.erdos_renyi(n, 16.0 / (n - 1), seed=100 + i))
+            desc.append(f"er-{scale}")
+        else:
+            gs.append(graphs.rmat(scale, ef, seed=100 + i, undirected=True))
+            desc.append(f"rmat-{scale}-{ef}")
+    gids = np.repeat(np.arange(64, dtype=np.int32), 16)
+    srcs = np.concatenate([g.sample_sources(16, 200 + i) for i, g in enumerate(gs)]).astype(np.int32)
+    return gs, desc, gids, srcs
+
+
+def served_set(main_graph):
+    """32 resident graphs: 24 R-MAT (scales 14..22, edge factor 16; the scale-22
+    one is the headline graph) and 8 grids of 64K..16M vertices."""
+    from back40computing_b200 import graphs
+    gs, desc = [], []
+    scales = [14, 15, 16, 17, 18, 19, 20, 21, 14, 15, 16, 17, 18, 19, 20, 14, 15, 16, 17, 18, 19, 14, 16, 22]
+    for i, sc in enumerate(scales):
+        if sc == 22:
+            gs.append(main_graph)
+        else:
+            gs.append(graphs.rmat(sc, 16, seed=300 + i, undirected=True))
+        desc.append(f"rmat-{sc}")
+    for w in (256, 512, 1024, 2048):
+        gs.append(graphs.grid2d(w))
+        desc.append(f"grid2d-{w}")
+    for w in (40, 64, 128, 256):
+        gs.append(graphs.grid3d(w))
+        desc.append(f"grid3d-{w}")
+    return gs, desc
+
+
+def _crc(a):
+    import zlib
+    return zlib.crc32(np.ascontiguousarray(a).view(np.uint8))
+
+
+class SequentialSearches:
+    """Back-to-back plain single searches (Reset + EnactSearch on the
+    expand-contract enactor), one resident CsrProblem per graph."""
+
+    def __init__(self, b, gs, stream):
+        self.b = b
+        self.stream = stream
+        self.problems = []
+        for g in gs:
+            p = b.CsrProblem(False).from_graph(g)
+            p.set_stream(stream.cuda_stream)
+            self.problems.append(p)
+        self.en = b.make_enactor(HEADLINE)
+        self.en.set_stream(stream.cuda_stream)
+        self.ft = self.en.GetFrontierType()
+
+    def enqueue(self, gid, src):
+        b = self.b
+        b.check(self.problems[gid].ResetAsync(self.ft, 1.3))
+        b.check(self.en.EnactSearchAsync(self.problems[gid], int(src), 0, 1))
+
+    def labels(self, gid):
+        b = self.b
+        b.check(self.en.Sync())
+        return self.problems[gid].labels()
+
+    def close(self):
+        for p in self.problems:
+            p.close()
+        self.problems = []
+        del self.en
+
+
+def batched_leg(b, torch, stream, args):
+    """1024 searches over 64 graphs: one batched launch (CUDA graph replay) vs
+    the same searches as back-to-back EnactSearch calls; device time, labels
+    compared by checksum for every search."""
+    from back40computing_b200.batch import BfsBatch
+    gs, desc, gids, srcs = batched_set()
+    n = len(gids)
+    seq = SequentialSearches(b, gs, stream)
+    crc_seq = np.zeros(n, np.int64)
+    edges = np.zeros(n, np.int64)
+    degs = [g.degrees().astype(np.int64) for g in gs]
+    for i in range(n):
+        seq.enqueue(gids[i], srcs[i])
+        lab = seq.labels(gids[i])
+        crc_seq[i] = _crc(lab)
+        edges[i] = int(degs[gids[i]][lab > -1].sum())
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def time_seq():
+        ev[0].record(stream)
+        for i in range(n):
+            seq.enqueue(gids[i], srcs[i])
+        ev[1].record(stream)
+        b.check(seq.en.Sync())
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1])
+
+    for _ in range(args.warmup):
+        time_seq()
+    seq_ms = [time_seq() for _ in range(args.steps)]
+    seq.close()
+
+    batch = BfsBatch()
+    batch.set_stream(stream.cuda_stream)
+    for g in gs:
+        batch.add_graph(g)
+    batch.run(gids, srcs, use_cuda_graph=True)
+    mismatched = [i for i in range(n) if _crc(batch.labels(i)) != crc_seq[i]]
+    if mismatched:
+        raise SystemExit(f"bench: batched labels differ from single searches for searches {mismatched[:8]}")
+    for _ in range(args.warmup):
+        batch.run(gids, srcs, use_cuda_graph=True)
+    bat_ms = []
+    for _ in range(args.steps):
+        batch.run(gids, srcs, use_cuda_graph=True)
+        bat_ms.append(batch.last_elapsed_ms())
+    batch.close()
+    s_ms, b_ms = float(np.median(seq_ms)), float(np.median(bat_ms))
+    return {
+        "workload": "64 graphs (48 R-MAT scale 12..20 ef 8..32, 16 Erdos-Renyi mean degree 16), 16 sources each",
+        "searches": n, "graph_edges_total": int(sum(g.edges for g in gs)),
+        "queries_per_s": n / (b_ms / 1e3), "gteps": float(edges.sum()) / (b_ms / 1e3) / 1e9,
+        "ms_per_batch": b_ms,
+        "sequential_queries_per_s": n / (s_ms / 1e3), "sequential_ms": s_ms,
+        "speedup_vs_sequential": s_ms / b_ms,
+        "labels": "identical to single searches (crc32 of all %d label arrays)" % n,
+        "timing": "device time, median of %d; sequential = back-to-back async Reset+EnactSearch" % args.steps,
+    }
+
+
+def served_leg(b, torch, stream, args, main_graph):
+    """Poisson traces over 32 resident graphs through the continuous-batching
+    server, against sequential plain EnactSearch serving the same trace in FIFO
+    order (each query's measured device service time)."""
+    from back40computing_b200.serve import BfsServer, poisson_arrivals
+    gs, desc = served_set(main_graph)
+    G = len(gs)
+    pool = [g.sample_sources(16, 400 + i) for i, g in enumerate(gs)]
+    seq = SequentialSearches(b, gs, stream)
+    # Service time of every (graph, source) pair, alone, after a warm-up search.
+    service = np.zeros((G, 16))
+    crc = np.zeros((G, 16), np.int64)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for gi in range(G):
+        seq.enqueue(gi, pool[gi][0])
+        b.check(seq.en.Sync())
+        for k, s in enumerate(pool[gi]):
+            ev[0].record(stream)
+            seq.enqueue(gi, s)
+            ev[1].record(stream)
+            crc[gi, k] = _crc(seq.labels(gi))
+            service[gi, k] = ev[0].elapsed_time(ev[1]) * 1e3
+    seq.close()
+    budget = min(48 << 30, int(torch.cuda.mem_get_info()[0] * 0.6))
+    srv = BfsServer(max_slots=1024, hbm_budget_bytes=budget)
+    for g in gs:
+        srv.add_graph(g)
+
+    def trace(nq, rate, seed):
+        rng = np.random.default_rng(seed)
+        gids = rng.integers(0, G, nq).astype(np.int32)
+        ks = rng.integers(0, 16, nq)
+        srcs = np.array([pool[g][k] for g, k in zip(gids, ks)], np.int32)
+        arr = np.zeros(nq) if rate is None else poisson_arrivals(nq, rate, seed)
+        return gids, ks, srcs, arr
+
+    # Identity: a mixed trace with labels kept, every query against its lone search.
+    gids, ks, srcs, arr = trace(256, 50000.0, 11)
+    _, _, labs = srv.run_trace(gids, srcs, arr, keep_labels=True)
+    bad = [i for i in range(len(gids)) if _crc(labs[i]) != crc[gids[i], ks[i]]]
+    if bad:
+        raise SystemExit(f"bench: served labels differ from lone searches for queries {bad[:8]}")
+    del labs
+    out = {"workload": "32 resident graphs (24 R-MAT scale 14..22 ef 16, grid2d 256..2048, grid3d 40..256), "
+                       "queries (graph, source) uniform over graphs, 16 seeded sources per graph",
+           "labels": "identical alone and in the mix (crc32, 256-query trace at 50K req/s)"}
+    rates = []
+    for rate, nq in ((1000.0, 1000), (10000.0, 2000), (50000.0, 4000), (None, 4000)):
+        gids, ks, srcs, arr = trace(nq, rate, 21 + nq)
+        lat, span = srv.run_trace(gids, srcs, arr)
+        svc = service[gids, ks]
+        fin, t = np.zeros(nq), 0.0
+        for i in range(nq):
+            t = max(t, arr[i]) + svc[i]
+            fin[i] = t
+        slat = fin - arr
+        rates.append({
+            "rate_per_s": rate if rate is not None else "all at t=0", "queries": nq,
+            "queries_per_s": nq / (span / 1e6), "p50_us": float(np.percentile(lat, 50)),
+            "p99_us": float(np.percentile(lat, 99)),
+            "sequential_queries_per_s": nq / (fin[-1] / 1e6), "sequential_p50_us": float(np.percentile(slat, 50)),
+            "sequential_p99_us": float(np.percentile(slat, 99)),
+        })
+    st = srv.stats()
+    srv.close()
+    sat = rates[-1]
+    out.update({"rates": rates, "saturated_queries_per_s": sat["queries_per_s"],
+                "sequential_saturated_queries_per_s": sat["sequential_queries_per_s"],
+                "speedup_vs_sequential": sat["queries_per_s"] / sat["sequential_queries_per_s"],
+                "server": st,
+                "timing": "server: host clock in the request loop, real-time replay; sequential: FIFO of each "
+                          "query's device service time (Reset+EnactSearch alone), no host overhead"})
+    return out
+
+
+# ------------------------------------------------------------------------------------------
 # Our arm
 # ------------------------------------------------------------------------------------------
 
@@ -373,6 +603,13 @@ def main():
                "ms_per_step": secs / args.steps * 1e3}
         del en
 
+    # Batched and served legs (one GPU; replicas add nothing to their comparison).
+    batched = served = None
+    if world == 1 and not args.no_batched:
+        batched = batched_leg(b, torch, stream, args)
+    if world == 1 and not args.no_served:
+        served = served_leg(b, torch, stream, args, g)
+
     # CPU baseline: the reference's CPU BFS on a bounded sample, rank 0 at N=1.
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -408,6 +645,8 @@ def main():
         "clocks": head["clocks"],
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "batched": batched,
+        "served": served,
     }
     print(json.dumps(line), flush=True)
 
