@@ -77,6 +77,8 @@ SIGNATURES = {
     "b40c_server_run_trace": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                       POINTER(c_double)]),
     "b40c_server_stats": (c_int, [c_void_p, POINTER(c_longlong), POINTER(c_longlong)]),
+    "b40c_enact_search_no_alloc": (c_int, [c_int, c_int, c_void_p, c_void_p, c_int, c_void_p, POINTER(c_int),
+                                           c_void_p]),
 }
 
 _lib = None

@@ -18,8 +18,8 @@ INCLUDE = ROOT / "include"
 LIB = PKG / "libb40c_bfs.so"
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["bfs_kernels.cu", "bfs_host.cu", "ms_kernels.cu", "ms_host.cu", "server_host.cu", "graph_gen.cpp",
-           "graph_io.cpp"]
+SOURCES = ["bfs_kernels.cu", "bfs_host.cu", "ms_kernels.cu", "ms_host.cu", "server_host.cu", "no_alloc.cu",
+           "graph_gen.cpp", "graph_io.cpp"]
 DRIVER = PKG / "test_bfs"
 
 

@@ -238,6 +238,29 @@ int b40c_server_run_trace(b40c_server_t *server, int n, const int *graph_ids, co
 /* Epochs run and the largest number of concurrent searches in the last trace. */
 int b40c_server_stats(b40c_server_t *server, long long *epochs, long long *max_active);
 
+/* ---- search without allocation (no counterpart in the reference) --------
+ * For callers that must not allocate device memory while they search: code
+ * that runs while a CUDA graph is being captured on its stream, frameworks
+ * whose allocator owns all device memory, and latency-bound loops that cannot
+ * afford the synchronisation cudaMalloc/cudaFree may cause.  Runs one fused
+ * expand-contract search (default policy, depth labels) over a CSR the caller
+ * already holds on the current device: d_row_offsets (nodes + 1 entries,
+ * non-decreasing from 0 to edges) and d_column_indices (edges entries, each
+ * in [0, nodes)), writing nodes depth labels to d_labels (-1 = unreached).
+ * *search_depth (may be NULL) gets the value b40c_enactor_get_statistics
+ * reports for that search.  Synchronous on stream (NULL = default stream).
+ * Allocates nothing: its scratch memory (counters, visited bitmask, frontier
+ * queues, chunk tables) comes from one static 32 MiB device array that every
+ * GPU loading the library holds until exit; a graph whose scratch would not
+ * fit (about 1M vertices with 16M edges fits) is rejected with
+ * B40C_ERR_INVALID_VALUE and a message naming both sizes.  The first call on
+ * each device looks up that array's device address; make it before any
+ * stream capture.  All calls on a device share the array: calls that overlap
+ * on the GPU race and corrupt each other's results. */
+int b40c_enact_search_no_alloc(int nodes, int edges, const int *d_row_offsets,
+                               const int *d_column_indices, int src, int *d_labels,
+                               int *search_depth, void *stream);
+
 /* ---- failure detection -------------------------------------------------- */
 /* Runs the bounded grid barrier on a cooperative grid with one arrival that
  * never comes: every block gives up after wait_limit_us and the call returns
