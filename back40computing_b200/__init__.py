@@ -8,6 +8,7 @@ from .bfs import (  # noqa: F401
     CsrProblem,
     EnactorContractExpand,
     EnactorExpandContract,
+    EnactorHybrid,
     EnactorTwoPhase,
     FrontierType,
     Strategy,

@@ -258,10 +258,17 @@ class EnactorTwoPhase(_Enactor):
     STRATEGY = Strategy.TWO_PHASE
 
 
+class EnactorHybrid(_Enactor):
+    """bfs::EnactorHybrid<INSTRUMENT> (enactor_hybrid.cuh:64-758): contract-expand
+    levels while the edge frontier is small, two-phase levels while it is large."""
+    STRATEGY = Strategy.HYBRID
+
+
 ENACTORS = {
     Strategy.EXPAND_CONTRACT: EnactorExpandContract,
     Strategy.CONTRACT_EXPAND: EnactorContractExpand,
     Strategy.TWO_PHASE: EnactorTwoPhase,
+    Strategy.HYBRID: EnactorHybrid,
 }
 
 

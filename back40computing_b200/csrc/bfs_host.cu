@@ -307,8 +307,6 @@ int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size,
         return set_error(B40C_ERR_ILLEGAL_STATE, "problem needs FromHostProblem and Reset before a search");
     if (src < 0 || src >= p->nodes)
         return set_error(B40C_ERR_INVALID_VALUE, "source %d outside [0, %lld)", src, (long long)p->nodes);
-    if (e->strategy == B40C_HYBRID)
-        return set_error(B40C_ERR_NOT_SUPPORTED, "hybrid strategy not available in this build");
     int rc = ensure_enactor_buffers(e, p);
     if (rc) return rc;
     BfsParams bp;
@@ -324,7 +322,11 @@ int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size,
         cudaStreamWaitEvent(s, dep, 0);
         cudaEventDestroy(dep);
     }
-    if (variant == B40C_VARIANT_DEFAULT) variant = B40C_VARIANT_FUSED;
+    if (variant < B40C_VARIANT_DEFAULT || variant > B40C_VARIANT_ITERATIVE)
+        return set_error(B40C_ERR_INVALID_VALUE, "unknown variant %d", variant);
+    // The hybrid switches between its two bodies inside one persistent launch;
+    // like the reference's EnactorHybrid it has a single way to run a search.
+    if (variant == B40C_VARIANT_DEFAULT || e->strategy == B40C_HYBRID) variant = B40C_VARIANT_FUSED;
     if (bp.levels)
         CUDA_TRY(cudaMemsetAsync(bp.levels, 0, sizeof(LevelRecord) * LEVEL_LOG_CAP, s), "level log clear");
     CUDA_TRY(cudaEventRecord(e->ev0, s), "cudaEventRecord");

@@ -457,7 +457,8 @@ template <int THREADS, bool MP>
 struct ContractExpandSink {
     const BfsParams &p;
     Smem<THREADS, MP> &sm;
-    int it;
+    int it;  // depth label of the contracted vertices
+    int q;   // ring phase: reads queue[q&1], writes queue[(q+1)&1] and ring slot q+1
     uint64_t pol;
 
     __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
@@ -481,7 +482,7 @@ struct ContractExpandSink {
         for (int j = 0; j < 4; j++)
             if ((surv >> j) & 1u) ws.surv[pre[j]] = u[j];
         __syncwarp();
-        const int nq = (it + 1) & 1;
+        const int nq = (q + 1) & 1;
         PositionSink<MP> out{p.queue[nq], p.pred_queue[nq]};
         for (unsigned g = 0; g < total; g += 32) {
             int v = -1, start = 0, len = 0;
@@ -489,8 +490,8 @@ struct ContractExpandSink {
                 v = ws.surv[g + lane_id()];
                 row_range(p, v, start, len);
             }
-            if (place1<THREADS>(p, it + 1, len > 0, start, len, v)) len = 0;
-            warp_lists<MP, true>(p, ws, out, pol, start, len, v, &p.ctr->qlen[(it + 1) & 3]);
+            if (place1<THREADS>(p, q + 1, len > 0, start, len, v)) len = 0;
+            warp_lists<MP, true>(p, ws, out, pol, start, len, v, &p.ctr->qlen[(q + 1) & 3]);
         }
         __syncwarp();
     }
@@ -577,14 +578,15 @@ __device__ __forceinline__ void edge_tiles(const int *q_in, const int *pq_in, un
     }
 }
 
-// Contract-expand level it (contract_expand_atomic/cta.cuh:573-709).
+// Contract-expand level it in ring phase q (contract_expand_atomic/cta.cuh:573-709);
+// q == it except in the hybrid kernel, whose two-phase levels take two phases.
 template <int THREADS, bool MP>
-__device__ void ce_level(const BfsParams &p, int it, unsigned L, unsigned nch, unsigned nwch, Smem<THREADS, MP> &sm,
-                         uint64_t pol) {
-    ContractExpandSink<THREADS, MP> sink{p, sm, it, pol};
-    gather_chunks<THREADS>(p, p.chunks[it & 1], nch, sink, pol);
-    gather_wchunks(p, p.wchunks[it & 1], nwch, sink, pol);
-    edge_tiles<MP>(p.queue[it & 1], p.pred_queue[it & 1], L, sink);
+__device__ void ce_level(const BfsParams &p, int it, int q, unsigned L, unsigned nch, unsigned nwch,
+                         Smem<THREADS, MP> &sm, uint64_t pol) {
+    ContractExpandSink<THREADS, MP> sink{p, sm, it, q, pol};
+    gather_chunks<THREADS>(p, p.chunks[q & 1], nch, sink, pol);
+    gather_wchunks(p, p.wchunks[q & 1], nwch, sink, pol);
+    edge_tiles<MP>(p.queue[q & 1], p.pred_queue[q & 1], L, sink);
 }
 
 // Two-phase contract, phase qi = 2 * it.
@@ -767,7 +769,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
             c->total_queued += L;
             log_phase(p, it, L, nch, nw);
         }
-        ce_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
+        ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, pol);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         it++;
     }
@@ -811,6 +813,58 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
     finish_search(p, it, qi + 1);
 }
 
+// Hybrid (the reference's EnactorHybrid, enactor_hybrid.cuh:279-555): a level
+// whose incoming edge frontier is small runs as one contract-expand phase; a
+// level whose frontier exceeds 4 edges per thread of the grid (the reference's
+// SATURATION_QUIT = 4 * 128 per 128-thread CTA, :571, checked by
+// contract_expand_atomic/kernel.cuh:653 and two_phase/contract_atomic/kernel.cuh:338)
+// runs as a two-phase contract phase and expand phase.  Both bodies take and
+// leave the same edge frontier, so the switch happens inside one persistent
+// launch instead of between kernels.  Every CTA reads the same counters after
+// the barrier and so takes the same branch.  The level log is indexed by phase.
+template <int THREADS, bool MP>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(BfsParams p) {
+    Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
+    init_hist(sm, p.cull_flags);
+    const uint64_t pol = policy_evict_first();
+    Counters *c = p.ctr;
+    const unsigned long long saturation = 4ull * THREADS * gridDim.x;
+    int it = 0, q = 0;
+    for (;;) {
+        unsigned L = ld_cg(&c->qlen[q & 3]);
+        const unsigned nch = ld_cg(&c->big[q & 3]), nw = ld_cg(&c->wch[q & 3]);
+        if (stop_level_loop(p, it, L + nch + nw)) break;
+        if (leader()) {
+            ring_prepare(c, q);
+            c->total_queued += L;
+            log_phase(p, q, L, nch, nw);
+        }
+        const unsigned long long edges =
+            L + (unsigned long long)nch * chunk_edges<THREADS>() + (unsigned long long)nw * WARP_CHUNK;
+        if (edges <= saturation) {
+            ce_level<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
+            if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+            q++;
+            it++;
+            continue;
+        }
+        tp_contract<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
+        if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        q++;
+        L = ld_cg(&c->qlen[q & 3]);
+        if (L == 0u) break;  // no vertex discovered: stop without ++, as two-phase does
+        if (leader()) {
+            ring_prepare(c, q);
+            log_phase(p, q, L, 0u, 0u);
+        }
+        tp_expand<THREADS, MP>(p, q, L, sm, pol);
+        if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        q++;
+        it++;
+    }
+    finish_search(p, it, q);
+}
+
 // ---- per-level kernels for the graph-driven (iterative) variants ----------------
 
 template <int THREADS, bool MP>
@@ -832,7 +886,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_level_kernel(
     const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3], nw = p.ctr->wch[it & 3];
     if (L + nch + nw == 0u || p.ctr->error) return;
     if (leader()) log_phase(p, it, L, nch, nw);
-    ce_level<THREADS, MP>(p, it, L, nch, nw, sm, policy_evict_first());
+    ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, policy_evict_first());
 }
 
 // Two-phase per-level: qi = 2 * it (contract) and 2 * it + 1 (expand).
@@ -929,6 +983,7 @@ static KernelFn fused_fn(int strategy) {
     switch (strategy) {
     case STRATEGY_EXPAND_CONTRACT: return ec_fused_kernel<THREADS, MP>;
     case STRATEGY_CONTRACT_EXPAND: return ce_fused_kernel<THREADS, MP>;
+    case STRATEGY_HYBRID: return hy_fused_kernel<THREADS, MP>;
     default: return tp_fused_kernel<THREADS, MP>;
     }
 }

@@ -12,6 +12,7 @@ enum Strategy : int {
     STRATEGY_EXPAND_CONTRACT = 0,
     STRATEGY_CONTRACT_EXPAND = 1,
     STRATEGY_TWO_PHASE = 2,
+    STRATEGY_HYBRID = 3,  // contract-expand or two-phase per level, by frontier size (fused only)
 };
 
 enum CullFlags : unsigned {

@@ -46,7 +46,6 @@ class RangePool {
         free_.clear();
         if (capacity) free_[0] = capacity;
         capacity_ = capacity;
-        used_ = 0;
     }
     bool alloc(size_t n, size_t *off) {
         if (n == 0) n = 1;
@@ -57,7 +56,6 @@ class RangePool {
                 size_t next = it->first + n;
                 free_.erase(it);
                 if (rest) free_[next] = rest;
-                used_ += n;
                 return true;
             }
         }
@@ -65,7 +63,6 @@ class RangePool {
     }
     void release(size_t off, size_t n) {
         if (n == 0) n = 1;
-        used_ -= n;
         auto it = free_.emplace(off, n).first;
         auto nx = std::next(it);
         if (nx != free_.end() && it->first + it->second == nx->first) {
@@ -81,11 +78,10 @@ class RangePool {
         }
     }
     size_t capacity() const { return capacity_; }
-    size_t used() const { return used_; }
 
   private:
     std::map<size_t, size_t> free_;
-    size_t capacity_ = 0, used_ = 0;
+    size_t capacity_ = 0;
 };
 
 struct ResidentGraph {

@@ -1,7 +1,7 @@
 // test_bfs: command-line driver over the drop-in C++ API, shaped like the
 // reference's test/bfs/test_bfs.cu (main :903-1148, RunTests :600-756).
 //
-//   test_bfs <graph> <args> [--strategy=0,1,2] [--src=<v>|randomize] [--i=<n>]
+//   test_bfs <graph> <args> [--strategy=0,1,2,3] [--src=<v>|randomize] [--i=<n>]
 //            [--queue-sizing=<f>] [--mark-pred] [--max-ctas=<n>] [--variant=<0|1|2>]
 //            [--labels-out=<file>] [--quiet]
 //   graphs: grid2d <width> | grid3d <width> | rmat <scale> <edge-factor> [<seed>]
@@ -111,6 +111,7 @@ int run(const Args &a, b40c_csr_t &g, int default_src) {
     bfs::EnactorExpandContract<false> expand_contract;
     bfs::EnactorContractExpand<false> contract_expand;
     bfs::EnactorTwoPhase<false> two_phase;
+    bfs::EnactorHybrid<false> hybrid;
     std::vector<int> labels((size_t)g.nodes);
     std::vector<int> sources((size_t)std::max(1, a.iterations));
     if (a.src == "randomize" || (a.src.empty() && default_src < 0)) {
@@ -138,6 +139,7 @@ int run(const Args &a, b40c_csr_t &g, int default_src) {
             if (strategy == 0) B40C_RUN(expand_contract);
             else if (strategy == 1) B40C_RUN(contract_expand);
             else if (strategy == 2) B40C_RUN(two_phase);
+            else if (strategy == 3) B40C_RUN(hybrid);
             else {
                 fprintf(stderr, "strategy %d not provided\n", strategy);
                 return 1;
@@ -177,7 +179,7 @@ int main(int argc, char **argv) {
     int default_src = 0;
     if (build_graph(a, &g, &default_src)) {
         fprintf(stderr, "usage: test_bfs <grid2d w|grid3d w|rmat scale ef [seed]|erdos n deg [seed]|market file> "
-                        "[--strategy=0,1,2] [--src=v|randomize] [--i=n] [--queue-sizing=f] [--mark-pred] "
+                        "[--strategy=0,1,2,3] [--src=v|randomize] [--i=n] [--queue-sizing=f] [--mark-pred] "
                         "[--max-ctas=n] [--variant=0|1|2] [--labels-out=file] [--quiet]\n");
         return 1;
     }

@@ -5,8 +5,8 @@ self-loops removed, duplicates kept, symmetrized (~134M int32 CSR entries);
 64 sources drawn with seed 2 among vertices of degree > 0.  Synthetic, seeded.
 
 A step is one BFS from each of the 64 sources (Reset + EnactSearch each).  The
-headline strategy is expand-contract (fused persistent kernel); contract-expand
-and two-phase are timed the same way and reported under "strategies".
+headline strategy is expand-contract (fused persistent kernel); contract-expand,
+two-phase and hybrid are timed the same way and reported under "strategies".
 
   value   GTEPS = sum of edges_visited over the step's searches / device time,
           CSR resident in HBM, CUDA events on the enactor's stream.
@@ -51,7 +51,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "GTEPS (R-MAT s22 BFS)"
 UNIT = "GTEPS"
 NUM_SOURCES = 64
-STRATEGY_NAMES = {0: "expand_contract", 1: "contract_expand", 2: "two_phase"}
+STRATEGY_NAMES = {0: "expand_contract", 1: "contract_expand", 2: "two_phase", 3: "hybrid"}
 HEADLINE = 0
 
 
@@ -63,7 +63,7 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=22)
     ap.add_argument("--edge-factor", type=int, default=16)
-    ap.add_argument("--strategies", default="0,1,2")
+    ap.add_argument("--strategies", default="0,1,2,3")
     ap.add_argument("--variant", type=int, default=1, help="1 fused, 2 iterative (graph-driven)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -100,6 +100,16 @@ class EnactorTwoPhase : public EnactorCommon<B40C_TWO_PHASE, INSTRUMENT> {
     explicit EnactorTwoPhase(bool DEBUG = false) : EnactorCommon<B40C_TWO_PHASE, INSTRUMENT>(DEBUG) {}
 };
 
+/* enactor_hybrid.cuh:64-758: contract-expand levels while the edge frontier is
+ * small, two-phase levels while it is large (one persistent launch here).  The
+ * reference class offers only EnactSearch; EnactFusedSearch and
+ * EnactIterativeSearch run the same search. */
+template <bool INSTRUMENT>
+class EnactorHybrid : public EnactorCommon<B40C_HYBRID, INSTRUMENT> {
+  public:
+    explicit EnactorHybrid(bool DEBUG = false) : EnactorCommon<B40C_HYBRID, INSTRUMENT>(DEBUG) {}
+};
+
 }  // namespace bfs
 }  // namespace graph
 }  // namespace b40c

@@ -14,7 +14,7 @@ from conftest import golden_paths, load_golden
 
 pytestmark = pytest.mark.gpu
 
-STRATEGIES = [0, 1, 2]  # expand-contract, contract-expand, two-phase
+STRATEGIES = [0, 1, 2, 3]  # expand-contract, contract-expand, two-phase, hybrid
 VARIANTS = [1, 2]       # fused (persistent kernel), iterative (graph-driven per-level)
 
 
@@ -23,16 +23,16 @@ def bfs_mod():
     return b
 
 
-def expected_search_depth(strategy, g, labels):
+def expected_search_depths(strategy, g, labels):
     """GetStatistics search_depth (= iteration - 1) by strategy, derived from the
     reference's level loops: expand-contract and two-phase stop after the level
     that discovers nothing (depth d); contract-expand runs one more sweep over
-    the edges of the deepest level when it has any (d + 1)."""
+    the edges of the deepest level when it has any (d + 1).  The hybrid ends in
+    whichever body its last level ran, so either value is its own."""
     d = int(labels.max())
-    if strategy == 1:
-        deg = np.diff(g.row_offsets)
-        return d + 1 if (deg[labels == d] > 0).any() else d
-    return d
+    deg = np.diff(g.row_offsets)
+    ce = d + 1 if (deg[labels == d] > 0).any() else d
+    return {0: {d}, 1: {ce}, 2: {d}, 3: {d, ce}}[strategy]
 
 
 def run_search(g, strategy, variant, src, mark_pred=False, sizing=1.3, policy=None, problem=None,
@@ -63,7 +63,7 @@ def test_golden_labels_bit_exact(cuda_device, path, strategy, variant):
         labels, (_, search_depth, _) = run_search(g, strategy, variant, s, problem=prob)
         assert np.array_equal(labels, golden[i]), f"{path.stem} src {s}: first mismatch at " \
             f"{int(np.nonzero(labels != golden[i])[0][0])}"
-        assert search_depth == expected_search_depth(strategy, g, golden[i])
+        assert search_depth in expected_search_depths(strategy, g, golden[i])
         assert depths[i] == golden[i].max() + 1  # SimpleReferenceBfs search_depth
 
 
@@ -150,7 +150,7 @@ def test_edge_cases(cuda_device, oracle, case, strategy):
         for variant in VARIANTS:
             labels, (_, depth, _) = run_search(g, strategy, variant, s)
             assert oracle.first_mismatch(labels, ref) == -1, (case, s, variant)
-            assert depth == expected_search_depth(strategy, g, ref)
+            assert depth in expected_search_depths(strategy, g, ref)
             preds, _ = run_search(g, strategy, variant, s, mark_pred=True)
             assert oracle.check_predecessors(g, preds, ref)[0] == -1
 
@@ -174,7 +174,7 @@ def test_grid2d_1024_contract_expand(cuda_device, oracle):
     for strategy in STRATEGIES:
         labels, (_, depth, _) = run_search(g, strategy, 0, src)
         assert oracle.first_mismatch(labels, ref) == -1
-        assert depth == expected_search_depth(strategy, g, ref)
+        assert depth in expected_search_depths(strategy, g, ref)
 
 
 def test_overflow_reports_invalid_configuration(cuda_device, rmat16):
@@ -281,3 +281,27 @@ def test_level_log_matches_oracle_levels(cuda_device, oracle, rmat16):
             assert r["frontier"] <= n and (r["frontier"] == n or r["chunks"] + r["wchunks"] > 0)
         assert log[-1]["frontier"] == 0 and log[-1]["chunks"] == 0 and log[-1]["wchunks"] == 0
         assert all(log[i]["start_ns"] <= log[i + 1]["start_ns"] for i in range(len(log) - 1))
+
+
+def test_hybrid_switches_between_bodies(cuda_device, oracle, rmat16):
+    """A small grid lowers the hybrid's saturation point (4 edges per thread), so
+    most levels run as two phases; the full grid runs more of them as one
+    contract-expand phase.  Labels are the same whichever body runs."""
+    b = bfs_mod()
+    g = rmat16
+    s = int(g.sample_sources(1, 5)[0])
+    ref, _ = oracle.bfs(g, s)
+    d = int(ref.max())
+    prob = b.CsrProblem(False).from_graph(g)
+    en = b.EnactorHybrid()
+    en.set_level_log(True)
+    phases = {}
+    for grid in (1, 16, 0):
+        b.check(prob.Reset(en.GetFrontierType(), 1.3))
+        b.check(en.EnactSearch(prob, s, grid))
+        assert oracle.first_mismatch(prob.labels(), ref) == -1
+        _, depth, _ = en.GetStatistics()
+        assert depth in expected_search_depths(3, g, ref)
+        phases[grid] = len(en.level_log()) - 1  # the last record marks the end
+    assert phases[1] > d + 1          # two-phase levels ran
+    assert phases[0] <= phases[1]     # the full grid runs at least as many levels in one phase
