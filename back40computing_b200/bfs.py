@@ -226,18 +226,25 @@ class _Enactor:
 
     def level_log(self, max_records: int = 4096) -> list:
         """Per-level records of the last search: start time (ns, relative to the
-        first level), input frontier queue length, input CTA and warp chunks."""
+        first level), input frontier queue length, input CTA and warp chunks,
+        and whether the level ran bottom-up."""
         ts = (ctypes.c_int64 * max_records)()
         fr = (ctypes.c_int * max_records)()
         ch = (ctypes.c_int * max_records)()
         wc = (ctypes.c_int * max_records)()
+        bu = (ctypes.c_int * max_records)()
         n = ctypes.c_int()
-        check(lib().b40c_enactor_level_log(self._h, max_records, ts, fr, ch, wc, ctypes.byref(n)))
+        check(lib().b40c_enactor_level_log(self._h, max_records, ts, fr, ch, wc, bu, ctypes.byref(n)))
         if n.value == 0:
             return []
         t0 = ts[0]
-        return [{"level": i, "start_ns": ts[i] - t0, "frontier": fr[i], "chunks": ch[i], "wchunks": wc[i]}
+        return [{"level": i, "start_ns": ts[i] - t0, "frontier": fr[i], "chunks": ch[i], "wchunks": wc[i],
+                 "bottom_up": bool(bu[i])}
                 for i in range(n.value)]
+
+    def set_direction_optimizing(self, alpha: int = 14, beta: int = 24) -> None:
+        """Bottom-up levels for fused expand-contract searches (alpha = 0: off)."""
+        check(lib().b40c_enactor_set_direction_optimizing(self._h, int(alpha), int(beta)))
 
     def set_wait_limit_us(self, us: int) -> None:
         check(lib().b40c_enactor_set_wait_limit_us(self._h, int(us)))

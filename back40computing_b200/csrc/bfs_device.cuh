@@ -53,6 +53,11 @@ struct alignas(256) Counters {
     unsigned long long total_queued;  // sum of frontier lengths (instrumented)
     unsigned retired[4];  // multi-search: searches retired at the start of level q, at [q&3]
     unsigned pad_e[54];
+    // Direction-optimizing expand-contract: the vertices discovered as input of
+    // phase q (mf: the sum of their degrees, nf: their number), at [q&3].
+    unsigned long long mf[4];
+    unsigned nf[4];
+    unsigned pad_f[52];
     unsigned bar_count;  // grid barrier
     unsigned bar_gen;
     unsigned pad_g[61];
@@ -161,6 +166,12 @@ __device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wai
 }
 
 // ---- scans -------------------------------------------------------------------------
+__device__ __forceinline__ int warp_sum(int x) { return __reduce_add_sync(0xffffffffu, x); }
+__device__ __forceinline__ long long warp_sum_ll(long long x) {
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) x += __shfl_xor_sync(0xffffffffu, x, d);
+    return x;
+}
 __device__ __forceinline__ int warp_inclusive_scan(int x) {
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {

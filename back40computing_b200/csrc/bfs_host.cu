@@ -71,6 +71,8 @@ struct b40c_problem {
     bool reset_once = false;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
+    int symmetric = -1;                    // -1 unknown, 0 no, 1 yes (checked on first use)
+    unsigned long long *d_sym = nullptr;   // 4 hash sums of the symmetry check
 };
 
 struct b40c_enactor {
@@ -80,6 +82,7 @@ struct b40c_enactor {
     int threads = 256;
     int warp_th = 64, cta_th = 1024;
     unsigned cull_flags = CULL_HISTORY;
+    unsigned do_alpha = 0, do_beta = 0;  // direction-optimizing expand-contract (0: top-down only)
     unsigned long long wait_ns = 5000000000ull;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
@@ -163,6 +166,26 @@ void free_problem_device(b40c_problem *p) {
         p->d_queue[i] = p->d_pred[i] = nullptr;
         p->queue_elems[i] = p->pred_elems[i] = 0;
     }
+    cudaFree(p->d_sym);
+    p->d_sym = nullptr;
+    p->symmetric = -1;
+}
+
+// Whether every entry v of row u has an entry u in row v (a symmetric,
+// undirected graph), which bottom-up levels need.  Decided once per graph by
+// two 64-bit hash sums over the entries and their reverses (a non-symmetric
+// graph passes only on a double 64-bit collision), with a host wait.
+int ensure_symmetry_known(b40c_problem *p) {
+    if (p->symmetric >= 0) return B40C_SUCCESS;
+    cudaStream_t s = problem_stream(p);
+    if (!p->d_sym) CUDA_TRY(cudaMalloc(&p->d_sym, 4 * sizeof(unsigned long long)), "cudaMalloc symmetry sums");
+    unsigned long long h[4] = {0, 0, 0, 0};
+    CUDA_TRY(cudaMemsetAsync(p->d_sym, 0, sizeof(h), s), "symmetry sums clear");
+    CUDA_TRY(launch_symmetry_hash(p->d_row_offsets, p->d_col, int(p->nodes), p->d_sym, s), "symmetry check launch");
+    CUDA_TRY(cudaMemcpyAsync(h, p->d_sym, sizeof(h), cudaMemcpyDeviceToHost, s), "symmetry sums copy");
+    CUDA_TRY(cudaStreamSynchronize(s), "symmetry check");
+    p->symmetric = (h[0] == h[1] && h[2] == h[3]) ? 1 : 0;
+    return B40C_SUCCESS;
 }
 
 // Host ranges this library registered for stream_from_host, with the number
@@ -294,6 +317,9 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
     bp.warp_th = e->warp_th;
     bp.cta_th = std::max(e->cta_th, e->warp_th);
     bp.cull_flags = e->cull_flags;
+    bp.edges = p->edges;
+    bp.do_alpha = 0;  // enabled by enqueue_search for searches that can run bottom-up
+    bp.do_beta = 0;
     if (qcap < 1) return set_error(B40C_ERR_ILLEGAL_STATE, "frontier queues not allocated: call Reset first");
     if (p->mark_pred && e->strategy != B40C_EXPAND_CONTRACT && (!p->d_pred[0] || !p->d_pred[1]))
         return set_error(B40C_ERR_ILLEGAL_STATE,
@@ -327,6 +353,14 @@ int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size,
     // The hybrid switches between its two bodies inside one persistent launch;
     // like the reference's EnactorHybrid it has a single way to run a search.
     if (variant == B40C_VARIANT_DEFAULT || e->strategy == B40C_HYBRID) variant = B40C_VARIANT_FUSED;
+    // Bottom-up levels: fused expand-contract, depth labels, symmetric graph.
+    if (e->strategy == B40C_EXPAND_CONTRACT && variant == B40C_VARIANT_FUSED && !p->mark_pred && e->do_alpha) {
+        if ((rc = ensure_symmetry_known(p))) return rc;
+        if (p->symmetric == 1) {
+            bp.do_alpha = e->do_alpha;
+            bp.do_beta = e->do_beta;
+        }
+    }
     if (bp.levels)
         CUDA_TRY(cudaMemsetAsync(bp.levels, 0, sizeof(LevelRecord) * LEVEL_LOG_CAP, s), "level log clear");
     CUDA_TRY(cudaEventRecord(e->ev0, s), "cudaEventRecord");
@@ -603,7 +637,13 @@ extern "C" int b40c_enactor_create(int strategy, int instrument, int debug, b40c
     e->strategy = strategy;
     // Measured defaults on R-MAT graphs: expand-contract gathers lists of
     // 128+ edges with warps, the edge-frontier strategies lists of 64+.
-    if (strategy == B40C_EXPAND_CONTRACT) e->warp_th = 128;
+    // Expand-contract switches direction with the published alpha = 14,
+    // beta = 24 (Beamer, Asanovic and Patterson, SC 2012).
+    if (strategy == B40C_EXPAND_CONTRACT) {
+        e->warp_th = 128;
+        e->do_alpha = 14;
+        e->do_beta = 24;
+    }
     e->instrument = instrument != 0;
     e->debug = debug != 0;
     cudaError_t ce = cudaGetDevice(&e->device);
@@ -743,7 +783,7 @@ extern "C" int b40c_enactor_set_level_log(b40c_enactor_t *e, int enable) {
 }
 
 extern "C" int b40c_enactor_level_log(b40c_enactor_t *e, int max_records, int64_t *t_start_ns, int *frontier,
-                                      int *chunks, int *wchunks, int *count) {
+                                      int *chunks, int *wchunks, int *bottom_up, int *count) {
     clear_error();
     if (!e || !count || max_records < 0) return set_error(B40C_ERR_INVALID_VALUE, "invalid argument");
     *count = 0;
@@ -767,8 +807,20 @@ extern "C" int b40c_enactor_level_log(b40c_enactor_t *e, int max_records, int64_
         if (frontier) frontier[i] = (int)h[i].frontier;
         if (chunks) chunks[i] = (int)h[i].chunks;
         if (wchunks) wchunks[i] = (int)h[i].wchunks;
+        if (bottom_up) bottom_up[i] = (int)h[i].bottom_up;
     }
     *count = n;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_set_direction_optimizing(b40c_enactor_t *e, int alpha, int beta) {
+    clear_error();
+    if (!e || alpha < 0 || beta < 0 || (alpha > 0 && beta == 0))
+        return set_error(B40C_ERR_INVALID_VALUE, "direction switch: alpha >= 0, and beta >= 1 when alpha > 0");
+    if (alpha > 0 && e->strategy != B40C_EXPAND_CONTRACT)
+        return set_error(B40C_ERR_NOT_SUPPORTED, "bottom-up levels exist for the expand-contract strategy only");
+    e->do_alpha = unsigned(alpha);
+    e->do_beta = unsigned(beta);
     return B40C_SUCCESS;
 }
 

@@ -59,6 +59,8 @@ struct WarpSmem {
     int surv[WINDOW];
     int obuf[OBUF];
     unsigned nbuf;
+    unsigned disc_n;             // direction-optimizing counts of this warp's discoveries
+    unsigned long long disc_m;   // in the current level, added to the counters at its end
 };
 
 template <int THREADS, bool MP>
@@ -309,6 +311,34 @@ __device__ __forceinline__ void gather_wchunks(const BfsParams &p, const int4 *t
     }
 }
 
+// Both chunk tables of a phase.  When their slices of 128 edges (one 16-byte
+// load per lane) number no more than the grid's warps, every warp takes one
+// slice: a small level then finishes in one pass instead of the 4 passes a
+// CTA or warp needs for a whole chunk.  Otherwise CTAs stream CTA chunks and
+// warps stream warp chunks.
+template <int THREADS, class Sink>
+__device__ __forceinline__ void gather_chunk_tables(const BfsParams &p, const int4 *ctable, unsigned nch,
+                                                    const int4 *wtable, unsigned nw, const Sink &sink,
+                                                    uint64_t pol) {
+    constexpr unsigned SLICE = 128;
+    constexpr unsigned CS = chunk_edges<THREADS>() / SLICE, WS = WARP_CHUNK / SLICE;
+    if (nch > (unsigned)p.chunk_cap) nch = p.chunk_cap;
+    if (nw > (unsigned)p.wchunk_cap) nw = p.wchunk_cap;
+    const unsigned long long slices = (unsigned long long)nch * CS + (unsigned long long)nw * WS;
+    if (slices > (unsigned long long)grid_warps()) {
+        gather_chunks<THREADS>(p, ctable, nch, sink, pol);
+        gather_wchunks(p, wtable, nw, sink, pol);
+        return;
+    }
+    const unsigned w = global_warp();
+    if (w >= slices) return;
+    const int4 ch = w < nch * CS ? __ldcg(ctable + w / CS) : __ldcg(wtable + (w - nch * CS) / WS);
+    const unsigned k = w < nch * CS ? w % CS : (w - nch * CS) % WS;
+    const int a0 = (ch.x & ~3) + int(k * SLICE);
+    const int s0 = max(a0, ch.x), e0 = min(a0 + int(SLICE), ch.x + ch.y);
+    if (e0 > s0) gather_list<32>(p.col, p.vec_end, s0, e0 - s0, ch.z, 0u, lane_id(), sink, pol);
+}
+
 // Warp- and scan-based gather of one list per lane (start, len, owner pred).
 // With POSITIONAL the warp first reserves room for all its lists in the output
 // queue with one atomicAdd on qlen_out (short lists first, then the others) and
@@ -391,11 +421,45 @@ __device__ __forceinline__ unsigned warp_next_tile(unsigned *steal) {
     return __shfl_sync(FULL, t, 0);
 }
 
+// Next run of tiles for a warp that finished run r: the first W runs go one
+// per warp without atomics (a small phase then costs no counter traffic);
+// runs beyond them are handed out by the steal counter.
+__device__ __forceinline__ unsigned next_run(unsigned nruns, unsigned *steal) {
+    const unsigned W = grid_warps();
+    return nruns > W ? W + warp_next_tile(steal) : nruns;
+}
+
 // ---------------------------------------------------------------------------------------
 // Sinks: what happens to each gathered element.  Called by every lane of a
 // warp together with up to 4 elements per lane; bit j of valid marks u[j];
 // output positions (edge-frontier queues) are out0 + j.
 // ---------------------------------------------------------------------------------------
+
+// Direction-optimizing counts: a warp sums its discoveries (n vertices with
+// deg edges per lane) in shared memory during a level and adds them to the
+// counters of phase q once, at the level's end (one atomic pair per warp;
+// an atomic per discovery group would make the counters a hot spot).
+template <bool MP>
+__device__ __forceinline__ void count_discovered(WarpSmem<MP> &ws, int n, long long deg) {
+    const int nt = warp_sum(n);
+    const long long dt = warp_sum_ll(deg);
+    if (lane_id() == 0) {
+        ws.disc_n += unsigned(nt);
+        ws.disc_m += (unsigned long long)dt;
+    }
+}
+template <bool MP>
+__device__ __forceinline__ void flush_discovered(const BfsParams &p, WarpSmem<MP> &ws, int q) {
+    if (lane_id() == 0) {
+        if (ws.disc_n) {
+            atomicAdd(&p.ctr->nf[q & 3], ws.disc_n);
+            atomicAdd(&p.ctr->mf[q & 3], ws.disc_m);
+        }
+        ws.disc_n = 0u;
+        ws.disc_m = 0ull;
+    }
+    __syncwarp();
+}
 
 // Expand-contract: mark and label each neighbour at discovery (label it+1,
 // expand_contract_atomic/cta.cuh:181-218).  A discovered vertex's list becomes
@@ -422,11 +486,14 @@ struct DiscoverSink {
                 row_range(p, u[j], st[j], ln[j]);
             }
         }
+        if (p.do_alpha)
+            count_discovered(sm.w[threadIdx.x >> 5], __popc(disc), (long long)ln[0] + ln[1] + ln[2] + ln[3]);
         const unsigned enq = disc & ~place4<THREADS>(p, label, disc, st, ln, u);
         stage4(sm.w[threadIdx.x >> 5], enq, u, q_out, qlen_out, p.qcap, &p.ctr->error);
     }
     __device__ __forceinline__ void drain() const {
         stage_drain(sm.w[threadIdx.x >> 5], q_out, qlen_out, p.qcap, &p.ctr->error);
+        if (p.do_alpha) flush_discovered(p, sm.w[threadIdx.x >> 5], label);
     }
 };
 
@@ -532,15 +599,14 @@ __device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, u
     Counters *c = p.ctr;
     const int nq = (it + 1) & 1;
     DiscoverSink<THREADS, MP> sink{p, sm, p.queue[nq], &c->qlen[(it + 1) & 3], it + 1};
-    gather_chunks<THREADS>(p, p.chunks[it & 1], nch, sink, pol);
-    gather_wchunks(p, p.wchunks[it & 1], nwch, sink, pol);
+    gather_chunk_tables<THREADS>(p, p.chunks[it & 1], nch, p.wchunks[it & 1], nwch, sink, pol);
     WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
     const int *q_in = p.queue[it & 1];
     const unsigned ntiles = (L + 31) / 32;
     const unsigned grab = tile_grab(ntiles);
-    for (;;) {
-        const unsigned t0 = warp_next_tile(&c->steal[it & 3]) * grab;
-        if (t0 >= ntiles) break;
+    const unsigned nruns = (ntiles + grab - 1) / grab;
+    for (unsigned r = global_warp(); r < nruns; r = next_run(nruns, &c->steal[it & 3])) {
+        const unsigned t0 = r * grab;
         for (unsigned t = t0; t < t0 + grab && t < ntiles; t++) {
             const unsigned idx = t * 32 + lane_id();
             int v = -1, start = 0, len = 0;
@@ -552,6 +618,65 @@ __device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, u
         }
     }
     sink.drain();
+}
+
+// Bottom-up level it of direction-optimizing BFS (Beamer, Asanovic and
+// Patterson, "Direction-Optimizing Breadth-First Search", SC 2012): every
+// unvisited vertex looks for a neighbour at depth it, and the first one found
+// makes it a depth-(it+1) vertex.  Warp w of the grid takes visited-mask
+// words w, w + W, ...; lane j takes the word's vertex 32w + j and scans its
+// list 4 entries at a time until a parent turns up.  A word has one writer in
+// the level, so its new bits are a plain store.  Vertices without edges are
+// marked visited but never labelled: on a symmetric graph no list leads to
+// them, and later bottom-up levels skip them.  The discovered vertices are
+// counted and placed for level it+1 exactly as top-down discovery places them,
+// so either direction can run next.  Depth labels only (no predecessors).
+template <int THREADS, bool MP>
+__device__ void bu_level(const BfsParams &p, int it, Smem<THREADS, MP> &sm) {
+    static_assert(!MP, "bottom-up levels test depth labels");
+    Counters *c = p.ctr;
+    int *q_out = p.queue[(it + 1) & 1];
+    unsigned *qlen_out = &c->qlen[(it + 1) & 3];
+    WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
+    const unsigned nwords = (unsigned(p.nodes) + 31u) >> 5;
+    const unsigned W = grid_warps();
+    const int lane = lane_id();
+    for (unsigned w = global_warp(); w < nwords; w += W) {
+        const unsigned mword = ld_cg(p.mask + w);
+        if (mword == FULL) continue;  // warp-uniform
+        const int v = int(w * 32u) + lane;
+        const bool open = v < p.nodes && !((mword >> lane) & 1u);
+        int start = 0, len = 0;
+        if (open) row_range(p, v, start, len);
+        bool scan = open && len > 0, found = false;
+        for (int k = 0; __any_sync(FULL, scan); k += 4) {
+            if (scan) {
+                int u[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) u[j] = k + j < len ? __ldg(p.col + start + k + j) : -1;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    if (k + j < len) {
+                        if ((unsigned)u[j] < (unsigned)p.nodes) {
+                            found |= ld_cg(p.labels + u[j]) == it;
+                        } else {
+                            atomicOr(&c->error, ERR_BAD_VERTEX);
+                        }
+                    }
+                }
+                if (found || k + 4 >= len) scan = false;
+            }
+        }
+        const unsigned fb = __ballot_sync(FULL, found), zb = __ballot_sync(FULL, open && len == 0);
+        if (lane == 0 && (fb | zb)) __stcg(p.mask + w, mword | fb | zb);
+        if (found) p.labels[v] = it + 1;
+        count_discovered(ws, found ? 1 : 0, found ? len : 0);
+        const bool placed = place1<THREADS>(p, it + 1, found, start, len, v);
+        const int vv[4] = {v, 0, 0, 0};
+        stage4(ws, (found && !placed) ? 1u : 0u, vv, q_out, qlen_out, p.qcap, &c->error);
+    }
+    stage_drain(ws, q_out, qlen_out, p.qcap, &c->error);
+    flush_discovered(p, ws, it + 1);
 }
 
 // Edge-frontier phase input: warp tiles of 128 elements (4 per lane,
@@ -584,8 +709,7 @@ template <int THREADS, bool MP>
 __device__ void ce_level(const BfsParams &p, int it, int q, unsigned L, unsigned nch, unsigned nwch,
                          Smem<THREADS, MP> &sm, uint64_t pol) {
     ContractExpandSink<THREADS, MP> sink{p, sm, it, q, pol};
-    gather_chunks<THREADS>(p, p.chunks[q & 1], nch, sink, pol);
-    gather_wchunks(p, p.wchunks[q & 1], nwch, sink, pol);
+    gather_chunk_tables<THREADS>(p, p.chunks[q & 1], nch, p.wchunks[q & 1], nwch, sink, pol);
     edge_tiles<MP>(p.queue[q & 1], p.pred_queue[q & 1], L, sink);
 }
 
@@ -594,8 +718,7 @@ template <int THREADS, bool MP>
 __device__ void tp_contract(const BfsParams &p, int it, int qi, unsigned L, unsigned nch, unsigned nwch,
                             Smem<THREADS, MP> &sm, uint64_t pol) {
     ContractSink<THREADS, MP> sink{p, sm, p.queue[(qi + 1) & 1], &p.ctr->qlen[(qi + 1) & 3], it};
-    gather_chunks<THREADS>(p, p.chunks[qi & 1], nch, sink, pol);
-    gather_wchunks(p, p.wchunks[qi & 1], nwch, sink, pol);
+    gather_chunk_tables<THREADS>(p, p.chunks[qi & 1], nch, p.wchunks[qi & 1], nwch, sink, pol);
     edge_tiles<MP>(p.queue[qi & 1], p.pred_queue[qi & 1], L, sink);
     sink.drain();
 }
@@ -610,9 +733,9 @@ __device__ void tp_expand(const BfsParams &p, int qi, unsigned L, Smem<THREADS, 
     const int *q_in = p.queue[qi & 1];
     const unsigned ntiles = (L + 31) / 32;
     const unsigned grab = tile_grab(ntiles);
-    for (;;) {
-        const unsigned t0 = warp_next_tile(&c->steal[qi & 3]) * grab;
-        if (t0 >= ntiles) break;
+    const unsigned nruns = (ntiles + grab - 1) / grab;
+    for (unsigned r = global_warp(); r < nruns; r = next_run(nruns, &c->steal[qi & 3])) {
+        const unsigned t0 = r * grab;
         for (unsigned t = t0; t < t0 + grab && t < ntiles; t++) {
             const unsigned idx = t * 32 + lane_id();
             int v = -1, start = 0, len = 0;
@@ -632,25 +755,31 @@ __device__ __forceinline__ void ring_prepare(Counters *c, int q) {
     c->qlen[(q + 2) & 3] = 0u;
     c->big[(q + 2) & 3] = 0u;
     c->wch[(q + 2) & 3] = 0u;
+    c->nf[(q + 2) & 3] = 0u;
+    c->mf[(q + 2) & 3] = 0ull;
     c->steal[(q + 1) & 3] = 0u;
 }
 
 __device__ __forceinline__ void log_phase(const BfsParams &p, int idx, unsigned frontier, unsigned chunks,
-                                          unsigned wchunks) {
+                                          unsigned wchunks, unsigned bottom_up = 0u) {
     if (p.levels && idx < p.level_cap) {
         LevelRecord r;
         r.t_start = globaltimer_ns();
         r.frontier = frontier;
         r.chunks = chunks;
         r.wchunks = wchunks;
-        r.pad = 0;
+        r.bottom_up = bottom_up;
         p.levels[idx] = r;
     }
 }
 
 template <int THREADS, bool MP>
 __device__ __forceinline__ void init_hist(Smem<THREADS, MP> &sm, unsigned flags) {
-    if (lane_id() == 0) sm.w[threadIdx.x >> 5].nbuf = 0;
+    if (lane_id() == 0) {
+        sm.w[threadIdx.x >> 5].nbuf = 0;
+        sm.w[threadIdx.x >> 5].disc_n = 0;
+        sm.w[threadIdx.x >> 5].disc_m = 0;
+    }
     __syncwarp();
     if (flags & CULL_HISTORY) {
         // Tag 0xffffffff matches no mask word (word indices stay below 2^27).
@@ -691,6 +820,8 @@ __global__ void search_init_kernel(BfsParams p, int strategy, int mark_pred, int
         // discovered vertex's list.
         int start, len;
         row_range(p, p.src, start, len);
+        c->nf[0] = 1u;
+        c->mf[0] = (unsigned long long)len;
         const int a0 = start & ~3, span = start + len - a0;
         const bool cta = len >= p.cta_th, wrp = !cta && len >= p.warp_th;
         const int CH = cta ? cta_chunk : WARP_CHUNK;
@@ -732,22 +863,51 @@ __device__ __forceinline__ void finish_search(const BfsParams &p, int iteration,
     }
 }
 
+// Direction of the next level (Beamer et al., SC 2012): top-down turns
+// bottom-up once the frontier's edges mf exceed the unvisited vertices' edges
+// / alpha, and bottom-up turns back once the frontier holds fewer than
+// nodes / beta vertices and is shrinking.  Every CTA keeps the same state and
+// reads the same counters after a barrier, so all take the same direction.
+struct DirectionChoice {
+    unsigned long long explored = 0;  // degrees summed over the vertices visited so far
+    unsigned prev_nf = 0;
+    bool bottom_up = false;
+
+    __device__ __forceinline__ bool next(const BfsParams &p, unsigned nf, unsigned long long mf) {
+        explored += mf;
+        const unsigned long long total = (unsigned long long)p.edges;
+        const unsigned long long unexplored = total > explored ? total - explored : 0ull;
+        if (!bottom_up) bottom_up = mf * p.do_alpha > unexplored;
+        else bottom_up = !((unsigned long long)nf * p.do_beta < (unsigned long long)p.nodes && nf < prev_nf);
+        prev_nf = nf;
+        return bottom_up;
+    }
+};
+
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(BfsParams p) {
     Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const uint64_t pol = policy_evict_first();
     Counters *c = p.ctr;
+    DirectionChoice dir;
     int it = 0;
     for (;;) {
         const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]), nw = ld_cg(&c->wch[it & 3]);
         if (stop_level_loop(p, it, L + nch + nw)) break;
+        bool bottom_up = false;
+        if (!MP && p.do_alpha) bottom_up = dir.next(p, ld_cg(&c->nf[it & 3]), __ldcg(&c->mf[it & 3]));
         if (leader()) {
             ring_prepare(c, it);
             c->total_queued += L;
-            log_phase(p, it, L, nch, nw);
+            log_phase(p, it, L, nch, nw, bottom_up ? 1u : 0u);
         }
-        ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
+        if constexpr (!MP) {
+            if (bottom_up) bu_level<THREADS, MP>(p, it, sm);
+            else ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
+        } else {
+            ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
+        }
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         it++;
     }
@@ -965,6 +1125,47 @@ __global__ void level_control_kernel(BfsParams p, int strategy) {
     cudaGraphSetConditional((cudaGraphConditionalHandle)p.cond_handle, more ? 1u : 0u);
 }
 
+// SplitMix64's output function (Steele, Lea and Flood, OOPSLA 2014) as a 64-bit mixer.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x;
+}
+
+// sums[0] / sums[1]: hash sums of (u, v) / (v, u) over every entry v of row u;
+// sums[2] / sums[3]: the same with a second, salted hash.  A warp per row.
+__global__ void symmetry_hash_kernel(const int *row_offsets, const int *col, int nodes, unsigned long long *sums) {
+    constexpr unsigned long long SALT = 0x5851f42d4c957f2dull;
+    unsigned long long a0 = 0, b0 = 0, a1 = 0, b1 = 0;
+    const int lane = lane_id();
+    const int W = grid_warps();
+    for (int v = global_warp(); v < nodes; v += W) {
+        const int s = __ldg(row_offsets + v), e = __ldg(row_offsets + v + 1);
+        for (int k = s + lane; k < e; k += 32) {
+            const unsigned u = (unsigned)__ldg(col + k);
+            const unsigned long long fwd = ((unsigned long long)(unsigned)v << 32) | u;
+            const unsigned long long rev = ((unsigned long long)u << 32) | (unsigned)v;
+            a0 += mix64(fwd);
+            b0 += mix64(rev);
+            a1 += mix64(fwd ^ SALT);
+            b1 += mix64(rev ^ SALT);
+        }
+    }
+    a0 = (unsigned long long)warp_sum_ll((long long)a0);
+    b0 = (unsigned long long)warp_sum_ll((long long)b0);
+    a1 = (unsigned long long)warp_sum_ll((long long)a1);
+    b1 = (unsigned long long)warp_sum_ll((long long)b1);
+    if (lane == 0) {
+        atomicAdd(sums + 0, a0);
+        atomicAdd(sums + 1, b0);
+        atomicAdd(sums + 2, a1);
+        atomicAdd(sums + 3, b1);
+    }
+}
+
 // Failure-detection probe: the barrier waits for gridDim.x + 1 arrivals, so no
 // CTA is ever released and each one leaves after wait_ns.
 __global__ void barrier_timeout_probe_kernel(Counters *c, unsigned long long wait_ns) {
@@ -1083,6 +1284,16 @@ cudaError_t level_grid_limit(const KernelConfig &kc, int *grid) {
         if (e) return e;
     }
     return grid_for((const void *)f.level_a, kc.threads, smem_bytes(kc), grid);
+}
+
+cudaError_t launch_symmetry_hash(const int *row_offsets, const int *col, int nodes, unsigned long long *sums,
+                                 cudaStream_t stream) {
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (!e) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e) return e;
+    symmetry_hash_kernel<<<sms * 8, 256, 0, stream>>>(row_offsets, col, nodes, sums);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_fused(const BfsParams &p, const KernelConfig &kc, int grid, cudaStream_t stream) {

@@ -28,7 +28,7 @@ struct LevelRecord {
     unsigned frontier;
     unsigned chunks;
     unsigned wchunks;
-    unsigned pad;
+    unsigned bottom_up;  // 1 when the level ran bottom-up (direction-optimizing)
 };
 
 // Everything a BFS kernel needs, passed by value.
@@ -55,6 +55,14 @@ struct BfsParams {
     int warp_th;  // lists >= warp_th are cut into warp chunks; shorter ones go through a warp scan
     int cta_th;   // lists >= cta_th are cut into CTA chunks
     unsigned cull_flags;
+    // Direction-optimizing expand-contract (fused only; the graph must be
+    // symmetric): a level runs bottom-up once the frontier's edges exceed the
+    // unvisited vertices' edges / do_alpha, and returns to top-down once the
+    // frontier holds fewer than nodes / do_beta vertices and shrinks.
+    // do_alpha = 0: top-down only.
+    unsigned do_alpha;
+    unsigned do_beta;
+    long long edges;  // CSR entries (for the unvisited-edge count)
 };
 
 // Edges per CTA chunk: four passes of one 16-byte load per thread of a CTA.
@@ -75,6 +83,11 @@ cudaError_t launch_search_init(const BfsParams &p, const KernelConfig &kc, cudaS
 cudaError_t fused_grid_limit(const KernelConfig &kc, int *grid);
 // Grid of the per-level kernels (SMs x occupancy).
 cudaError_t level_grid_limit(const KernelConfig &kc, int *grid);
+// Two 64-bit hash sums over the CSR's entries, of (u, v) and of (v, u); equal
+// sums mean the graph is symmetric (up to a hash collision).  sums[0..3] must
+// start at zero.
+cudaError_t launch_symmetry_hash(const int *row_offsets, const int *col, int nodes, unsigned long long *sums,
+                                 cudaStream_t stream);
 // Cooperative launch of the persistent kernel that runs every BFS level.
 cudaError_t launch_fused(const BfsParams &p, const KernelConfig &kc, int grid, cudaStream_t stream);
 // Builds a graph whose conditional-while node runs one BFS level per pass:

@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(THREADS, MS_MIN_BLOCKS(THREADS)) ms_fused_kern
                 r.frontier = nq;
                 r.chunks = nch;
                 r.wchunks = nw;
-                r.pad = 0;
+                r.bottom_up = 0;
                 p.levels[L] = r;
             }
         }

@@ -142,9 +142,20 @@ int b40c_enactor_set_level_log(b40c_enactor_t *enactor, int enable);
  * NULL); *count gets the number copied, the last one being the end marker
  * (all counts 0).  frontier counts queued vertices (edge-frontier strategies:
  * queued edges); lists long enough to be cut into chunks are counted in
- * chunks / wchunks instead.  Levels of the two-phase strategy are its phases. */
+ * chunks / wchunks instead; bottom_up is 1 for a level that ran bottom-up.
+ * Levels of the two-phase strategy are its phases. */
 int b40c_enactor_level_log(b40c_enactor_t *enactor, int max_records, int64_t *t_start_ns,
-                           int *frontier, int *chunks, int *wchunks, int *count);
+                           int *frontier, int *chunks, int *wchunks, int *bottom_up, int *count);
+/* Direction-optimizing expand-contract (an addition; the reference's
+ * expand-contract is top-down only): a level runs bottom-up -- each unvisited
+ * vertex scans its list for a parent in the frontier -- once the frontier's
+ * edges exceed the unvisited vertices' edges / alpha, and returns to top-down
+ * once the frontier holds fewer than nodes / beta vertices and shrinks
+ * (Beamer, Asanovic and Patterson, SC 2012).  Defaults alpha = 14, beta = 24;
+ * alpha = 0 turns it off.  It applies to fused searches with depth labels on
+ * symmetric graphs, checked once per graph on the device; other searches stay
+ * top-down.  Labels, search depth and total_queued are those of top-down. */
+int b40c_enactor_set_direction_optimizing(b40c_enactor_t *enactor, int alpha, int beta);
 /* Spin limit of every device-side wait (grid barrier), in microseconds. */
 int b40c_enactor_set_wait_limit_us(b40c_enactor_t *enactor, long long us);
 

@@ -305,3 +305,84 @@ def test_hybrid_switches_between_bodies(cuda_device, oracle, rmat16):
         phases[grid] = len(en.level_log()) - 1  # the last record marks the end
     assert phases[1] > d + 1          # two-phase levels ran
     assert phases[0] <= phases[1]     # the full grid runs at least as many levels in one phase
+
+
+def _ec_search(prob, g, src, alpha, log=True):
+    b = bfs_mod()
+    en = b.EnactorExpandContract()
+    en.set_direction_optimizing(alpha, 24 if alpha else 0)
+    en.set_level_log(log)
+    b.check(prob.Reset(en.GetFrontierType(), 1.0))
+    b.check(en.EnactSearch(prob, int(src)))
+    return prob.labels(), en.GetStatistics(), en.level_log() if log else []
+
+
+@pytest.mark.parametrize("graph", ["rmat16", "er", "grid2d", "rmat_sparse"])
+def test_direction_optimizing_matches_top_down(cuda_device, oracle, rmat16, graph):
+    """Bottom-up levels change neither labels nor search depth nor total_queued."""
+    b = bfs_mod()
+    g = {"rmat16": lambda: rmat16, "er": lambda: b.erdos_renyi(20000, 24 / 19999, seed=6),
+         "grid2d": lambda: b.grid2d(200), "rmat_sparse": lambda: b.rmat(15, 2, seed=9)}[graph]()
+    prob = b.CsrProblem(False).from_graph(g)
+    for s in g.sample_sources(3, 17):
+        ref, _ = oracle.bfs(g, int(s))
+        td_labels, td_stats, td_log = _ec_search(prob, g, s, 0)
+        do_labels, do_stats, do_log = _ec_search(prob, g, s, 14)
+        assert oracle.first_mismatch(td_labels, ref) == -1
+        assert oracle.first_mismatch(do_labels, ref) == -1
+        assert do_stats[1] == td_stats[1] == int(ref.max())
+        assert not any(r["bottom_up"] for r in td_log)
+        if graph in ("rmat16", "er"):
+            assert any(r["bottom_up"] for r in do_log), do_log
+
+
+def test_direction_optimizing_low_alpha_runs_most_levels_bottom_up(cuda_device, oracle, rmat16):
+    """alpha = 1, beta = 1: bottom-up from the first level whose frontier edges
+    exceed the unvisited edges, and it stays there."""
+    b = bfs_mod()
+    g = rmat16
+    prob = b.CsrProblem(False).from_graph(g)
+    en = b.EnactorExpandContract()
+    en.set_direction_optimizing(1, 1)
+    en.set_level_log(True)
+    for s in g.sample_sources(4, 21):
+        ref, _ = oracle.bfs(g, int(s))
+        b.check(prob.Reset(en.GetFrontierType(), 1.0))
+        b.check(en.EnactSearch(prob, int(s)))
+        assert oracle.first_mismatch(prob.labels(), ref) == -1
+        assert any(r["bottom_up"] for r in en.level_log())
+
+
+def test_direction_optimizing_skips_directed_graphs(cuda_device, oracle):
+    """A directed graph fails the symmetry check and is searched top-down only."""
+    b = bfs_mod()
+    path = [p for p in golden_paths() if p.stem == "ref_random_3000_d"][0]
+    g, sources, golden, _ = load_golden(path)
+    prob = b.CsrProblem(False).from_graph(g)
+    for i, s in enumerate(sources[:3]):
+        labels, _, log = _ec_search(prob, g, s, 1)
+        assert np.array_equal(labels, golden[i])
+        assert not any(r["bottom_up"] for r in log)
+
+
+def test_direction_optimizing_with_predecessors_stays_top_down(cuda_device, oracle, rmat16):
+    b = bfs_mod()
+    g = rmat16
+    s = int(g.sample_sources(1, 23)[0])
+    ref, _ = oracle.bfs(g, s)
+    prob = b.CsrProblem(True).from_graph(g)
+    preds, _, log = _ec_search(prob, g, s, 1)
+    assert oracle.check_predecessors(g, preds, ref)[0] == -1
+    assert not any(r["bottom_up"] for r in log)
+
+
+def test_direction_switch_arguments(cuda_device):
+    b = bfs_mod()
+    en = b.EnactorExpandContract()
+    with pytest.raises(b.BfsError):
+        en.set_direction_optimizing(14, 0)
+    with pytest.raises(b.BfsError):
+        en.set_direction_optimizing(-1, 24)
+    with pytest.raises(b.BfsError):
+        b.EnactorContractExpand().set_direction_optimizing(14, 24)
+    b.EnactorContractExpand().set_direction_optimizing(0, 0)
