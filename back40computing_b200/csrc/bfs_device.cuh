@@ -57,7 +57,8 @@ struct alignas(256) Counters {
     // phase q (mf: the sum of their degrees, nf: their number), at [q&3].
     unsigned long long mf[4];
     unsigned nf[4];
-    unsigned pad_f[52];
+    unsigned zmarked;  // vertices without edges that bottom-up levels marked visited (whole search)
+    unsigned pad_f[51];
     unsigned bar_count;  // grid barrier
     unsigned bar_gen;
     unsigned pad_g[61];

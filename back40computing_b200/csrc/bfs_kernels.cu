@@ -623,57 +623,131 @@ __device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, u
 // Bottom-up level it of direction-optimizing BFS (Beamer, Asanovic and
 // Patterson, "Direction-Optimizing Breadth-First Search", SC 2012): every
 // unvisited vertex looks for a neighbour at depth it, and the first one found
-// makes it a depth-(it+1) vertex.  Warp w of the grid takes visited-mask
-// words w, w + W, ...; lane j takes the word's vertex 32w + j and scans its
-// list 4 entries at a time until a parent turns up.  A word has one writer in
-// the level, so its new bits are a plain store.  Vertices without edges are
+// makes it a depth-(it+1) vertex.
+//
+// A warp takes BU_WORDS consecutive mask words per step; lane j owns vertex
+// 32w + j of each word w and scans its list BU_PROBE entries per round until a
+// parent turns up; rounds are software-pipelined (the entries of round k+1 are
+// loaded before round k's probes are tested).  A word has one writer in the
+// level, so its new bits are a plain store.  Vertices without edges are
 // marked visited but never labelled: on a symmetric graph no list leads to
 // them, and later bottom-up levels skip them.  The discovered vertices are
-// counted and placed for level it+1 exactly as top-down discovery places them,
-// so either direction can run next.  Depth labels only (no predecessors).
+// counted and placed for level it+1 exactly as top-down discovery places
+// them, so either direction can run next.  Depth labels only.
+constexpr int BU_WORDS = 4;  // = the 4 lists per lane that place4 and stage4 take
+constexpr int BU_PROBE = 2;
+static_assert(BU_WORDS == 4, "bottom-up steps hand 4 vertices per lane to place4 / stage4");
+
+// One bottom-up step: visited-mask words w0 .. w0 + BU_WORDS - 1.
 template <int THREADS, bool MP>
-__device__ void bu_level(const BfsParams &p, int it, Smem<THREADS, MP> &sm) {
+__device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0, unsigned nwords, WarpSmem<MP> &ws,
+                                        int *q_out, unsigned *qlen_out) {
+    Counters *c = p.ctr;
+    const int lane = lane_id();
+    unsigned mw[BU_WORDS];
+#pragma unroll
+    for (int j = 0; j < BU_WORDS; j++) mw[j] = w0 + j < nwords ? ld_cg(p.mask + w0 + j) : FULL;
+    bool any_open = false;
+#pragma unroll
+    for (int j = 0; j < BU_WORDS; j++) any_open |= mw[j] != FULL;
+    if (!any_open) return;  // warp-uniform
+    int v[BU_WORDS], st[BU_WORDS], ln[BU_WORDS];
+    unsigned open = 0, scan = 0, found = 0;
+#pragma unroll
+    for (int j = 0; j < BU_WORDS; j++) {
+        v[j] = int((w0 + j) * 32u) + lane;
+        st[j] = 0;
+        ln[j] = 0;
+        if (v[j] < p.nodes && !((mw[j] >> lane) & 1u)) {
+            open |= 1u << j;
+            row_range(p, v[j], st[j], ln[j]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < BU_WORDS; j++)
+        if (((open >> j) & 1u) && ln[j] > 0) scan |= 1u << j;
+    // Probes are ordinary (L1-cached) label loads: the depth-it labels they
+    // look for were written before the level's grid barrier, whose
+    // release/acquire orders them before these loads; labels written during
+    // this level are it+1 and never match.
+    int u[BU_WORDS][BU_PROBE];
+#pragma unroll
+    for (int j = 0; j < BU_WORDS; j++)
+#pragma unroll
+        for (int e = 0; e < BU_PROBE; e++)
+            u[j][e] = ((scan >> j) & 1u) && e < ln[j] ? __ldg(p.col + st[j] + e) : -1;
+    for (int k = 0; __any_sync(FULL, scan != 0u); k += BU_PROBE) {
+        int un[BU_WORDS][BU_PROBE];
+#pragma unroll
+        for (int j = 0; j < BU_WORDS; j++)
+#pragma unroll
+            for (int e = 0; e < BU_PROBE; e++) {
+                const int kk = k + BU_PROBE + e;
+                un[j][e] = ((scan >> j) & 1u) && kk < ln[j] ? __ldg(p.col + st[j] + kk) : -1;
+            }
+#pragma unroll
+        for (int j = 0; j < BU_WORDS; j++) {
+#pragma unroll
+            for (int e = 0; e < BU_PROBE; e++) {
+                if (((scan >> j) & 1u) && k + e < ln[j]) {
+                    const unsigned x = (unsigned)u[j][e];
+                    if (x < (unsigned)p.nodes) {
+                        if (__ldca(p.labels + x) == it) found |= 1u << j;
+                    } else {
+                        atomicOr(&c->error, ERR_BAD_VERTEX);
+                    }
+                }
+            }
+            if (((found >> j) & 1u) || k + BU_PROBE >= ln[j]) scan &= ~(1u << j);
+        }
+#pragma unroll
+        for (int j = 0; j < BU_WORDS; j++)
+#pragma unroll
+            for (int e = 0; e < BU_PROBE; e++) u[j][e] = un[j][e];
+    }
+    int nfound = 0;
+    long long dfound = 0;
+#pragma unroll
+    for (int j = 0; j < BU_WORDS; j++) {
+        const bool f = (found >> j) & 1u;
+        const unsigned fb = __ballot_sync(FULL, f);
+        const unsigned zb = __ballot_sync(FULL, ((open >> j) & 1u) && ln[j] == 0);
+        if (lane == 0 && (fb | zb)) __stcg(p.mask + w0 + j, mw[j] | fb | zb);
+        if (lane == 0 && zb) atomicAdd(&c->zmarked, unsigned(__popc(zb)));
+        if (f) {
+            p.labels[v[j]] = it + 1;
+            nfound++;
+            dfound += ln[j];
+        }
+    }
+    count_discovered(ws, nfound, dfound);
+    const unsigned placed = place4<THREADS>(p, it + 1, found, st, ln, v);
+    stage4(ws, found & ~placed, v, q_out, qlen_out, p.qcap, &c->error);
+}
+
+// open: an estimate of the vertices still unvisited.
+template <int THREADS, bool MP>
+__device__ void bu_level(const BfsParams &p, int it, Smem<THREADS, MP> &sm, unsigned open) {
     static_assert(!MP, "bottom-up levels test depth labels");
     Counters *c = p.ctr;
     int *q_out = p.queue[(it + 1) & 1];
     unsigned *qlen_out = &c->qlen[(it + 1) & 3];
     WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
     const unsigned nwords = (unsigned(p.nodes) + 31u) >> 5;
+    const unsigned nsteps = (nwords + BU_WORDS - 1) / BU_WORDS;
     const unsigned W = grid_warps();
-    const int lane = lane_id();
-    for (unsigned w = global_warp(); w < nwords; w += W) {
-        const unsigned mword = ld_cg(p.mask + w);
-        if (mword == FULL) continue;  // warp-uniform
-        const int v = int(w * 32u) + lane;
-        const bool open = v < p.nodes && !((mword >> lane) & 1u);
-        int start = 0, len = 0;
-        if (open) row_range(p, v, start, len);
-        bool scan = open && len > 0, found = false;
-        for (int k = 0; __any_sync(FULL, scan); k += 4) {
-            if (scan) {
-                int u[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) u[j] = k + j < len ? __ldg(p.col + start + k + j) : -1;
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    if (k + j < len) {
-                        if ((unsigned)u[j] < (unsigned)p.nodes) {
-                            found |= ld_cg(p.labels + u[j]) == it;
-                        } else {
-                            atomicOr(&c->error, ERR_BAD_VERTEX);
-                        }
-                    }
-                }
-                if (found || k + 4 >= len) scan = false;
-            }
-        }
-        const unsigned fb = __ballot_sync(FULL, found), zb = __ballot_sync(FULL, open && len == 0);
-        if (lane == 0 && (fb | zb)) __stcg(p.mask + w, mword | fb | zb);
-        if (found) p.labels[v] = it + 1;
-        count_discovered(ws, found ? 1 : 0, found ? len : 0);
-        const bool placed = place1<THREADS>(p, it + 1, found, start, len, v);
-        const int vv[4] = {v, 0, 0, 0};
-        stage4(ws, (found && !placed) ? 1u : 0u, vv, q_out, qlen_out, p.qcap, &c->error);
+    // While many vertices are open, steps go one per warp, then to whichever
+    // warp is free (a step's cost depends on how long its lists scan, so a
+    // static split leaves most warps waiting at the level's barrier for a few
+    // slow ones); a warp asks for its next step when it starts one, hiding the
+    // atomic's latency.  Once few are open, most steps only read full mask
+    // words, and a static interleave spares the counter its atomics.
+    const bool dynamic = nsteps > W && (unsigned long long)open * 8ull > (unsigned long long)p.nodes;
+    for (unsigned step = global_warp(); step < nsteps;) {
+        unsigned nxt = 0;
+        if (dynamic && lane_id() == 0) nxt = atomicAdd(&c->steal[it & 3], 1u);
+        bu_step<THREADS, MP>(p, it, step * BU_WORDS, nwords, ws, q_out, qlen_out);
+        step = dynamic ? W + __shfl_sync(FULL, nxt, 0) : step + W;
     }
     stage_drain(ws, q_out, qlen_out, p.qcap, &c->error);
     flush_discovered(p, ws, it + 1);
@@ -870,11 +944,13 @@ __device__ __forceinline__ void finish_search(const BfsParams &p, int iteration,
 // reads the same counters after a barrier, so all take the same direction.
 struct DirectionChoice {
     unsigned long long explored = 0;  // degrees summed over the vertices visited so far
+    unsigned visited = 0;             // vertices visited so far
     unsigned prev_nf = 0;
     bool bottom_up = false;
 
     __device__ __forceinline__ bool next(const BfsParams &p, unsigned nf, unsigned long long mf) {
         explored += mf;
+        visited += nf;
         const unsigned long long total = (unsigned long long)p.edges;
         const unsigned long long unexplored = total > explored ? total - explored : 0ull;
         if (!bottom_up) bottom_up = mf * p.do_alpha > unexplored;
@@ -903,7 +979,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
             log_phase(p, it, L, nch, nw, bottom_up ? 1u : 0u);
         }
         if constexpr (!MP) {
-            if (bottom_up) bu_level<THREADS, MP>(p, it, sm);
+            if (bottom_up) {
+                const unsigned done = dir.visited + ld_cg(&c->zmarked);
+                bu_level<THREADS, MP>(p, it, sm, done < unsigned(p.nodes) ? unsigned(p.nodes) - done : 0u);
+            }
             else ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
         } else {
             ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
