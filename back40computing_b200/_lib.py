@@ -65,6 +65,8 @@ SIGNATURES = {
     "b40c_batch_add_graph": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, POINTER(c_int)]),
     "b40c_batch_set_policy": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
     "b40c_batch_set_stream": (c_int, [c_void_p, c_void_p]),
+    "b40c_batch_set_direction_optimizing": (c_int, [c_void_p, c_int, c_int]),
+    "b40c_server_set_direction_optimizing": (c_int, [c_void_p, c_int, c_int]),
     "b40c_batch_run": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int]),
     "b40c_batch_run_async": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int]),
     "b40c_batch_sync": (c_int, [c_void_p]),

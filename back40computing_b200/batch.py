@@ -50,6 +50,10 @@ class BfsBatch:
         check(lib().b40c_batch_set_policy(self._h, cta_threads, warp_gather_threshold, cta_gather_threshold,
                                           cull_flags))
 
+    def set_direction_optimizing(self, alpha: int = 14, beta: int = 24) -> None:
+        """Bottom-up levels per search on symmetric graphs (alpha = 0: off)."""
+        check(lib().b40c_batch_set_direction_optimizing(self._h, int(alpha), int(beta)))
+
     def set_stream(self, stream_handle: int | None) -> None:
         check(lib().b40c_batch_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)))
 

@@ -58,7 +58,8 @@ struct alignas(256) Counters {
     unsigned long long mf[4];
     unsigned nf[4];
     unsigned zmarked;  // vertices without edges that bottom-up levels marked visited (whole search)
-    unsigned pad_f[51];
+    unsigned bu_steal[4];  // multi-search: next bottom-up step of level q, at [q&3]
+    unsigned pad_f[47];
     unsigned bar_count;  // grid barrier
     unsigned bar_gen;
     unsigned pad_g[61];

@@ -46,6 +46,7 @@ struct GraphRes {
     int *d_col = nullptr;
     int nodes = 0;
     long long edges = 0;
+    int symmetric = 0;
 };
 
 }  // namespace
@@ -55,6 +56,7 @@ struct b40c_batch {
     bool mark_pred = false;
     int threads = 256, warp_th = 128, cta_th = 1024;
     unsigned cull_flags = CULL_HISTORY;
+    unsigned do_alpha = 14, do_beta = 24;  // direction-optimizing (published alpha, beta); 0: top-down only
     unsigned long long wait_ns = 5000000000ull;
     std::vector<GraphRes> graphs;
     MsGraph *d_graphs = nullptr;
@@ -81,6 +83,16 @@ struct b40c_batch {
     size_t wchunk_cap[2] = {0, 0};
     int2 *d_admit = nullptr;
     size_t admit_cap = 0;
+    unsigned *d_nf = nullptr;  // direction-optimizing state, per slot
+    size_t nf_cap = 0;
+    unsigned long long *d_mf = nullptr;
+    size_t mf_cap = 0;
+    MsDir *d_dir = nullptr;
+    size_t dir_cap = 0;
+    unsigned char *d_bu = nullptr;
+    size_t bu_cap = 0;
+    unsigned *d_bu_prefix = nullptr;
+    size_t bu_prefix_cap = 0;
     Counters *d_ctr = nullptr;
     Counters *h_ctr = nullptr;
     MsSlotState *h_state = nullptr;  // pinned
@@ -203,6 +215,11 @@ extern "C" int b40c_batch_destroy(b40c_batch_t *b) {
         cudaFree(b->d_wchunks[i]);
     }
     cudaFree(b->d_admit);
+    cudaFree(b->d_nf);
+    cudaFree(b->d_mf);
+    cudaFree(b->d_dir);
+    cudaFree(b->d_bu);
+    cudaFree(b->d_bu_prefix);
     cudaFree(b->d_ctr);
     cudaFreeHost(b->h_ctr);
     cudaFreeHost(b->h_state);
@@ -237,17 +254,27 @@ extern "C" int b40c_batch_add_graph(b40c_batch_t *b, int nodes, int edges, const
     CUDA_TRY(cudaMemcpy(g.d_row, h_row, sizeof(int) * (size_t(nodes) + 1), cudaMemcpyHostToDevice), "upload");
     CUDA_TRY(cudaMemset(g.d_col + edges, 0, 4 * sizeof(int)), "column padding");
     if (edges) CUDA_TRY(cudaMemcpy(g.d_col, h_col, sizeof(int) * size_t(edges), cudaMemcpyHostToDevice), "upload");
+    CUDA_TRY(ms_graph_symmetric(g.d_row, g.d_col, nodes, &g.symmetric), "graph symmetry check");
     b->graphs.push_back(g);
     // Refresh the device graph table.
     std::vector<MsGraph> table(b->graphs.size());
     for (size_t i = 0; i < b->graphs.size(); i++)
         table[i] = MsGraph{b->graphs[i].d_row, b->graphs[i].d_col, b->graphs[i].nodes,
-                           int(b->graphs[i].edges + 4)};
+                           int(b->graphs[i].edges + 4), int(b->graphs[i].edges), b->graphs[i].symmetric};
     int rc = grow(&b->d_graphs, &b->graphs_cap, table.size(), "batch graph table");
     if (rc) return rc;
     CUDA_TRY(cudaMemcpy(b->d_graphs, table.data(), sizeof(MsGraph) * table.size(), cudaMemcpyHostToDevice),
              "graph table upload");
     *graph_id = int(b->graphs.size()) - 1;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_batch_set_direction_optimizing(b40c_batch_t *b, int alpha, int beta) {
+    clear_error();
+    if (!b || alpha < 0 || beta < 0 || (alpha > 0 && beta == 0))
+        return set_error(B40C_ERR_INVALID_VALUE, "direction switch: alpha >= 0, and beta >= 1 when alpha > 0");
+    b->do_alpha = unsigned(alpha);
+    b->do_beta = unsigned(beta);
     return B40C_SUCCESS;
 }
 
@@ -324,6 +351,12 @@ extern "C" int b40c_batch_run_async(b40c_batch_t *b, int num_searches, const int
     if ((rc = grow(&b->d_state, &b->state_cap, size_t(num_searches), "batch slot states"))) return rc;
     if ((rc = grow(&b->d_alive, &b->alive_cap, 4 * size_t(num_searches), "batch alive flags"))) return rc;
     if ((rc = grow(&b->d_admit, &b->admit_cap, size_t(num_searches), "batch sources"))) return rc;
+    const size_t S = size_t(num_searches);
+    if ((rc = grow(&b->d_nf, &b->nf_cap, 4 * S, "batch direction counts"))) return rc;
+    if ((rc = grow(&b->d_mf, &b->mf_cap, 4 * S, "batch direction degree sums"))) return rc;
+    if ((rc = grow(&b->d_dir, &b->dir_cap, S, "batch direction states"))) return rc;
+    if ((rc = grow(&b->d_bu, &b->bu_cap, S, "batch bottom-up flags"))) return rc;
+    if ((rc = grow(&b->d_bu_prefix, &b->bu_prefix_cap, S + 1, "batch bottom-up steps"))) return rc;
     for (int i = 0; i < 2; i++) {
         if ((rc = grow(&b->d_queue[i], &b->queue_cap[i], labels_total + 1, "batch frontier"))) return rc;
         if ((rc = grow(&b->d_chunks[i], &b->chunk_cap[i], chunks_need, "batch CTA chunks"))) return rc;
@@ -356,6 +389,13 @@ extern "C" int b40c_batch_run_async(b40c_batch_t *b, int num_searches, const int
     p.cta_th = std::max(b->cta_th, b->warp_th);
     p.cull_flags = b->cull_flags;
     p.max_levels = 0;
+    p.do_alpha = b->mark_pred ? 0u : b->do_alpha;
+    p.do_beta = b->do_beta;
+    p.nf = b->d_nf;
+    p.mf = b->d_mf;
+    p.dir = b->d_dir;
+    p.bu = b->d_bu;
+    p.bu_prefix = b->d_bu_prefix;
     const bool params_changed = grew || std::memcmp(&p, &b->params, sizeof(MsParams)) != 0 || grid != b->grid;
     b->params = p;
     b->grid = grid;

@@ -42,6 +42,7 @@ template <int THREADS, bool MP>
 struct MsSmem {
     MsWarp<MP> w[THREADS / 32];
     unsigned long long vcache[VCACHE];  // (global mask word << 32) | word value
+    unsigned warp_tot[THREADS / 32];    // bookkeeping scan of bottom-up steps
     unsigned flag;
 };
 
@@ -178,6 +179,31 @@ __device__ __forceinline__ void ms_stage4(MsWarp<MP> &ws, unsigned flags, const 
     __syncwarp();
 }
 
+// ---- direction-optimizing counts ------------------------------------------------------------
+
+// Adds discovered vertices (bit j of disc: vertex of slot sl[j] with ln[j]
+// edges) to their slots' counters of level q: lanes holding the same slot are
+// grouped by __match_any_sync and their group leader adds the group's count
+// and degree sum (degrees of distinct vertices of one graph: the sum stays
+// below the graph's edge count, which fits in 32 bits).
+__device__ __forceinline__ void count_slot_discoveries(const MsParams &p, int q, unsigned disc, const int (&ln)[4],
+                                                       const int (&sl)[4]) {
+    const unsigned lane = lane_id();
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const bool d = (disc >> j) & 1u;
+        const unsigned peers = __match_any_sync(FULL, d ? (unsigned)sl[j] : (0x80000000u | lane));
+        if (d) {
+            const unsigned sum = __reduce_add_sync(peers, (unsigned)ln[j]);
+            if (lane == unsigned(__ffs(peers) - 1)) {
+                const size_t at = size_t(q & 3) * size_t(p.nslots) + size_t(sl[j]);
+                atomicAdd(p.nf + at, unsigned(__popc(peers)));
+                atomicAdd(p.mf + at, (unsigned long long)sum);
+            }
+        }
+    }
+}
+
 // ---- the multi-search sink ---------------------------------------------------------------
 
 // Expand-contract discovery for elements of possibly different slots: bit j
@@ -236,6 +262,7 @@ struct MsSink {
                 }
             }
         }
+        if (p.do_alpha) count_slot_discoveries(p, level + 1, disc, ln, sl);
         const unsigned enq = disc & ~ms_place4<THREADS>(p, level + 1, disc, st, ln, u, sl);
         const int nq = (level + 1) & 1;
         ms_stage4(sm.w[threadIdx.x >> 5], enq, u, sl, p.queue[nq], &p.ctr->qlen[(level + 1) & 3], p.qcap,
@@ -268,7 +295,7 @@ __device__ void ms_level(const MsParams &p, int L, unsigned nq_in, unsigned nch,
         const int4 *t = p.chunks[L & 1];
         for (unsigned k = blockIdx.x; k < n; k += gridDim.x) {
             const int4 c = __ldcg(t + k);
-            if (c.y <= 0) continue;
+            if (c.y <= 0 || (p.do_alpha && p.bu[c.w])) continue;  // a bottom-up slot sweeps its mask instead
             const MsGraph g = p.graphs[load_slot(p, c.w).graph];
             MsSlotSink<THREADS, MP> ss{sink, c.w};
             gather_list<THREADS>(g.col, g.vec_end, c.x, c.y, c.z, 0u, threadIdx.x, ss, pol);
@@ -281,7 +308,7 @@ __device__ void ms_level(const MsParams &p, int L, unsigned nq_in, unsigned nch,
         const unsigned W = grid_warps();
         for (unsigned k = global_warp(); k < n; k += W) {
             const int4 c = __ldcg(t + k);
-            if (c.y <= 0) continue;
+            if (c.y <= 0 || (p.do_alpha && p.bu[c.w])) continue;
             const MsGraph g = p.graphs[load_slot(p, c.w).graph];
             MsSlotSink<THREADS, MP> ss{sink, c.w};
             gather_list<32>(g.col, g.vec_end, c.x, c.y, c.z, 0u, lane_id(), ss, pol);
@@ -300,7 +327,7 @@ __device__ void ms_level(const MsParams &p, int L, unsigned nq_in, unsigned nch,
         int slot = 0, v = -1, start = 0, len = 0;
         const int *col = nullptr;
         int vec_end = 0;
-        if (idx < nq_in) {
+        if (idx < nq_in && !(p.do_alpha && p.bu[__ldcg(&q_in[idx].x)])) {
             const int2 e = __ldcg(q_in + idx);
             slot = e.x;
             v = e.y;
@@ -360,6 +387,179 @@ __device__ void ms_level(const MsParams &p, int L, unsigned nq_in, unsigned nch,
     __syncwarp();
 }
 
+// ---- bottom-up levels ------------------------------------------------------------------
+
+// Bottom-up step of slot s (direction-optimizing BFS, Beamer, Asanovic and
+// Patterson, SC 2012; the single-search bu_step of bfs_kernels.cu with slot
+// offsets): mask words w0 .. w0+3 of the slot; lane j owns vertex 32w + j of
+// each word and scans its list 2 entries per round, software-pipelined, for a
+// neighbour at the slot's depth L - start_level.  Label probes are ordinary
+// (L1-cached) loads, ordered after the labels they look for by the grid
+// barriers before the level.  A word has one writer in the level.
+template <int THREADS, bool MP>
+__device__ __forceinline__ void ms_bu_step(const MsParams &p, int L, int s, unsigned w0, MsWarp<MP> &ws) {
+    const MsSlot d = load_slot(p, s);
+    const MsGraph g = p.graphs[d.graph];
+    const unsigned nwords = (unsigned(d.nodes) + 31u) >> 5;
+    unsigned *mask = p.mask + d.mask_off;
+    int *labels = p.labels + d.label_off;
+    const int depth = L - d.start_level;
+    const int lane = lane_id();
+    unsigned mw[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) mw[j] = w0 + j < nwords ? ld_cg(mask + w0 + j) : FULL;
+    if (mw[0] == FULL && mw[1] == FULL && mw[2] == FULL && mw[3] == FULL) return;  // warp-uniform
+    int v[4], st[4], ln[4];
+    unsigned open = 0, scan = 0, found = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        v[j] = int((w0 + j) * 32u) + lane;
+        st[j] = 0;
+        ln[j] = 0;
+        if (v[j] < d.nodes && !((mw[j] >> lane) & 1u)) {
+            open |= 1u << j;
+            st[j] = __ldg(g.row + v[j]);
+            ln[j] = __ldg(g.row + v[j] + 1) - st[j];
+            if (ln[j] > 0) scan |= 1u << j;
+        }
+    }
+    int u[4][2];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) u[j][e] = ((scan >> j) & 1u) && e < ln[j] ? __ldg(g.col + st[j] + e) : -1;
+    for (int k = 0; __any_sync(FULL, scan != 0u); k += 2) {
+        int un[4][2];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 2; e++)
+                un[j][e] = ((scan >> j) & 1u) && k + 2 + e < ln[j] ? __ldg(g.col + st[j] + k + 2 + e) : -1;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                if (((scan >> j) & 1u) && k + e < ln[j]) {
+                    const unsigned x = (unsigned)u[j][e];
+                    if (x < (unsigned)d.nodes) {
+                        if (__ldca(labels + x) == depth) found |= 1u << j;
+                    } else {
+                        atomicOr(&p.ctr->error, ERR_BAD_VERTEX);
+                    }
+                }
+            }
+            if (((found >> j) & 1u) || k + 2 >= ln[j]) scan &= ~(1u << j);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) u[j][e] = un[j][e];
+    }
+    unsigned nfound = 0, dfound = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const bool f = (found >> j) & 1u;
+        const unsigned fb = __ballot_sync(FULL, f);
+        const unsigned zb = __ballot_sync(FULL, ((open >> j) & 1u) && ln[j] == 0);
+        if (lane == 0 && (fb | zb)) __stcg(mask + w0 + j, mw[j] | fb | zb);
+        if (f) {
+            labels[v[j]] = depth + 1;
+            nfound++;
+            dfound += unsigned(ln[j]);
+        }
+    }
+    nfound = __reduce_add_sync(FULL, nfound);
+    dfound = __reduce_add_sync(FULL, dfound);
+    if (nfound == 0u) return;  // warp-uniform
+    if (lane == 0) {
+        const size_t at = size_t((L + 1) & 3) * size_t(p.nslots) + size_t(s);
+        atomicAdd(p.nf + at, nfound);
+        atomicAdd(p.mf + at, (unsigned long long)dfound);
+        mark_alive(p, L + 1, s);
+    }
+    const int sl[4] = {s, s, s, s};
+    const unsigned placed = ms_place4<THREADS>(p, L + 1, found, st, ln, v, sl);
+    ms_stage4(ws, found & ~placed, v, sl, p.queue[(L + 1) & 1], &p.ctr->qlen[(L + 1) & 3], p.qcap, &p.ctr->error);
+}
+
+// The bottom-up steps of every bottom-up slot, numbered in slot order by
+// bu_prefix: a warp takes step g (first one per warp, then dynamically) and
+// finds its slot by binary search.
+template <int THREADS, bool MP>
+__device__ void ms_bu_level(const MsParams &p, int L, MsWarp<MP> &ws) {
+    const unsigned total = __ldcg(p.bu_prefix + p.nslots);
+    const unsigned W = grid_warps();
+    for (unsigned g = global_warp(); g < total;) {
+        unsigned nxt = 0;
+        if (total > W && lane_id() == 0) nxt = atomicAdd(&p.ctr->bu_steal[L & 3], 1u);
+        int lo = 0, hi = p.nslots;  // last s with bu_prefix[s] <= g
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldcg(p.bu_prefix + mid) <= g) lo = mid;
+            else hi = mid;
+        }
+        ms_bu_step<THREADS, MP>(p, L, lo, (g - __ldcg(p.bu_prefix + lo)) * 4u, ws);
+        g = total > W ? W + __shfl_sync(FULL, nxt, 0) : total;
+    }
+}
+
+// Direction of level L for every slot (block 0, before the level's work):
+// the rule of the single-search DirectionChoice applied to the slot's counts,
+// then bu_prefix as an exclusive scan of the bottom-up slots' step counts.
+// Also clears the counts level L+1 will fill into ring entry (L+2)&3.
+template <int THREADS, bool MP>
+__device__ void ms_directions(const MsParams &p, int L, MsSmem<THREADS, MP> &sm) {
+    __syncthreads();  // the retirements ms_bookkeeping just wrote are read below
+    const unsigned char *in = p.alive + size_t(L & 3) * size_t(p.nslots);
+    const int per = (p.nslots + THREADS - 1) / THREADS;
+    const int s0 = min(p.nslots, int(threadIdx.x) * per), s1 = min(p.nslots, s0 + per);
+    unsigned mine = 0;
+    for (int s = s0; s < s1; s++) {
+        const size_t at = size_t(L & 3) * size_t(p.nslots) + size_t(s);
+        const size_t clr = size_t((L + 2) & 3) * size_t(p.nslots) + size_t(s);
+        p.nf[clr] = 0u;
+        p.mf[clr] = 0ull;
+        bool bottom_up = false;
+        if (!MP && p.state[s].active && in[s]) {
+            const MsSlot d = load_slot(p, s);
+            const MsGraph g = p.graphs[d.graph];
+            MsDir dr = p.dir[s];
+            const unsigned nf = p.nf[at];
+            const unsigned long long mf = p.mf[at];
+            dr.explored += mf;
+            dr.visited += nf;
+            if (g.symmetric) {
+                const unsigned long long total = (unsigned long long)g.edges;
+                const unsigned long long unexplored = total > dr.explored ? total - dr.explored : 0ull;
+                if (!dr.bottom_up) bottom_up = mf * p.do_alpha > unexplored;
+                else bottom_up = !((unsigned long long)nf * p.do_beta < (unsigned long long)d.nodes && nf < dr.prev_nf);
+            }
+            dr.prev_nf = nf;
+            dr.bottom_up = bottom_up ? 1 : 0;
+            p.dir[s] = dr;
+            if (bottom_up) mine += ((unsigned(d.nodes) + 31u) / 32u + 3u) / 4u;
+        }
+        p.bu[s] = bottom_up ? 1 : 0;
+    }
+    // exclusive scan of the per-thread step counts, then the per-slot prefix
+    const unsigned incl = (unsigned)warp_inclusive_scan(int(mine));
+    if (lane_id() == 31) sm.warp_tot[threadIdx.x >> 5] = incl;
+    __syncthreads();
+    unsigned base = 0;
+    for (int w = 0; w < int(threadIdx.x >> 5); w++) base += sm.warp_tot[w];
+    unsigned run = base + incl - mine;
+    for (int s = s0; s < s1; s++) {
+        p.bu_prefix[s] = run;
+        if (p.bu[s]) {
+            const MsSlot d = load_slot(p, s);
+            run += ((unsigned(d.nodes) + 31u) / 32u + 3u) / 4u;
+        }
+    }
+    if (threadIdx.x == THREADS - 1) p.bu_prefix[p.nslots] = run;
+    if (threadIdx.x == 0) p.ctr->bu_steal[(L + 1) & 3] = 0u;
+    __syncthreads();
+}
+
 // One CTA retires the slots without input for level L and clears the alive
 // entries level L+1 will fill.  final_sweep: the batch has no work left, so
 // every active slot ends here.
@@ -409,6 +609,12 @@ __global__ void __launch_bounds__(THREADS, MS_MIN_BLOCKS(THREADS)) ms_fused_kern
         const bool empty = nq + nch + nw == 0u;
         if (blockIdx.x == 0) ms_bookkeeping(p, L, empty);
         if (empty || L >= L_end || (p.stop_on_retire && retired_before)) break;
+        // Direction-optimizing: every CTA needs the level's per-slot directions
+        // before it takes any work, so they are decided first, behind a barrier.
+        if (p.do_alpha) {
+            if (blockIdx.x == 0) ms_directions<THREADS, MP>(p, L, sm);
+            if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        }
         if (leader()) {
             ms_ring_prepare(c, L);
             if (p.levels && L < p.level_cap) {
@@ -422,6 +628,16 @@ __global__ void __launch_bounds__(THREADS, MS_MIN_BLOCKS(THREADS)) ms_fused_kern
             }
         }
         ms_level<THREADS, MP>(p, L, nq, nch, nw, sm, pol);
+        if constexpr (!MP) {  // bottom-up levels test depth labels
+            if (p.do_alpha) {
+                MsWarp<MP> &ws = sm.w[threadIdx.x >> 5];
+                ms_bu_level<THREADS, MP>(p, L, ws);
+            const unsigned n = ws.nbuf;
+            if (n) ms_flush(ws, n, p.queue[(L + 1) & 1], &c->qlen[(L + 1) & 3], p.qcap, &c->error);
+                if (lane_id() == 0) ws.nbuf = 0;
+                __syncwarp();
+            }
+        }
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         L++;
     }
@@ -456,6 +672,15 @@ __global__ void ms_admit_kernel(MsParams p, const int2 *slot_src, int count, int
     p.alive[size_t(L & 3) * size_t(p.nslots) + slot] = 1;
     const MsGraph g = p.graphs[d.graph];
     const int start = g.row[src], len = g.row[src + 1] - start;
+    if (p.do_alpha) {
+        MsDir dr = {};
+        p.dir[slot] = dr;
+        for (int q = 0; q < 4; q++) {
+            const size_t at = size_t(q) * size_t(p.nslots) + size_t(slot);
+            p.nf[at] = q == (L & 3) ? 1u : 0u;
+            p.mf[at] = q == (L & 3) ? (unsigned long long)len : 0ull;
+        }
+    }
     constexpr int CH = chunk_edges<THREADS>();
     const bool cta = len >= p.cta_th, wrp = !cta && len >= p.warp_th;
     if (cta || wrp) {
@@ -507,6 +732,17 @@ MsKernelFn pick(const MsKernelConfig &kc, size_t *smem) {
 }
 
 }  // namespace
+
+cudaError_t ms_graph_symmetric(const int *d_row, const int *d_col, int nodes, int *symmetric) {
+    unsigned long long *d = nullptr, h[4] = {0, 0, 0, 0};
+    cudaError_t e = cudaMalloc(&d, sizeof(h));
+    if (!e) e = cudaMemset(d, 0, sizeof(h));
+    if (!e) e = launch_symmetry_hash(d_row, d_col, nodes, d, 0);
+    if (!e) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (!e) *symmetric = (h[0] == h[1] && h[2] == h[3]) ? 1 : 0;
+    return e;
+}
 
 cudaError_t ms_grid_limit(const MsKernelConfig &kc, int *grid) {
     size_t smem = 0;

@@ -13,6 +13,18 @@ struct MsGraph {
     const int *col;  // edges (+4 padding)
     int nodes;
     int vec_end;     // 16-byte column loads are safe below this index
+    int edges;
+    int symmetric;   // 1: every entry has its reverse (bottom-up levels allowed)
+};
+
+// Direction-optimizing state of one search slot, updated at the start of
+// every level by the bookkeeping CTA.
+struct MsDir {
+    unsigned long long explored;  // degrees summed over the slot's visited vertices
+    unsigned visited;             // the slot's visited vertices
+    unsigned prev_nf;             // its frontier size at the previous level
+    int bottom_up;                // 1: the current level runs bottom-up
+    int pad;
 };
 
 struct MsSlot {
@@ -54,6 +66,18 @@ struct MsParams {
     unsigned cull_flags;
     int max_levels;  // levels to run in this launch before returning (<= 0: until no work)
     int stop_on_retire;  // return at the level after one where a search retired
+    // Direction-optimizing searches (do_alpha = 0: top-down only): per slot,
+    // the vertices discovered as input of level q (nf) and their degree sum
+    // (mf) at [(q & 3) * nslots + slot]; the direction state; the current
+    // level's bottom-up flag; and bu_prefix[s] = the bottom-up steps (4 mask
+    // words each) of the slots before s, bu_prefix[nslots] their total.
+    unsigned do_alpha;
+    unsigned do_beta;
+    unsigned *nf;
+    unsigned long long *mf;
+    MsDir *dir;
+    unsigned char *bu;
+    unsigned *bu_prefix;
 };
 
 struct MsKernelConfig {
@@ -61,6 +85,9 @@ struct MsKernelConfig {
     bool mark_pred;
 };
 
+// Whether a resident graph is symmetric (the hash check of
+// launch_symmetry_hash; allocates and frees a 32-byte buffer, waits).
+cudaError_t ms_graph_symmetric(const int *d_row, const int *d_col, int nodes, int *symmetric);
 // Largest co-resident grid of the multi-search kernel.
 cudaError_t ms_grid_limit(const MsKernelConfig &kc, int *grid);
 // Cooperative launch: runs levels from Counters::cur_it until no search has

@@ -89,6 +89,7 @@ struct ResidentGraph {
     int *d_col = nullptr;
     int nodes = 0;
     long long edges = 0;
+    int symmetric = 0;
 };
 
 struct SlotUse {
@@ -123,6 +124,12 @@ struct b40c_server {
     int4 *d_wchunks[2] = {nullptr, nullptr};
     int2 *d_admit = nullptr;
     int *d_clear = nullptr;
+    unsigned do_alpha = 14, do_beta = 24;  // direction-optimizing (published alpha, beta); 0: top-down only
+    unsigned *d_nf = nullptr;              // direction-optimizing state, per slot
+    unsigned long long *d_mf = nullptr;
+    MsDir *d_dir = nullptr;
+    unsigned char *d_bu = nullptr;
+    unsigned *d_bu_prefix = nullptr;
     Counters *d_ctr = nullptr;
     Counters *h_ctr = nullptr;
     MsSlot *h_slots = nullptr;
@@ -169,6 +176,11 @@ int server_alloc(b40c_server *s, long long budget) {
     CUDA_TRY(cudaMalloc(&s->d_admit, sizeof(int2) * S), "server admissions");
     CUDA_TRY(cudaMalloc(&s->d_clear, sizeof(int) * S), "server clears");
     CUDA_TRY(cudaMalloc(&s->d_ctr, sizeof(Counters)), "server counters");
+    CUDA_TRY(cudaMalloc(&s->d_nf, sizeof(unsigned) * 4 * S), "server direction counts");
+    CUDA_TRY(cudaMalloc(&s->d_mf, sizeof(unsigned long long) * 4 * S), "server direction degree sums");
+    CUDA_TRY(cudaMalloc(&s->d_dir, sizeof(MsDir) * S), "server direction states");
+    CUDA_TRY(cudaMalloc(&s->d_bu, S), "server bottom-up flags");
+    CUDA_TRY(cudaMalloc(&s->d_bu_prefix, sizeof(unsigned) * (S + 1)), "server bottom-up steps");
     CUDA_TRY(cudaHostAlloc(&s->h_ctr, sizeof(Counters), cudaHostAllocDefault), "server pinned counters");
     CUDA_TRY(cudaHostAlloc(&s->h_slots, sizeof(MsSlot) * S, cudaHostAllocDefault), "server pinned slots");
     CUDA_TRY(cudaHostAlloc(&s->h_state, sizeof(MsSlotState) * S, cudaHostAllocDefault), "server pinned states");
@@ -207,6 +219,13 @@ void fill_params(b40c_server *s) {
     p.cull_flags = s->cull_flags;
     p.max_levels = s->epoch_levels;
     p.stop_on_retire = 1;
+    p.do_alpha = s->mark_pred ? 0u : s->do_alpha;
+    p.do_beta = s->do_beta;
+    p.nf = s->d_nf;
+    p.mf = s->d_mf;
+    p.dir = s->d_dir;
+    p.bu = s->d_bu;
+    p.bu_prefix = s->d_bu_prefix;
 }
 
 // Chunk entries a search of graph g can need in one level (as the batch sizes them).
@@ -271,6 +290,11 @@ extern "C" int b40c_server_destroy(b40c_server_t *s) {
     }
     cudaFree(s->d_admit);
     cudaFree(s->d_clear);
+    cudaFree(s->d_nf);
+    cudaFree(s->d_mf);
+    cudaFree(s->d_dir);
+    cudaFree(s->d_bu);
+    cudaFree(s->d_bu_prefix);
     cudaFree(s->d_ctr);
     cudaFreeHost(s->h_ctr);
     cudaFreeHost(s->h_slots);
@@ -303,16 +327,27 @@ extern "C" int b40c_server_add_graph(b40c_server_t *s, int nodes, int edges, con
     CUDA_TRY(cudaMemcpy(g.d_row, h_row, sizeof(int) * (size_t(nodes) + 1), cudaMemcpyHostToDevice), "upload");
     CUDA_TRY(cudaMemset(g.d_col + edges, 0, 4 * sizeof(int)), "column padding");
     if (edges) CUDA_TRY(cudaMemcpy(g.d_col, h_col, sizeof(int) * size_t(edges), cudaMemcpyHostToDevice), "upload");
+    CUDA_TRY(ms_graph_symmetric(g.d_row, g.d_col, nodes, &g.symmetric), "graph symmetry check");
     s->graphs.push_back(g);
     std::vector<MsGraph> table(s->graphs.size());
     for (size_t i = 0; i < s->graphs.size(); i++)
-        table[i] = MsGraph{s->graphs[i].d_row, s->graphs[i].d_col, s->graphs[i].nodes, int(s->graphs[i].edges + 4)};
+        table[i] = MsGraph{s->graphs[i].d_row, s->graphs[i].d_col, s->graphs[i].nodes, int(s->graphs[i].edges + 4),
+                           int(s->graphs[i].edges), s->graphs[i].symmetric};
     cudaFree(s->d_graphs);
     s->d_graphs = nullptr;
     CUDA_TRY(cudaMalloc(&s->d_graphs, sizeof(MsGraph) * table.size()), "server graph table");
     CUDA_TRY(cudaMemcpy(s->d_graphs, table.data(), sizeof(MsGraph) * table.size(), cudaMemcpyHostToDevice),
              "graph table upload");
     *graph_id = int(s->graphs.size()) - 1;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_server_set_direction_optimizing(b40c_server_t *s, int alpha, int beta) {
+    clear_error();
+    if (!s || alpha < 0 || beta < 0 || (alpha > 0 && beta == 0))
+        return set_error(B40C_ERR_INVALID_VALUE, "direction switch: alpha >= 0, and beta >= 1 when alpha > 0");
+    s->do_alpha = unsigned(alpha);
+    s->do_beta = unsigned(beta);
     return B40C_SUCCESS;
 }
 

@@ -58,6 +58,10 @@ class BfsServer:
         check(lib().b40c_server_set_policy(self._h, cta_threads, warp_gather_threshold, cta_gather_threshold,
                                            cull_flags, epoch_levels))
 
+    def set_direction_optimizing(self, alpha: int = 14, beta: int = 24) -> None:
+        """Bottom-up levels per query on symmetric graphs (alpha = 0: off)."""
+        check(lib().b40c_server_set_direction_optimizing(self._h, int(alpha), int(beta)))
+
     def run_trace(self, graph_ids, sources, arrival_us, keep_labels: bool = False):
         """Replays the trace in real time; returns (latency_us, makespan_us[, labels])."""
         gids = np.ascontiguousarray(graph_ids, dtype=np.int32)

@@ -210,6 +210,11 @@ int b40c_batch_add_graph(b40c_batch_t *batch, int nodes, int edges, const int *h
 int b40c_batch_set_policy(b40c_batch_t *batch, int cta_threads, int warp_gather_threshold,
                           int cta_gather_threshold, int cull_flags);
 int b40c_batch_set_stream(b40c_batch_t *batch, void *stream);
+/* Bottom-up levels per search, as b40c_enactor_set_direction_optimizing
+ * (default alpha = 14, beta = 24; alpha = 0: top-down only): a search over a
+ * symmetric graph switches direction by its own frontier, independently of
+ * the other searches of the batch.  Depth labels only. */
+int b40c_batch_set_direction_optimizing(b40c_batch_t *batch, int alpha, int beta);
 /* Runs search i from sources[i] on graph graph_ids[i], i < num_searches, and
  * waits.  use_cuda_graph captures the launch sequence (pool clears, admission
  * kernel, persistent kernel) once and replays it for identical batches. */
@@ -236,6 +241,8 @@ int b40c_server_create(int mark_predecessors, int max_slots, long long hbm_budge
 int b40c_server_destroy(b40c_server_t *server);
 int b40c_server_add_graph(b40c_server_t *server, int nodes, int edges, const int *h_column_indices,
                           const int *h_row_offsets, int *graph_id);
+/* Bottom-up levels per query, as b40c_batch_set_direction_optimizing. */
+int b40c_server_set_direction_optimizing(b40c_server_t *server, int alpha, int beta);
 /* Policy as b40c_batch_set_policy, plus the level cap of one epoch (0 keeps). */
 int b40c_server_set_policy(b40c_server_t *server, int cta_threads, int warp_gather_threshold,
                            int cta_gather_threshold, int cull_flags, int epoch_levels);

@@ -83,3 +83,23 @@ def test_batch_edge_cases(cuda_device, oracle):
     srcs = [0, 0, 1, 0, 777]
     batch.run(gids, srcs)
     _check(oracle, batch, graphs, gids, srcs)
+
+
+@pytest.mark.parametrize("alpha,beta", [(0, 0), (1, 1), (14, 24), (1000, 1)],
+                         ids=["top-down", "eager-bottom-up", "default", "late-bottom-up"])
+def test_batch_direction_optimizing(cuda_device, oracle, mixed_graphs, alpha, beta):
+    """Each search switches direction by its own frontier; a directed graph
+    (which fails the symmetry check) stays top-down in the same batch."""
+    from conftest import golden_paths, load_golden
+    from back40computing_b200.batch import BfsBatch
+    directed, _, _, _ = load_golden([p for p in golden_paths() if p.stem == "ref_random_3000_d"][0])
+    graphs = list(mixed_graphs) + [directed]
+    batch = BfsBatch()
+    batch.set_direction_optimizing(alpha, beta)
+    ids = [batch.add_graph(g) for g in graphs]
+    gids = ids * 4
+    srcs = [int(graphs[g].sample_sources(1, 31 + k)[0]) for k, g in enumerate(gids)]
+    batch.run(gids, srcs, use_cuda_graph=True)
+    _check(oracle, batch, graphs, gids, srcs)
+    batch.run(gids, srcs, use_cuda_graph=True)  # replay
+    _check(oracle, batch, graphs, gids, srcs)

@@ -87,3 +87,14 @@ def test_trace_validation(cuda_device, graphs):
         srv.run_trace([0, 0], [1, 2], [5.0, 1.0])
     with pytest.raises(BfsError):
         srv.run_trace([3], [1], [0.0])
+
+
+@pytest.mark.parametrize("alpha,beta", [(0, 0), (1, 1)], ids=["top-down", "eager-bottom-up"])
+def test_direction_switch_does_not_change_results(cuda_device, oracle, graphs, alpha, beta):
+    srv = _server(graphs, max_slots=48, hbm_budget_bytes=128 << 20)
+    srv.set_direction_optimizing(alpha, beta)
+    gids, srcs, arr = _trace(graphs, 40, 100000.0, seed=13)
+    _, _, labels = srv.run_trace(gids, srcs, arr, keep_labels=True)
+    for i, (g, s) in enumerate(zip(gids, srcs)):
+        alone, _ = oracle.bfs(graphs[g], int(s))
+        assert oracle.first_mismatch(labels[i], alone) == -1
