@@ -167,6 +167,46 @@ __device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wai
     return grid_barrier(c, wait_ns, smem_flag, gridDim.x);
 }
 
+// The same barrier with a serial section: the CTA whose arrival completes the
+// count runs serial() with all its threads (it may use __syncthreads) before
+// it publishes the new generation, so serial() sees everything every CTA did
+// before the barrier and every CTA sees its results after it.
+template <class F>
+__device__ __forceinline__ bool grid_barrier_serial(Counters *c, unsigned long long wait_ns, unsigned *smem_flag,
+                                                    unsigned *smem_last, const F &serial) {
+    __syncthreads();
+    unsigned gen = 0;
+    if (threadIdx.x == 0) {
+        gen = ld_acquire_gpu(&c->bar_gen);
+        const unsigned arrived = atom_add_acqrel_gpu(&c->bar_count, 1u);
+        *smem_last = arrived == gridDim.x - 1 ? 1u : 0u;
+    }
+    __syncthreads();
+    if (*smem_last) {
+        serial();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            st_relaxed_gpu(&c->bar_count, 0u);
+            st_release_gpu(&c->bar_gen, gen + 1u);
+        }
+    } else if (threadIdx.x == 0) {
+        const unsigned long long t0 = globaltimer_ns();
+        unsigned ns = 32;
+        while (ld_acquire_gpu(&c->bar_gen) == gen) {
+            if (ld_relaxed_gpu(&c->error) != 0u) break;
+            if (globaltimer_ns() - t0 > wait_ns) {
+                atomicOr(&c->error, ERR_BARRIER_TIMEOUT);
+                break;
+            }
+            __nanosleep(ns);
+            if (ns < 256) ns <<= 1;
+        }
+    }
+    if (threadIdx.x == 0) *smem_flag = ld_relaxed_gpu(&c->error);
+    __syncthreads();
+    return *smem_flag == 0u;
+}
+
 // ---- scans -------------------------------------------------------------------------
 __device__ __forceinline__ int warp_sum(int x) { return __reduce_add_sync(0xffffffffu, x); }
 __device__ __forceinline__ long long warp_sum_ll(long long x) {

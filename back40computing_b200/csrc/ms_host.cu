@@ -354,7 +354,7 @@ extern "C" int b40c_batch_run_async(b40c_batch_t *b, int num_searches, const int
     const size_t S = size_t(num_searches);
     if ((rc = grow(&b->d_nf, &b->nf_cap, 4 * S, "batch direction counts"))) return rc;
     if ((rc = grow(&b->d_mf, &b->mf_cap, 4 * S, "batch direction degree sums"))) return rc;
-    if ((rc = grow(&b->d_dir, &b->dir_cap, S, "batch direction states"))) return rc;
+    if ((rc = grow(&b->d_dir, &b->dir_cap, 2 * S, "batch direction states"))) return rc;
     if ((rc = grow(&b->d_bu, &b->bu_cap, S, "batch bottom-up flags"))) return rc;
     if ((rc = grow(&b->d_bu_prefix, &b->bu_prefix_cap, S + 1, "batch bottom-up steps"))) return rc;
     for (int i = 0; i < 2; i++) {

@@ -44,6 +44,7 @@ struct MsSmem {
     unsigned long long vcache[VCACHE];  // (global mask word << 32) | word value
     unsigned warp_tot[THREADS / 32];    // bookkeeping scan of bottom-up steps
     unsigned flag;
+    unsigned last;                      // grid_barrier_serial: this CTA arrived last
 };
 
 template <int THREADS, bool MP>
@@ -483,23 +484,37 @@ __device__ __forceinline__ void ms_bu_step(const MsParams &p, int L, int s, unsi
 }
 
 // The bottom-up steps of every bottom-up slot, numbered in slot order by
-// bu_prefix: a warp takes step g (first one per warp, then dynamically) and
-// finds its slot by binary search.
+// bu_prefix, go out in runs of R consecutive steps (R grows with the total so
+// that a warp takes about 8 runs: many large slots would otherwise make the
+// run counter a hot spot); the first run per warp is static, the rest are
+// handed out by the counter, asked for when the previous run starts.  A run's
+// slot is found by binary search and followed across slot boundaries.
 template <int THREADS, bool MP>
 __device__ void ms_bu_level(const MsParams &p, int L, MsWarp<MP> &ws) {
     const unsigned total = __ldcg(p.bu_prefix + p.nslots);
     const unsigned W = grid_warps();
-    for (unsigned g = global_warp(); g < total;) {
+    const unsigned R = max(1u, total / (8u * W));
+    const unsigned runs = (total + R - 1) / R;
+    for (unsigned r = global_warp(); r < runs;) {
         unsigned nxt = 0;
-        if (total > W && lane_id() == 0) nxt = atomicAdd(&p.ctr->bu_steal[L & 3], 1u);
-        int lo = 0, hi = p.nslots;  // last s with bu_prefix[s] <= g
+        if (runs > W && lane_id() == 0) nxt = atomicAdd(&p.ctr->bu_steal[L & 3], 1u);
+        const unsigned g0 = r * R, g1 = min(total, g0 + R);
+        int lo = 0, hi = p.nslots;  // last s with bu_prefix[s] <= g0
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (__ldcg(p.bu_prefix + mid) <= g) lo = mid;
+            if (__ldcg(p.bu_prefix + mid) <= g0) lo = mid;
             else hi = mid;
         }
-        ms_bu_step<THREADS, MP>(p, L, lo, (g - __ldcg(p.bu_prefix + lo)) * 4u, ws);
-        g = total > W ? W + __shfl_sync(FULL, nxt, 0) : total;
+        unsigned s_begin = __ldcg(p.bu_prefix + lo), s_end = __ldcg(p.bu_prefix + lo + 1);
+        for (unsigned g = g0; g < g1; g++) {
+            while (g >= s_end) {  // next slot with steps
+                lo++;
+                s_begin = s_end;
+                s_end = __ldcg(p.bu_prefix + lo + 1);
+            }
+            ms_bu_step<THREADS, MP>(p, L, lo, (g - s_begin) * 4u, ws);
+        }
+        r = runs > W ? W + __shfl_sync(FULL, nxt, 0) : runs;
     }
 }
 
@@ -509,7 +524,7 @@ __device__ void ms_bu_level(const MsParams &p, int L, MsWarp<MP> &ws) {
 // Also clears the counts level L+1 will fill into ring entry (L+2)&3.
 template <int THREADS, bool MP>
 __device__ void ms_directions(const MsParams &p, int L, MsSmem<THREADS, MP> &sm) {
-    __syncthreads();  // the retirements ms_bookkeeping just wrote are read below
+    __syncthreads();
     const unsigned char *in = p.alive + size_t(L & 3) * size_t(p.nslots);
     const int per = (p.nslots + THREADS - 1) / THREADS;
     const int s0 = min(p.nslots, int(threadIdx.x) * per), s1 = min(p.nslots, s0 + per);
@@ -523,7 +538,7 @@ __device__ void ms_directions(const MsParams &p, int L, MsSmem<THREADS, MP> &sm)
         if (!MP && p.state[s].active && in[s]) {
             const MsSlot d = load_slot(p, s);
             const MsGraph g = p.graphs[d.graph];
-            MsDir dr = p.dir[s];
+            MsDir dr = p.dir[size_t((L + 1) & 1) * size_t(p.nslots) + size_t(s)];  // state after level L-1
             const unsigned nf = p.nf[at];
             const unsigned long long mf = p.mf[at];
             dr.explored += mf;
@@ -536,7 +551,7 @@ __device__ void ms_directions(const MsParams &p, int L, MsSmem<THREADS, MP> &sm)
             }
             dr.prev_nf = nf;
             dr.bottom_up = bottom_up ? 1 : 0;
-            p.dir[s] = dr;
+            p.dir[size_t(L & 1) * size_t(p.nslots) + size_t(s)] = dr;
             if (bottom_up) mine += ((unsigned(d.nodes) + 31u) / 32u + 3u) / 4u;
         }
         p.bu[s] = bottom_up ? 1 : 0;
@@ -556,7 +571,7 @@ __device__ void ms_directions(const MsParams &p, int L, MsSmem<THREADS, MP> &sm)
         }
     }
     if (threadIdx.x == THREADS - 1) p.bu_prefix[p.nslots] = run;
-    if (threadIdx.x == 0) p.ctr->bu_steal[(L + 1) & 3] = 0u;
+    if (threadIdx.x == 0) p.ctr->bu_steal[L & 3] = 0u;
     __syncthreads();
 }
 
@@ -610,8 +625,12 @@ __global__ void __launch_bounds__(THREADS, MS_MIN_BLOCKS(THREADS)) ms_fused_kern
         if (blockIdx.x == 0) ms_bookkeeping(p, L, empty);
         if (empty || L >= L_end || (p.stop_on_retire && retired_before)) break;
         // Direction-optimizing: every CTA needs the level's per-slot directions
-        // before it takes any work, so they are decided first, behind a barrier.
-        if (p.do_alpha) {
+        // before it takes any work.  The last CTA to reach the previous level's
+        // barrier decides them; a launch's first level decides them behind a
+        // barrier of its own (deciding a level again gives the same result:
+        // the state read is that of the level before, in the other half of
+        // dir).
+        if (p.do_alpha && L == L_first) {
             if (blockIdx.x == 0) ms_directions<THREADS, MP>(p, L, sm);
             if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         }
@@ -638,7 +657,12 @@ __global__ void __launch_bounds__(THREADS, MS_MIN_BLOCKS(THREADS)) ms_fused_kern
                 __syncwarp();
             }
         }
-        if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        if (p.do_alpha) {
+            if (!grid_barrier_serial(c, p.wait_ns, &sm.flag, &sm.last, [&] { ms_directions<THREADS, MP>(p, L + 1, sm); }))
+                break;
+        } else if (!grid_barrier(c, p.wait_ns, &sm.flag)) {
+            break;
+        }
         L++;
     }
     if (leader()) {
@@ -675,6 +699,7 @@ __global__ void ms_admit_kernel(MsParams p, const int2 *slot_src, int count, int
     if (p.do_alpha) {
         MsDir dr = {};
         p.dir[slot] = dr;
+        p.dir[size_t(p.nslots) + size_t(slot)] = dr;
         for (int q = 0; q < 4; q++) {
             const size_t at = size_t(q) * size_t(p.nslots) + size_t(slot);
             p.nf[at] = q == (L & 3) ? 1u : 0u;

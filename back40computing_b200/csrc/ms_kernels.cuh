@@ -68,7 +68,8 @@ struct MsParams {
     int stop_on_retire;  // return at the level after one where a search retired
     // Direction-optimizing searches (do_alpha = 0: top-down only): per slot,
     // the vertices discovered as input of level q (nf) and their degree sum
-    // (mf) at [(q & 3) * nslots + slot]; the direction state; the current
+    // (mf) at [(q & 3) * nslots + slot]; the direction state after level q at
+    // [(q & 1) * nslots + slot]; the current
     // level's bottom-up flag; and bu_prefix[s] = the bottom-up steps (4 mask
     // words each) of the slots before s, bu_prefix[nslots] their total.
     unsigned do_alpha;

@@ -178,7 +178,7 @@ int server_alloc(b40c_server *s, long long budget) {
     CUDA_TRY(cudaMalloc(&s->d_ctr, sizeof(Counters)), "server counters");
     CUDA_TRY(cudaMalloc(&s->d_nf, sizeof(unsigned) * 4 * S), "server direction counts");
     CUDA_TRY(cudaMalloc(&s->d_mf, sizeof(unsigned long long) * 4 * S), "server direction degree sums");
-    CUDA_TRY(cudaMalloc(&s->d_dir, sizeof(MsDir) * S), "server direction states");
+    CUDA_TRY(cudaMalloc(&s->d_dir, sizeof(MsDir) * 2 * S), "server direction states");
     CUDA_TRY(cudaMalloc(&s->d_bu, S), "server bottom-up flags");
     CUDA_TRY(cudaMalloc(&s->d_bu_prefix, sizeof(unsigned) * (S + 1)), "server bottom-up steps");
     CUDA_TRY(cudaHostAlloc(&s->h_ctr, sizeof(Counters), cudaHostAllocDefault), "server pinned counters");
