@@ -79,6 +79,25 @@ def dist_info():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def replica_sources(g, count, rank):
+    """Sources of one replica: each rank searches its own seeded sample."""
+    return g.sample_sources(count, 2 + 1000 * rank)
+
+
+def reduce_replicas(local_time, local_edges, world, device):
+    """(max time over ranks, edges summed over ranks): the replicas' aggregate
+    throughput is the total edges over the slowest rank's time."""
+    if world == 1:
+        return float(local_time), float(local_edges)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(local_time)], dtype=torch.float64, device=device)
+    e = torch.tensor([float(local_edges)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(e, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(e.item())
+
+
 def make_graph(scale, ef):
     from back40computing_b200 import graphs
     return graphs.rmat(scale, ef, 0.57, 0.19, 0.19, seed=1, undirected=True)
@@ -503,7 +522,7 @@ def main():
     dev = torch.device("cuda", local)
 
     g = make_graph(args.scale, args.edge_factor)
-    sources = g.sample_sources(args.sources, 2 + 1000 * rank)
+    sources = replica_sources(g, args.sources, rank)
     nsrc = len(sources)
     deg = g.degrees().astype(np.int64)
     strategies = [int(s) for s in args.strategies.split(",") if s.strip()]
@@ -565,14 +584,10 @@ def main():
         clk = clocks.stop() if clocks else None
         total_ms = t_start.elapsed_time(t_end)
         kern_ms = [a.elapsed_time(z) for a, z in zip(starts, ends)]
-        if world > 1:
-            t = torch.tensor([total_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
-        edges_step = float(E.sum())
+        total_ms, edges_all = reduce_replicas(total_ms, float(E.sum()) * args.steps, world, dev)
         bytes_alg = 4.0 * E + 20.0 * V
         results[strat] = {
-            "gteps": edges_step * args.steps * world / (total_ms / 1e3) / 1e9,
+            "gteps": edges_all / (total_ms / 1e3) / 1e9,
             "ms_per_step": total_ms / args.steps,
             "kernel_ms_mean": float(np.mean(kern_ms)),
             "kernel_ms_median": float(np.median(kern_ms)),
@@ -628,11 +643,8 @@ def main():
             e2e_step(False)
         torch.cuda.synchronize()
         secs = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([secs], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            secs = float(t.item())
-        e2e = {"value": float(E.sum()) * args.steps * world / secs / 1e9, "unit": UNIT,
+        secs, e2e_edges = reduce_replicas(secs, float(E.sum()) * args.steps, world, dev)
+        e2e = {"value": e2e_edges / secs / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": int(4 * (g.nodes + 1) + 4 * g.edges + 4 * nsrc),
                "d2h_bytes_per_step": int(4 * g.nodes * nsrc),
                "ms_per_step": secs / args.steps * 1e3}
