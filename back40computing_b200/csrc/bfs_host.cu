@@ -98,6 +98,10 @@ struct b40c_enactor {
     float last_ms = 0.f;
     int last_iteration = 0;
     long long last_total_queued = 0;
+    double last_duty = 0.0;
+    unsigned long long *d_busy = nullptr;  // INSTRUMENT: per-CTA busy ns of the last fused search
+    int busy_cap = 0;
+    int busy_grid = 0;  // CTAs of the last instrumented fused search (0: none)
     bool have_stats = false;
     bool timing_pending = false;
     // cached per-level graph
@@ -369,6 +373,18 @@ int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size,
         int limit = 0;
         CUDA_TRY(fused_grid_limit(kc, &limit), "occupancy query");
         int grid = max_grid_size > 0 ? std::min(max_grid_size, limit) : limit;
+        e->busy_grid = 0;
+        if (e->instrument) {
+            if (e->busy_cap < grid) {
+                cudaFree(e->d_busy);
+                e->d_busy = nullptr;
+                e->busy_cap = 0;
+                CUDA_TRY(cudaMalloc(&e->d_busy, sizeof(unsigned long long) * size_t(grid)), "cudaMalloc duty stats");
+                e->busy_cap = grid;
+            }
+            bp.cta_busy = e->d_busy;
+            e->busy_grid = grid;
+        }
         CUDA_TRY(launch_fused(bp, kc, grid, s), "cooperative launch of the fused BFS kernel");
     } else if (variant == B40C_VARIANT_ITERATIVE) {
         int limit = 0;
@@ -412,6 +428,20 @@ int finish_search(b40c_enactor *e) {
     }
     e->last_iteration = e->h_ctr->iteration;
     e->last_total_queued = (long long)e->h_ctr->total_queued;
+    e->last_duty = 0.0;
+    if (e->busy_grid > 0) {
+        // avg_duty as the reference accumulates it (kernel_runtime_stats.cuh:
+        // Accumulate): the CTAs' busy times over the longest one times the grid.
+        std::vector<unsigned long long> busy(size_t(e->busy_grid));
+        CUDA_TRY(cudaMemcpy(busy.data(), e->d_busy, sizeof(unsigned long long) * busy.size(), cudaMemcpyDeviceToHost),
+                 "duty stats copy");
+        unsigned long long total = 0, longest = 0;
+        for (unsigned long long b : busy) {
+            total += b;
+            longest = std::max(longest, b);
+        }
+        e->last_duty = longest ? double(total) / (double(longest) * double(busy.size())) : 0.0;
+    }
     e->have_stats = true;
     unsigned err = e->h_ctr->sticky | e->h_ctr->error;
     if (err) {
@@ -673,6 +703,7 @@ extern "C" int b40c_enactor_destroy(b40c_enactor_t *e) {
     cudaFree(e->d_wchunks[0]);
     cudaFree(e->d_wchunks[1]);
     cudaFree(e->d_levels);
+    cudaFree(e->d_busy);
     if (e->h_ctr) cudaFreeHost(e->h_ctr);
     cudaEventDestroy(e->ev0);
     cudaEventDestroy(e->ev1);
@@ -742,7 +773,7 @@ extern "C" int b40c_enactor_get_statistics(b40c_enactor_t *e, long long *total_q
     // GetStatistics: search_depth = iteration - 1 (enactor_contract_expand.cuh:245).
     if (total_queued) *total_queued = e->instrument ? e->last_total_queued : 0;
     if (search_depth) *search_depth = e->last_iteration - 1;
-    if (avg_duty) *avg_duty = 0.0;
+    if (avg_duty) *avg_duty = e->instrument ? e->last_duty : 0.0;
     return B40C_SUCCESS;
 }
 

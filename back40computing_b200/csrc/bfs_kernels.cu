@@ -864,6 +864,24 @@ __device__ __forceinline__ void init_hist(Smem<THREADS, MP> &sm, unsigned flags)
 
 __device__ __forceinline__ bool leader() { return blockIdx.x == 0 && threadIdx.x == 0; }
 
+// INSTRUMENT duty (the reference's KernelRuntimeStats MarkStart / MarkStop,
+// b40c/util/kernel_runtime_stats.cuh): thread 0 of each CTA sums the time from
+// a level's start to the moment all its warps finished the level's work.
+struct BusyClock {
+    unsigned long long busy = 0, t0 = 0;
+    __device__ __forceinline__ void start(const BfsParams &p) {
+        if (p.cta_busy && threadIdx.x == 0) t0 = globaltimer_ns();
+    }
+    __device__ __forceinline__ void stop(const BfsParams &p) {
+        if (!p.cta_busy) return;
+        __syncthreads();
+        if (threadIdx.x == 0) busy += globaltimer_ns() - t0;
+    }
+    __device__ __forceinline__ void flush(const BfsParams &p) const {
+        if (p.cta_busy && threadIdx.x == 0) p.cta_busy[blockIdx.x] = busy;
+    }
+};
+
 // The kernels keep Smem in dynamic shared memory (it can exceed the 48 KB
 // static limit at 512 threads); launches pass sizeof(Smem<THREADS, MP>).
 template <int THREADS, bool MP>
@@ -967,8 +985,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
     const uint64_t pol = policy_evict_first();
     Counters *c = p.ctr;
     DirectionChoice dir;
+    BusyClock clk;
     int it = 0;
     for (;;) {
+        clk.start(p);
         const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]), nw = ld_cg(&c->wch[it & 3]);
         if (stop_level_loop(p, it, L + nch + nw)) break;
         bool bottom_up = false;
@@ -987,9 +1007,11 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
         } else {
             ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
         }
+        clk.stop(p);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         it++;
     }
+    clk.flush(p);
     finish_search(p, it, it);
 }
 
@@ -999,8 +1021,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
     init_hist(sm, p.cull_flags);
     const uint64_t pol = policy_evict_first();
     Counters *c = p.ctr;
+    BusyClock clk;
     int it = 0;
     for (;;) {
+        clk.start(p);
         const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]), nw = ld_cg(&c->wch[it & 3]);
         if (stop_level_loop(p, it, L + nch + nw)) break;
         if (leader()) {
@@ -1009,9 +1033,11 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
             log_phase(p, it, L, nch, nw);
         }
         ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, pol);
+        clk.stop(p);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         it++;
     }
+    clk.flush(p);
     finish_search(p, it, it);
 }
 
@@ -1025,8 +1051,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
     init_hist(sm, p.cull_flags);
     const uint64_t pol = policy_evict_first();
     Counters *c = p.ctr;
+    BusyClock clk;
     int it = 0, qi = 0;
     for (;;) {
+        clk.start(p);
         unsigned L = ld_cg(&c->qlen[qi & 3]);
         const unsigned nch = ld_cg(&c->big[qi & 3]), nw = ld_cg(&c->wch[qi & 3]);
         if (stop_level_loop(p, it, L + nch + nw)) break;
@@ -1036,7 +1064,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
             log_phase(p, qi, L, nch, nw);
         }
         tp_contract<THREADS, MP>(p, it, qi, L, nch, nw, sm, pol);
+        clk.stop(p);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        clk.start(p);
         qi++;
         L = ld_cg(&c->qlen[qi & 3]);
         if (L == 0u) break;  // no vertex discovered: the reference stops without ++
@@ -1045,10 +1075,12 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
             log_phase(p, qi, L, 0u, 0u);
         }
         tp_expand<THREADS, MP>(p, qi, L, sm, pol);
+        clk.stop(p);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         qi++;
         it++;
     }
+    clk.flush(p);
     finish_search(p, it, qi + 1);
 }
 
@@ -1068,8 +1100,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
     const uint64_t pol = policy_evict_first();
     Counters *c = p.ctr;
     const unsigned long long saturation = 4ull * THREADS * gridDim.x;
+    BusyClock clk;
     int it = 0, q = 0;
     for (;;) {
+        clk.start(p);
         unsigned L = ld_cg(&c->qlen[q & 3]);
         const unsigned nch = ld_cg(&c->big[q & 3]), nw = ld_cg(&c->wch[q & 3]);
         if (stop_level_loop(p, it, L + nch + nw)) break;
@@ -1082,13 +1116,16 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
             L + (unsigned long long)nch * chunk_edges<THREADS>() + (unsigned long long)nw * WARP_CHUNK;
         if (edges <= saturation) {
             ce_level<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
+            clk.stop(p);
             if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
             q++;
             it++;
             continue;
         }
         tp_contract<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
+        clk.stop(p);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        clk.start(p);
         q++;
         L = ld_cg(&c->qlen[q & 3]);
         if (L == 0u) break;  // no vertex discovered: stop without ++, as two-phase does
@@ -1097,10 +1134,12 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
             log_phase(p, q, L, 0u, 0u);
         }
         tp_expand<THREADS, MP>(p, q, L, sm, pol);
+        clk.stop(p);
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         q++;
         it++;
     }
+    clk.flush(p);
     finish_search(p, it, q);
 }
 

@@ -63,6 +63,9 @@ struct BfsParams {
     unsigned do_alpha;
     unsigned do_beta;
     long long edges;  // CSR entries (for the unvisited-edge count)
+    // INSTRUMENT: per CTA of a fused kernel, the %globaltimer ns it spent in
+    // level work (barrier waits excluded), written at the kernel's end; NULL: off.
+    unsigned long long *cta_busy;
 };
 
 // Edges per CTA chunk: four passes of one 16-byte load per thread of a CTA.

@@ -114,7 +114,11 @@ int b40c_enact_search_async(b40c_enactor_t *enactor, b40c_problem_t *problem,
 /* Waits for the enactor's stream and reports flags raised by async searches. */
 int b40c_enactor_sync(b40c_enactor_t *enactor);
 /* GetStatistics(total_queued, search_depth, avg_duty)
- * (enactor_contract_expand.cuh:237-250).  search_depth = iteration - 1. */
+ * (enactor_contract_expand.cuh:237-250).  search_depth = iteration - 1.
+ * With INSTRUMENT: total_queued sums the levels' input frontiers, and
+ * avg_duty (fused searches) is the CTAs' time in level work -- barrier waits
+ * excluded -- over the longest CTA's time times the grid, as the reference's
+ * KernelRuntimeStats accumulate it (1.0: perfectly balanced levels); else 0. */
 int b40c_enactor_get_statistics(b40c_enactor_t *enactor, long long *total_queued,
                                 int *search_depth, double *avg_duty);
 /* Device time of the last synchronous search (CUDA events around its kernels). */

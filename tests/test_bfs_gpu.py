@@ -386,3 +386,26 @@ def test_direction_switch_arguments(cuda_device):
     with pytest.raises(b.BfsError):
         b.EnactorContractExpand().set_direction_optimizing(14, 24)
     b.EnactorContractExpand().set_direction_optimizing(0, 0)
+
+
+@pytest.mark.parametrize("strategy", STRATEGIES)
+def test_instrument_statistics(cuda_device, oracle, rmat16, strategy):
+    """INSTRUMENT: total_queued counts the levels' inputs and avg_duty is the
+    CTAs' busy share of the longest CTA (0 < duty <= 1); labels unchanged;
+    without INSTRUMENT both read 0 as in the reference."""
+    b = bfs_mod()
+    g = rmat16
+    s = int(g.sample_sources(1, 41)[0])
+    ref, _ = oracle.bfs(g, s)
+    prob = b.CsrProblem(False).from_graph(g)
+    for instrument in (True, False):
+        en = b.make_enactor(strategy, INSTRUMENT=instrument)
+        b.check(prob.Reset(en.GetFrontierType(), 1.3))
+        b.check(en.EnactSearch(prob, s))
+        assert oracle.first_mismatch(prob.labels(), ref) == -1
+        queued, depth, duty = en.GetStatistics()
+        if instrument:
+            assert queued > 0
+            assert 0.0 < duty <= 1.0
+        else:
+            assert queued == 0 and duty == 0.0
