@@ -1,0 +1,80 @@
+"""Autotuner: candidate grid, successive halving, cache, and (on a GPU) that
+the tuned policies give the oracle's labels."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+
+def test_candidates_cover_the_knobs():
+    from back40computing_b200 import tune
+    ec = tune.candidates(0)
+    assert {c["cta_threads"] for c in ec} == set(tune.CTA_THREADS)
+    assert {c["warp_gather_threshold"] for c in ec} == set(tune.WARP_THRESHOLDS)
+    assert {(c["alpha"], c["beta"]) for c in ec} == set(tune.DIRECTIONS)
+    assert all("alpha" not in c for c in tune.candidates(1))  # no direction switch off expand-contract
+    assert all(c["cta_gather_threshold"] >= c["warp_gather_threshold"] for c in ec)
+
+
+def test_successive_halving_finds_the_minimum():
+    from back40computing_b200 import tune
+    cands = [{"k": i} for i in range(40)]
+    calls = []
+
+    def measure(c):
+        calls.append(c["k"])
+        return abs(c["k"] - 17) + 1.0
+
+    best, t = tune.pick_best(cands, measure, rounds=3, keep=0.25)
+    assert best["k"] == 17 and t == 1.0
+    assert len(calls) < 40 * 3  # later rounds measure only the leaders
+
+
+def test_cache_round_trip(tmp_path):
+    from back40computing_b200 import tune
+    path = tmp_path / "tune.json"
+    c = tune.TuneCache(path)
+    c.put("enactor/0/x", {"cta_threads": 256}, 1.5)
+    assert tune.TuneCache(path).get("enactor/0/x") == {"cta_threads": 256}
+    assert tune.TuneCache(path).get("enactor/0/y") is None
+
+
+def test_graph_signature_and_symmetry():
+    import back40computing_b200 as b
+    from back40computing_b200 import tune
+    g = b.rmat(10, 8, seed=2)
+    assert tune.is_symmetric(g)
+    d = b.from_coo(4, [0, 1, 2], [1, 2, 3])
+    assert not tune.is_symmetric(d)
+    assert tune.graph_signature(g).endswith("sym") and tune.graph_signature(d).endswith("dir")
+
+
+@pytest.mark.gpu
+def test_tuned_policies_keep_labels(cuda_device, oracle):
+    import back40computing_b200 as b
+    from back40computing_b200 import tune
+    from back40computing_b200.batch import BfsBatch
+    g = b.rmat(13, 16, seed=8)
+    cache = tune.TuneCache(None)
+    small = tune.candidates(0)[::9]
+    pol = tune.tune_enactor(g, 0, num_sources=2, cache=cache, cands=small)
+    assert pol in small and cache.get(f"enactor/0/{tune.graph_signature(g)}") == pol
+    en = b.make_enactor(0)
+    tune.apply_enactor_policy(en, pol)
+    prob = b.CsrProblem(False).from_graph(g)
+    s = int(g.sample_sources(1, 3)[0])
+    b.check(prob.Reset(en.GetFrontierType(), 1.3))
+    b.check(en.EnactSearch(prob, s))
+    assert oracle.first_mismatch(prob.labels(), oracle.bfs(g, s)[0]) == -1
+
+    graphs = [g, b.grid2d(48)]
+    gids = [0, 1, 0, 1]
+    srcs = [int(graphs[k].sample_sources(1, 5 + i)[0]) for i, k in enumerate(gids)]
+    bpol = tune.tune_batch(graphs, gids, srcs, cache=cache, cands=small)
+    batch = BfsBatch()
+    tune.apply_batch_policy(batch, bpol)
+    for gg in graphs:
+        batch.add_graph(gg)
+    batch.run(gids, srcs)
+    for i, (k, s) in enumerate(zip(gids, srcs)):
+        assert oracle.first_mismatch(batch.labels(i), oracle.bfs(graphs[k], s)[0]) == -1
