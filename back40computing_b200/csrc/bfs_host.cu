@@ -64,6 +64,7 @@ struct b40c_problem {
     int *d_labels = nullptr;
     unsigned *d_mask = nullptr;
     size_t mask_bytes = 0;
+    size_t col_cap = 0, row_cap = 0, labels_cap = 0, mask_cap = 0;  // device allocations kept across uploads
     int *d_queue[2] = {nullptr, nullptr};
     int *d_pred[2] = {nullptr, nullptr};
     long long queue_elems[2] = {0, 0};
@@ -119,34 +120,14 @@ constexpr int LEVEL_LOG_CAP = 4096;
 cudaStream_t problem_stream(b40c_problem *p) { return p->stream ? p->stream : p->own_stream; }
 cudaStream_t enactor_stream(b40c_enactor *e) { return e->stream ? e->stream : e->own_stream; }
 
-int check_csr(int64_t nodes, int64_t edges, const int *row, const int *col) {
+// The ends of the row offsets, checked on the host; the rest of the CSR
+// (offsets that decrease, column ids out of range) is checked on the device
+// after the upload (device_check_csr).
+int check_csr_ends(int64_t nodes, int64_t edges, const int *row) {
     if (row[0] != 0) return set_error(B40C_ERR_INVALID_VALUE, "CSR row_offsets[0] = %d, expected 0", row[0]);
     if (row[nodes] != edges)
         return set_error(B40C_ERR_INVALID_VALUE, "CSR row_offsets[nodes] = %d, expected edges = %lld",
                          row[nodes], (long long)edges);
-    for (int64_t v = 0; v < nodes; v++)
-        if (row[v + 1] < row[v])
-            return set_error(B40C_ERR_INVALID_VALUE, "CSR row_offsets decrease at row %lld", (long long)v);
-    // Column ids checked on several threads (the arrays can be ~10^8 entries).
-    unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    std::vector<int64_t> bad(nt, -1);
-    std::vector<std::thread> pool;
-    int64_t chunk = (edges + nt - 1) / nt;
-    for (unsigned t = 0; t < nt; t++) {
-        pool.emplace_back([&, t] {
-            int64_t lo = std::min<int64_t>(edges, t * chunk), hi = std::min<int64_t>(edges, lo + chunk);
-            for (int64_t k = lo; k < hi; k++)
-                if ((unsigned)col[k] >= (unsigned)nodes) {
-                    bad[t] = k;
-                    break;
-                }
-        });
-    }
-    for (auto &th : pool) th.join();
-    for (unsigned t = 0; t < nt; t++)
-        if (bad[t] >= 0)
-            return set_error(B40C_ERR_INVALID_VALUE, "CSR column index %d at edge %lld outside [0, %lld)",
-                             col[bad[t]], (long long)bad[t], (long long)nodes);
     return B40C_SUCCESS;
 }
 
@@ -160,10 +141,12 @@ void free_problem_device(b40c_problem *p) {
     unmap_host(p);
     p->d_row_offsets = nullptr;
     p->d_col = nullptr;
+    p->col_cap = p->row_cap = 0;
     cudaFree(p->d_labels);
     cudaFree(p->d_mask);
     p->d_labels = nullptr;
     p->d_mask = nullptr;
+    p->labels_cap = p->mask_cap = 0;
     for (int i = 0; i < 2; i++) {
         cudaFree(p->d_queue[i]);
         cudaFree(p->d_pred[i]);
@@ -185,10 +168,30 @@ int ensure_symmetry_known(b40c_problem *p) {
     if (!p->d_sym) CUDA_TRY(cudaMalloc(&p->d_sym, 4 * sizeof(unsigned long long)), "cudaMalloc symmetry sums");
     unsigned long long h[4] = {0, 0, 0, 0};
     CUDA_TRY(cudaMemsetAsync(p->d_sym, 0, sizeof(h), s), "symmetry sums clear");
-    CUDA_TRY(launch_symmetry_hash(p->d_row_offsets, p->d_col, int(p->nodes), p->d_sym, s), "symmetry check launch");
+    CUDA_TRY(launch_symmetry_hash(p->d_row_offsets, p->d_col, int(p->nodes), p->edges, p->d_sym, s),
+             "symmetry check launch");
     CUDA_TRY(cudaMemcpyAsync(h, p->d_sym, sizeof(h), cudaMemcpyDeviceToHost, s), "symmetry sums copy");
     CUDA_TRY(cudaStreamSynchronize(s), "symmetry check");
     p->symmetric = (h[0] == h[1] && h[2] == h[3]) ? 1 : 0;
+    return B40C_SUCCESS;
+}
+
+// Checks the uploaded CSR on the device (rows whose offsets decrease, column
+// ids outside [0, nodes)) and reports the first fault as the host check
+// would, reading the offending values from the caller's arrays.
+int device_check_csr(b40c_problem *p, const int *h_row, const int *h_col) {
+    cudaStream_t s = problem_stream(p);
+    if (!p->d_sym) CUDA_TRY(cudaMalloc(&p->d_sym, 4 * sizeof(unsigned long long)), "cudaMalloc check buffer");
+    unsigned long long h[2];
+    CUDA_TRY(cudaMemsetAsync(p->d_sym, 0xff, sizeof(h), s), "CSR check clear");
+    CUDA_TRY(launch_csr_check(p->d_row_offsets, p->d_col, int(p->nodes), p->edges, p->d_sym, s), "CSR check launch");
+    CUDA_TRY(cudaMemcpyAsync(h, p->d_sym, sizeof(h), cudaMemcpyDeviceToHost, s), "CSR check copy");
+    CUDA_TRY(cudaStreamSynchronize(s), "CSR check");
+    if (h[0] != ~0ull)
+        return set_error(B40C_ERR_INVALID_VALUE, "CSR row_offsets decrease at row %lld", (long long)h[0]);
+    if (h[1] != ~0ull)
+        return set_error(B40C_ERR_INVALID_VALUE, "CSR column index %d at edge %lld outside [0, %lld)",
+                         h_col[h[1]], (long long)h[1], (long long)p->nodes);
     return B40C_SUCCESS;
 }
 
@@ -498,35 +501,61 @@ extern "C" int b40c_problem_from_host(b40c_problem_t *p, int stream_from_host, i
         return set_error(B40C_ERR_NOT_SUPPORTED, "FromHostProblem: multi-GPU slices are not provided");
     if (edges > INT32_MAX - 8192)
         return set_error(B40C_ERR_INVALID_VALUE, "FromHostProblem: %d edges too many for int32 SizeT", edges);
-    int rc = check_csr(nodes, edges, h_row, h_col);
+    int rc = check_csr_ends(nodes, edges, h_row);
     if (rc) return rc;
     CUDA_TRY(cudaSetDevice(p->device), "cudaSetDevice");
     cudaStreamSynchronize(problem_stream(p));
-    free_problem_device(p);
+    const bool was_mapped = p->mapped;
+    p->mapped = stream_from_host != 0 && edges > 0;
+    if (p->mapped || was_mapped) {
+        free_problem_device(p);  // mapped arrays are the caller's; device copies are not reused across modes
+    } else {
+        // A new upload into the same problem reuses its device buffers when they are large enough.
+        if (p->labels_cap < size_t(nodes)) {
+            cudaFree(p->d_labels);
+            p->d_labels = nullptr;
+            p->labels_cap = 0;
+        }
+        if (p->mask_cap < size_t((nodes + 31) / 32) * 4) {
+            cudaFree(p->d_mask);
+            p->d_mask = nullptr;
+            p->mask_cap = 0;
+        }
+    }
     p->nodes = nodes;
     p->edges = edges;
     p->reset_once = false;
-    p->mapped = stream_from_host != 0;
+    p->symmetric = -1;
     if (p->mapped) {
         if ((rc = map_host(p, h_row, sizeof(int) * (size_t(nodes) + 1), (void **)&p->d_row_offsets))) return rc;
-        if (edges > 0 && (rc = map_host(p, h_col, sizeof(int) * size_t(edges), (void **)&p->d_col))) return rc;
-        if (edges == 0) {
-            CUDA_TRY(cudaMalloc(&p->d_col, 16), "cudaMalloc column_indices");
-            p->mapped = false;  // nothing to stream; treat as device copy
-            CUDA_TRY(cudaMalloc(&p->d_row_offsets, sizeof(int) * (size_t(nodes) + 1)), "cudaMalloc row_offsets");
-            CUDA_TRY(cudaMemcpy(p->d_row_offsets, h_row, sizeof(int) * (size_t(nodes) + 1), cudaMemcpyHostToDevice),
-                     "cudaMemcpy row_offsets");
-        }
+        if ((rc = map_host(p, h_col, sizeof(int) * size_t(edges), (void **)&p->d_col))) return rc;
     } else {
         // Column array padded with 4 entries for 16-byte tail loads.
-        CUDA_TRY(cudaMalloc(&p->d_col, sizeof(int) * (size_t(edges) + 4)), "CsrProblem cudaMalloc d_column_indices");
+        if (p->col_cap < size_t(edges) + 4) {
+            cudaFree(p->d_col);
+            p->d_col = nullptr;
+            p->col_cap = 0;
+            CUDA_TRY(cudaMalloc(&p->d_col, sizeof(int) * (size_t(edges) + 4)), "CsrProblem cudaMalloc d_column_indices");
+            p->col_cap = size_t(edges) + 4;
+        }
+        if (p->row_cap < size_t(nodes) + 1) {
+            cudaFree(p->d_row_offsets);
+            p->d_row_offsets = nullptr;
+            p->row_cap = 0;
+            CUDA_TRY(cudaMalloc(&p->d_row_offsets, sizeof(int) * (size_t(nodes) + 1)), "CsrProblem cudaMalloc d_row_offsets");
+            p->row_cap = size_t(nodes) + 1;
+        }
         CUDA_TRY(cudaMemset(p->d_col + edges, 0, 4 * sizeof(int)), "cudaMemset column padding");
         if (edges)
             CUDA_TRY(cudaMemcpy(p->d_col, h_col, sizeof(int) * size_t(edges), cudaMemcpyHostToDevice),
                      "CsrProblem cudaMemcpy d_column_indices");
-        CUDA_TRY(cudaMalloc(&p->d_row_offsets, sizeof(int) * (size_t(nodes) + 1)), "CsrProblem cudaMalloc d_row_offsets");
         CUDA_TRY(cudaMemcpy(p->d_row_offsets, h_row, sizeof(int) * (size_t(nodes) + 1), cudaMemcpyHostToDevice),
                  "CsrProblem cudaMemcpy d_row_offsets");
+    }
+    if ((rc = device_check_csr(p, h_row, h_col))) {
+        free_problem_device(p);
+        p->nodes = p->edges = 0;
+        return rc;
     }
     return B40C_SUCCESS;
 }
@@ -538,12 +567,15 @@ static int problem_reset(b40c_problem *p, int frontier_type, double queue_sizing
     if (!(queue_sizing > 0.0)) queue_sizing = 1.3;  // test_bfs.cu:802 default
     CUDA_TRY(cudaSetDevice(p->device), "cudaSetDevice");
     cudaStream_t s = problem_stream(p);
-    if (!p->d_labels)
+    if (!p->d_labels) {
         CUDA_TRY(cudaMalloc(&p->d_labels, sizeof(int) * size_t(p->nodes)), "CsrProblem cudaMalloc d_labels");
+        p->labels_cap = size_t(p->nodes);
+    }
+    // ceil(nodes / 8) bytes as the reference (csr_problem.cuh:581-583), rounded to whole words.
+    p->mask_bytes = size_t((p->nodes + 31) / 32) * 4;
     if (!p->d_mask) {
-        // ceil(nodes / 8) bytes as the reference (csr_problem.cuh:581-583), rounded to whole words.
-        p->mask_bytes = size_t((p->nodes + 31) / 32) * 4;
         CUDA_TRY(cudaMalloc(&p->d_mask, p->mask_bytes), "CsrProblem cudaMalloc d_visited_mask");
+        p->mask_cap = p->mask_bytes;
     }
     long long n = p->nodes, m = p->edges;
     long long want[2] = {0, 0}, wpred[2] = {0, 0};

@@ -1254,34 +1254,63 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
 }
 
 // sums[0] / sums[1]: hash sums of (u, v) / (v, u) over every entry v of row u;
-// sums[2] / sums[3]: the same with a second, salted hash.  A warp per row.
-__global__ void symmetry_hash_kernel(const int *row_offsets, const int *col, int nodes, unsigned long long *sums) {
+// sums[2] / sums[3]: the same with a second, salted hash.  The entries are cut
+// into runs of SYM_RUN consecutive ones, one run per lane (a warp takes 32
+// runs): the lane finds the row of its first entry by binary search over the
+// row offsets and walks forward from there, so a hub's list is spread over as
+// many lanes as it has runs, whatever the vertex order.
+constexpr int SYM_RUN = 64;
+
+__device__ __forceinline__ void hash_entry(unsigned u, unsigned v, unsigned long long (&h)[4]) {
     constexpr unsigned long long SALT = 0x5851f42d4c957f2dull;
-    unsigned long long a0 = 0, b0 = 0, a1 = 0, b1 = 0;
-    const int lane = lane_id();
-    const int W = grid_warps();
-    for (int v = global_warp(); v < nodes; v += W) {
-        const int s = __ldg(row_offsets + v), e = __ldg(row_offsets + v + 1);
-        for (int k = s + lane; k < e; k += 32) {
-            const unsigned u = (unsigned)__ldg(col + k);
-            const unsigned long long fwd = ((unsigned long long)(unsigned)v << 32) | u;
-            const unsigned long long rev = ((unsigned long long)u << 32) | (unsigned)v;
-            a0 += mix64(fwd);
-            b0 += mix64(rev);
-            a1 += mix64(fwd ^ SALT);
-            b1 += mix64(rev ^ SALT);
+    const unsigned long long fwd = ((unsigned long long)u << 32) | v;
+    const unsigned long long rev = ((unsigned long long)v << 32) | u;
+    h[0] += mix64(fwd);
+    h[1] += mix64(rev);
+    h[2] += mix64(fwd ^ SALT);
+    h[3] += mix64(rev ^ SALT);
+}
+
+__global__ void symmetry_hash_kernel(const int *row_offsets, const int *col, int nodes, long long edges,
+                                     unsigned long long *sums) {
+    unsigned long long h[4] = {0, 0, 0, 0};
+    const long long W = grid_warps();
+    for (long long c = global_warp(); c * 32 * SYM_RUN < edges; c += W) {
+        const long long k0 = (c * 32 + lane_id()) * SYM_RUN;
+        if (k0 < edges) {
+            const long long k1 = min(edges, k0 + SYM_RUN);
+            int lo = 0, hi = nodes;  // last row lo with row_offsets[lo] <= k0
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (__ldg(row_offsets + mid) <= k0) lo = mid;
+                else hi = mid;
+            }
+            int r = lo;
+            long long next = __ldg(row_offsets + r + 1);
+            for (long long k = k0; k < k1; k++) {
+                while (k >= next) next = __ldg(row_offsets + (++r) + 1);
+                hash_entry(unsigned(r), (unsigned)__ldg(col + k), h);
+            }
         }
     }
-    a0 = (unsigned long long)warp_sum_ll((long long)a0);
-    b0 = (unsigned long long)warp_sum_ll((long long)b0);
-    a1 = (unsigned long long)warp_sum_ll((long long)a1);
-    b1 = (unsigned long long)warp_sum_ll((long long)b1);
-    if (lane == 0) {
-        atomicAdd(sums + 0, a0);
-        atomicAdd(sums + 1, b0);
-        atomicAdd(sums + 2, a1);
-        atomicAdd(sums + 3, b1);
-    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) h[j] = (unsigned long long)warp_sum_ll((long long)h[j]);
+    if (lane_id() == 0)
+#pragma unroll
+        for (int j = 0; j < 4; j++) atomicAdd(sums + j, h[j]);
+}
+
+// CSR checks on the device: out[0] = the first row v whose offsets decrease
+// (row[v+1] < row[v]), out[1] = the first entry outside [0, nodes); both stay
+// ~0 when there is none (out must start at ~0).
+__global__ void csr_check_kernel(const int *row_offsets, const int *col, int nodes, long long edges,
+                                 unsigned long long *out) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (long long v = t; v < nodes; v += stride)
+        if (__ldg(row_offsets + v + 1) < __ldg(row_offsets + v)) atomicMin(out + 0, (unsigned long long)v);
+    for (long long k = t; k < edges; k += stride)
+        if ((unsigned)__ldg(col + k) >= (unsigned)nodes) atomicMin(out + 1, (unsigned long long)k);
 }
 
 // Failure-detection probe: the barrier waits for gridDim.x + 1 arrivals, so no
@@ -1404,13 +1433,23 @@ cudaError_t level_grid_limit(const KernelConfig &kc, int *grid) {
     return grid_for((const void *)f.level_a, kc.threads, smem_bytes(kc), grid);
 }
 
-cudaError_t launch_symmetry_hash(const int *row_offsets, const int *col, int nodes, unsigned long long *sums,
-                                 cudaStream_t stream) {
+cudaError_t launch_symmetry_hash(const int *row_offsets, const int *col, int nodes, long long edges,
+                                 unsigned long long *sums, cudaStream_t stream) {
     int dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (!e) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e) return e;
-    symmetry_hash_kernel<<<sms * 8, 256, 0, stream>>>(row_offsets, col, nodes, sums);
+    symmetry_hash_kernel<<<sms * 8, 256, 0, stream>>>(row_offsets, col, nodes, edges, sums);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_csr_check(const int *row_offsets, const int *col, int nodes, long long edges,
+                             unsigned long long *out, cudaStream_t stream) {
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (!e) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e) return e;
+    csr_check_kernel<<<sms * 8, 256, 0, stream>>>(row_offsets, col, nodes, edges, out);
     return cudaGetLastError();
 }
 

@@ -89,8 +89,13 @@ cudaError_t level_grid_limit(const KernelConfig &kc, int *grid);
 // Two 64-bit hash sums over the CSR's entries, of (u, v) and of (v, u); equal
 // sums mean the graph is symmetric (up to a hash collision).  sums[0..3] must
 // start at zero.
-cudaError_t launch_symmetry_hash(const int *row_offsets, const int *col, int nodes, unsigned long long *sums,
-                                 cudaStream_t stream);
+cudaError_t launch_symmetry_hash(const int *row_offsets, const int *col, int nodes, long long edges,
+                                 unsigned long long *sums, cudaStream_t stream);
+// CSR validity on the device: out[0] = first row whose offsets decrease,
+// out[1] = first column entry outside [0, nodes); ~0 when none.  out[0..1]
+// must start at ~0.
+cudaError_t launch_csr_check(const int *row_offsets, const int *col, int nodes, long long edges,
+                             unsigned long long *out, cudaStream_t stream);
 // Cooperative launch of the persistent kernel that runs every BFS level.
 cudaError_t launch_fused(const BfsParams &p, const KernelConfig &kc, int grid, cudaStream_t stream);
 // Builds a graph whose conditional-while node runs one BFS level per pass:

@@ -254,7 +254,7 @@ extern "C" int b40c_batch_add_graph(b40c_batch_t *b, int nodes, int edges, const
     CUDA_TRY(cudaMemcpy(g.d_row, h_row, sizeof(int) * (size_t(nodes) + 1), cudaMemcpyHostToDevice), "upload");
     CUDA_TRY(cudaMemset(g.d_col + edges, 0, 4 * sizeof(int)), "column padding");
     if (edges) CUDA_TRY(cudaMemcpy(g.d_col, h_col, sizeof(int) * size_t(edges), cudaMemcpyHostToDevice), "upload");
-    CUDA_TRY(ms_graph_symmetric(g.d_row, g.d_col, nodes, &g.symmetric), "graph symmetry check");
+    CUDA_TRY(ms_graph_symmetric(g.d_row, g.d_col, nodes, edges, &g.symmetric), "graph symmetry check");
     b->graphs.push_back(g);
     // Refresh the device graph table.
     std::vector<MsGraph> table(b->graphs.size());

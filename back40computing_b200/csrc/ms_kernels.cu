@@ -758,11 +758,11 @@ MsKernelFn pick(const MsKernelConfig &kc, size_t *smem) {
 
 }  // namespace
 
-cudaError_t ms_graph_symmetric(const int *d_row, const int *d_col, int nodes, int *symmetric) {
+cudaError_t ms_graph_symmetric(const int *d_row, const int *d_col, int nodes, long long edges, int *symmetric) {
     unsigned long long *d = nullptr, h[4] = {0, 0, 0, 0};
     cudaError_t e = cudaMalloc(&d, sizeof(h));
     if (!e) e = cudaMemset(d, 0, sizeof(h));
-    if (!e) e = launch_symmetry_hash(d_row, d_col, nodes, d, 0);
+    if (!e) e = launch_symmetry_hash(d_row, d_col, nodes, edges, d, 0);
     if (!e) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (!e) *symmetric = (h[0] == h[1] && h[2] == h[3]) ? 1 : 0;

@@ -88,7 +88,7 @@ struct MsKernelConfig {
 
 // Whether a resident graph is symmetric (the hash check of
 // launch_symmetry_hash; allocates and frees a 32-byte buffer, waits).
-cudaError_t ms_graph_symmetric(const int *d_row, const int *d_col, int nodes, int *symmetric);
+cudaError_t ms_graph_symmetric(const int *d_row, const int *d_col, int nodes, long long edges, int *symmetric);
 // Largest co-resident grid of the multi-search kernel.
 cudaError_t ms_grid_limit(const MsKernelConfig &kc, int *grid);
 // Cooperative launch: runs levels from Counters::cur_it until no search has
