@@ -60,9 +60,10 @@ struct alignas(256) Counters {
     unsigned zmarked;  // vertices without edges that bottom-up levels marked visited (whole search)
     unsigned bu_steal[4];  // multi-search: next bottom-up step of level q, at [q&3]
     unsigned pad_f[47];
-    unsigned bar_count;  // grid barrier
-    unsigned bar_gen;
-    unsigned pad_g[61];
+    unsigned bar_count;  // grid_barrier_serial: arrivals of the current barrier
+    unsigned bar_gen;    // grid_barrier_serial: generation
+    unsigned long long bar_total;  // grid_barrier: arrivals since the counters were cleared
+    unsigned pad_g[59];
     unsigned sticky;  // OR of error over searches since the host last read it (not reset per search)
 };
 
@@ -87,6 +88,16 @@ __device__ __forceinline__ unsigned atom_add_acqrel_gpu(unsigned *p, unsigned v)
     unsigned old;
     asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
     return old;
+}
+__device__ __forceinline__ unsigned long long atom_add_acqrel_gpu_u64(unsigned long long *p, unsigned long long v) {
+    unsigned long long old;
+    asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ unsigned long long ld_acquire_gpu_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
 }
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
     unsigned long long t;
@@ -129,32 +140,31 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 
 // ---- grid barrier ----------------------------------------------------------------
 // All CTAs of a cooperative launch call this the same number of times.  Each
-// CTA's thread 0 reads the generation, arrives with an acq_rel add, and either
-// (last arrival) resets the count and publishes generation+1, or spins with an
-// acquire load until the generation moves, the error word becomes non-zero, or
-// wait_ns of %globaltimer time pass (then ERR_BARRIER_TIMEOUT is raised and
-// the CTA leaves the wait).  Returns false on any raised error, identically
-// for every thread of the CTA.
+// CTA's thread 0 arrives with an acq_rel add on a 64-bit count of all
+// arrivals since the counters were cleared; the barrier it is in ends when the
+// count reaches the next multiple of `expected`, which every waiting CTA sees
+// directly (no last-arriver flip of a generation word, one L2 round trip
+// less).  A waiting CTA spins with an acquire load until then, the error word
+// becomes non-zero, or wait_ns of %globaltimer time pass (then
+// ERR_BARRIER_TIMEOUT is raised and the CTA leaves the wait).  Returns false
+// on any raised error, identically for every thread of the CTA.
 __device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wait_ns,
                                              unsigned *smem_flag, unsigned expected) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned gen = ld_acquire_gpu(&c->bar_gen);
-        unsigned arrived = atom_add_acqrel_gpu(&c->bar_count, 1u);
-        if (arrived == expected - 1) {
-            st_relaxed_gpu(&c->bar_count, 0u);
-            st_release_gpu(&c->bar_gen, gen + 1u);
-        } else {
-            unsigned long long t0 = globaltimer_ns();
-            unsigned ns = 32;
-            while (ld_acquire_gpu(&c->bar_gen) == gen) {
+        const unsigned long long arrived = atom_add_acqrel_gpu_u64(&c->bar_total, 1ull);
+        const unsigned long long target = (arrived / expected + 1ull) * expected;
+        if (arrived + 1ull != target) {
+            const unsigned long long t0 = globaltimer_ns();
+            unsigned ns = 16;
+            while (ld_acquire_gpu_u64(&c->bar_total) < target) {
                 if (ld_relaxed_gpu(&c->error) != 0u) break;
                 if (globaltimer_ns() - t0 > wait_ns) {
                     atomicOr(&c->error, ERR_BARRIER_TIMEOUT);
                     break;
                 }
                 __nanosleep(ns);
-                if (ns < 256) ns <<= 1;
+                if (ns < 128) ns <<= 1;
             }
         }
         *smem_flag = ld_relaxed_gpu(&c->error);

@@ -990,9 +990,12 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
     for (;;) {
         clk.start(p);
         const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]), nw = ld_cg(&c->wch[it & 3]);
+        // the direction counts are loaded with the queue counts (one round trip)
+        const unsigned nf = p.do_alpha ? ld_cg(&c->nf[it & 3]) : 0u;
+        const unsigned long long mf = p.do_alpha ? __ldcg(&c->mf[it & 3]) : 0ull;
         if (stop_level_loop(p, it, L + nch + nw)) break;
         bool bottom_up = false;
-        if (!MP && p.do_alpha) bottom_up = dir.next(p, ld_cg(&c->nf[it & 3]), __ldcg(&c->mf[it & 3]));
+        if (!MP && p.do_alpha) bottom_up = dir.next(p, nf, mf);
         if (leader()) {
             ring_prepare(c, it);
             c->total_queued += L;

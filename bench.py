@@ -26,6 +26,9 @@ two-phase and hybrid are timed the same way and reported under "strategies".
           and p50/p99 latency against sequential EnactSearch serving the
           same trace.
 
+  lattices  grid2d 1024^2 and grid3d 256^3 single searches, every strategy
+          (deep, narrow searches: per-level cost rather than bandwidth).
+
 --impl reference runs the reference's own CPU BFS (SimpleReferenceBfs, built
 into oracle/_ref) on all host cores instead.  With torchrun each rank runs an
 independent replica (its own 64 sources; no collective on the data path) and
@@ -69,6 +72,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 1024-search batched leg")
     ap.add_argument("--no-served", action="store_true", help="skip the Poisson-trace serving leg")
+    ap.add_argument("--no-lattices", action="store_true", help="skip the grid2d / grid3d single-search leg")
     ap.add_argument("--verify", type=int, default=2, help="sources checked against the oracle")
     ap.add_argument("--sources", type=int, default=NUM_SOURCES, help="sources per step (64 for the bench line)")
     return ap.parse_args()
@@ -432,6 +436,47 @@ def batched_leg(b, torch, stream, args):
     }
 
 
+def lattice_leg(b, torch, stream, args):
+    """The lattice workloads: grid2d 1024 x 1024 from its centre (1,048,576
+    vertices, 4,190,208 entries) and grid3d 256^3 from vertex 0 (16,777,216
+    vertices, 100,270,080 entries; 766 levels): single searches with each
+    strategy, device time, labels checked against the oracle once."""
+    from back40computing_b200 import graphs
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle import Oracle
+    orc = Oracle()
+    out = {}
+    for name, g, src in (("grid2d-1024", graphs.grid2d(1024), 512 * 1024 + 512), ("grid3d-256", graphs.grid3d(256), 0)):
+        ref, _ = orc.bfs(g, src)
+        E = float(g.degrees()[ref > -1].astype(np.int64).sum())
+        prob = b.CsrProblem(False).from_graph(g)
+        prob.set_stream(stream.cuda_stream)
+        row = {"nodes": g.nodes, "edges": g.edges, "source": src, "depth": int(ref.max())}
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        for strat in (0, 1, 2, 3):
+            en = b.make_enactor(strat)
+            en.set_stream(stream.cuda_stream)
+            ft = en.GetFrontierType()
+            b.check(prob.Reset(ft, 1.3))
+            b.check(en.EnactSearch(prob, src))
+            if orc.first_mismatch(prob.labels(), ref) != -1:
+                raise SystemExit(f"bench: {name} labels of strategy {strat} differ from the oracle")
+            ms = []
+            for _ in range(max(3, args.steps // 2)):
+                b.check(prob.ResetAsync(ft, 1.3))
+                ev[0].record(stream)
+                b.check(en.EnactSearchAsync(prob, src, 0, 1))
+                ev[1].record(stream)
+                b.check(en.Sync())
+                ms.append(ev[0].elapsed_time(ev[1]))
+            t = float(np.median(ms))
+            row[STRATEGY_NAMES[strat]] = {"ms": t, "gteps": E / (t / 1e3) / 1e9, "us_per_level": t * 1e3 / (row["depth"] + 1)}
+            del en
+        prob.close()
+        out[name] = row
+    return out
+
+
 def served_leg(b, torch, stream, args, main_graph):
     """Poisson traces over 32 resident graphs through the continuous-batching
     server, against sequential plain EnactSearch serving the same trace in FIFO
@@ -667,6 +712,9 @@ def main():
         batched = batched_leg(b, torch, stream, args)
     if world == 1 and not args.no_served:
         served = served_leg(b, torch, stream, args, g)
+    lattices = None
+    if world == 1 and not args.no_lattices:
+        lattices = lattice_leg(b, torch, stream, args)
 
     # CPU baseline: the reference's CPU BFS on a bounded sample, rank 0 at N=1.
     cpu = None
@@ -708,6 +756,7 @@ def main():
         "cpu_baseline": cpu,
         "batched": batched,
         "served": served,
+        "lattices": lattices,
     }
     print(json.dumps(line), flush=True)
 
