@@ -650,6 +650,54 @@ extern "C" int b40c_problem_extract_results(b40c_problem_t *p, int *h_labels) {
     return B40C_SUCCESS;
 }
 
+extern "C" int b40c_problem_from_host_ids64(b40c_problem_t *p, int stream_from_host, int nodes, int edges,
+                                            const long long *h_col, const int *h_row, int num_gpus) {
+    clear_error();
+    if (!p || nodes <= 0 || edges < 0 || !h_row || (edges > 0 && !h_col))
+        return set_error(B40C_ERR_INVALID_VALUE, "FromHostProblem: invalid arguments");
+    if (stream_from_host)
+        return set_error(B40C_ERR_NOT_SUPPORTED,
+                         "FromHostProblem: 8-byte vertex ids are narrowed to the device's int32 layout, which "
+                         "stream_from_host cannot map");
+    // Every id of a graph whose sizes are int (SizeT) fits in int32: narrow
+    // on several host threads, rejecting ids outside [0, nodes).
+    std::vector<int> col(size_t(edges) + 1);
+    unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<long long> bad(nt, -1);
+    std::vector<std::thread> pool;
+    const long long chunk = (edges + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; t++) {
+        pool.emplace_back([&, t] {
+            const long long lo = std::min<long long>(edges, t * chunk), hi = std::min<long long>(edges, lo + chunk);
+            for (long long k = lo; k < hi; k++) {
+                const long long v = h_col[k];
+                if (v < 0 || v >= nodes) {
+                    bad[t] = k;
+                    break;
+                }
+                col[size_t(k)] = int(v);
+            }
+        });
+    }
+    for (auto &th : pool) th.join();
+    for (unsigned t = 0; t < nt; t++)
+        if (bad[t] >= 0)
+            return set_error(B40C_ERR_INVALID_VALUE, "CSR column index %lld at edge %lld outside [0, %d)",
+                             h_col[bad[t]], bad[t], nodes);
+    return b40c_problem_from_host(p, 0, nodes, edges, col.data(), h_row, num_gpus);
+}
+
+extern "C" int b40c_problem_extract_results_ids64(b40c_problem_t *p, long long *h_labels) {
+    clear_error();
+    if (!p || !h_labels) return set_error(B40C_ERR_INVALID_VALUE, "ExtractResults: NULL argument");
+    if (!p->d_labels) return set_error(B40C_ERR_ILLEGAL_STATE, "ExtractResults before Reset");
+    std::vector<int> tmp(size_t(p->nodes));
+    int rc = b40c_problem_extract_results(p, tmp.data());
+    if (rc) return rc;
+    for (size_t i = 0; i < tmp.size(); i++) h_labels[i] = tmp[i];
+    return B40C_SUCCESS;
+}
+
 extern "C" int b40c_problem_extract_results_async(b40c_problem_t *p, int *h_labels) {
     clear_error();
     if (!p || !h_labels) return set_error(B40C_ERR_INVALID_VALUE, "ExtractResults: NULL argument");

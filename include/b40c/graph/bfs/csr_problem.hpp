@@ -33,15 +33,34 @@ struct ProblemType {
     static const bool MARK_PREDECESSORS = _MARK_PREDECESSORS;
 };
 
+/* Host-side id width of FromHostProblem / ExtractResults: 4-byte ids go to
+ * the device as they are; 8-byte ids (the reference's g500 configuration,
+ * VertexId = long long with int sizes) are narrowed to the device's int32
+ * layout and widened on the way back. */
+inline int b40c_from_host_any(b40c_problem_t *h, int sfh, int n, int m, int *col, int *row, int g) {
+    return b40c_problem_from_host(h, sfh, n, m, col, row, g);
+}
+inline int b40c_from_host_any(b40c_problem_t *h, int sfh, int n, int m, long long *col, int *row, int g) {
+    return b40c_problem_from_host_ids64(h, sfh, n, m, col, row, g);
+}
+inline int b40c_extract_any(b40c_problem_t *h, int *labels) { return b40c_problem_extract_results(h, labels); }
+inline int b40c_extract_any(b40c_problem_t *h, long long *labels) {
+    return b40c_problem_extract_results_ids64(h, labels);
+}
+
 /*
  * bfs::CsrProblem<VertexId, SizeT, MARK_PREDECESSORS> (csr_problem.cuh:68-751).
- * VertexId and SizeT must be int (the device layout is int32).  Members that
- * reference callers read -- nodes, edges, num_gpus, and the single graph
- * slice's device pointers -- are kept up to date.
+ * SizeT must be int; VertexId int, or long long as the reference's g500
+ * graphs use (test/bfs/test_bfs.cu:1068-1093).  The device layout is int32
+ * either way: with 8-byte ids the slice's d_column_indices / d_labels point
+ * at int32 arrays.  Members that reference callers read -- nodes, edges,
+ * num_gpus, and the single graph slice's device pointers -- are kept up to
+ * date.
  */
 template <typename _VertexId, typename _SizeT, bool MARK_PREDECESSORS>
 struct CsrProblem {
-    static_assert(sizeof(_VertexId) == 4 && sizeof(_SizeT) == 4, "the B200 BFS stores int32 ids and offsets");
+    static_assert((sizeof(_VertexId) == 4 || sizeof(_VertexId) == 8) && sizeof(_SizeT) == 4,
+                  "the B200 BFS takes int or long long vertex ids with int sizes");
 
     typedef bfs::ProblemType<_VertexId, _SizeT, MARK_PREDECESSORS> ProblemType;
     typedef typename ProblemType::VertexId VertexId;
@@ -77,8 +96,8 @@ struct CsrProblem {
     /* csr_problem.cuh:328-403 */
     cudaError_t FromHostProblem(bool stream_from_host, SizeT nodes, SizeT edges, VertexId *h_column_indices,
                                 SizeT *h_row_offsets, int num_gpus) {
-        int rc = b40c_problem_from_host(handle, stream_from_host ? 1 : 0, nodes, edges, h_column_indices,
-                                        h_row_offsets, num_gpus);
+        int rc = b40c_from_host_any(handle, stream_from_host ? 1 : 0, (int)nodes, (int)edges, h_column_indices,
+                                    (int *)h_row_offsets, num_gpus);
         if (rc == 0) {
             this->nodes = nodes;
             this->edges = edges;
@@ -97,7 +116,7 @@ struct CsrProblem {
 
     /* csr_problem.cuh:255-273 */
     cudaError_t ExtractResults(VertexId *h_label) {
-        return (cudaError_t)b40c_problem_extract_results(handle, h_label);
+        return (cudaError_t)b40c_extract_any(handle, h_label);
     }
 
     /* csr_problem.cuh:188-218 (one slice) */

@@ -82,6 +82,14 @@ int b40c_problem_reset_async(b40c_problem_t *problem, int frontier_type, double 
 int b40c_problem_extract_results(b40c_problem_t *problem, int *h_labels);
 /* Enqueues the label copy on the problem's stream without waiting. */
 int b40c_problem_extract_results_async(b40c_problem_t *problem, int *h_labels);
+/* 8-byte vertex ids with int sizes, the reference's g500 configuration
+ * (VertexId = long long, SizeT = int; test/bfs/test_bfs.cu:1068-1093):
+ * the column ids are checked and narrowed to the device's int32 layout (every
+ * id of a graph with int sizes fits), labels are widened on the way out.
+ * stream_from_host is not available with 8-byte ids (cudaErrorNotSupported). */
+int b40c_problem_from_host_ids64(b40c_problem_t *problem, int stream_from_host, int nodes, int edges,
+                                 const long long *h_column_indices, const int *h_row_offsets, int num_gpus);
+int b40c_problem_extract_results_ids64(b40c_problem_t *problem, long long *h_labels);
 /* nodes, edges and the GraphSlice device pointers (:99-173). Any out pointer may be NULL. */
 int b40c_problem_info(b40c_problem_t *problem, int64_t *nodes, int64_t *edges,
                       void **d_row_offsets, void **d_column_indices,

@@ -409,3 +409,31 @@ def test_instrument_statistics(cuda_device, oracle, rmat16, strategy):
             assert 0.0 < duty <= 1.0
         else:
             assert queued == 0 and duty == 0.0
+
+
+def test_eight_byte_vertex_ids(cuda_device, oracle, rmat16):
+    """The g500 configuration (VertexId = long long, SizeT = int): ids are
+    narrowed on upload, labels widened on extraction, results unchanged."""
+    import ctypes
+    from back40computing_b200._lib import lib
+    b = bfs_mod()
+    g = rmat16
+    s = int(g.sample_sources(1, 44)[0])
+    ref, _ = oracle.bfs(g, s)
+    col64 = g.column_indices.astype(np.int64)
+    prob = b.CsrProblem(False)
+    P = ctypes.c_void_p
+    assert lib().b40c_problem_from_host_ids64(prob._h, 0, g.nodes, g.edges, col64.ctypes.data_as(P),
+                                              g.row_offsets.ctypes.data_as(P), 1) == 0
+    en = b.make_enactor(1)
+    b.check(prob.Reset(en.GetFrontierType(), 1.3))
+    b.check(en.EnactSearch(prob, s))
+    out = np.empty(g.nodes, np.int64)
+    assert lib().b40c_problem_extract_results_ids64(prob._h, out.ctypes.data_as(P)) == 0
+    assert np.array_equal(out, ref.astype(np.int64))
+    bad = col64.copy()
+    bad[7] = g.nodes + (1 << 33)
+    assert lib().b40c_problem_from_host_ids64(prob._h, 0, g.nodes, g.edges, bad.ctypes.data_as(P),
+                                              g.row_offsets.ctypes.data_as(P), 1) == 1
+    assert lib().b40c_problem_from_host_ids64(prob._h, 1, g.nodes, g.edges, col64.ctypes.data_as(P),
+                                              g.row_offsets.ctypes.data_as(P), 1) == 801

@@ -34,6 +34,17 @@ int run(int n, int m, int *col, int *row, int *labels) {
     contract_expand.GetStatistics(total_queued, search_depth, avg_duty);
     return csr_problem.ExtractResults(labels) ? 1 : 0;
 }
+// the reference's g500 configuration: 8-byte vertex ids, int sizes
+int run_g500(int n, int m, long long *col, int *row, long long *labels) {
+    bfs::CsrProblem<long long, int, false> csr_problem;
+    if (csr_problem.FromHostProblem(false, n, m, col, row, 1)) return 1;
+    bfs::EnactorHybrid<false> hybrid(false);
+    if (csr_problem.Reset(hybrid.GetFrontierType(), 1.3)) return 1;
+    if (hybrid.EnactSearch(csr_problem, (long long)0)) return 1;
+    long long total_queued = 0; long long search_depth = 0; double avg_duty = 0;
+    hybrid.GetStatistics(total_queued, search_depth, avg_duty);
+    return csr_problem.ExtractResults(labels) ? 1 : 0;
+}
 """)
     cuda_inc = "/usr/local/cuda/include"
     r = subprocess.run(["g++", "-std=c++11", "-c", "-I", str(ROOT / "include"), "-I", cuda_inc, str(src), "-o",
