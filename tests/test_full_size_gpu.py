@@ -1,0 +1,62 @@
+"""Parity at the bench's full size: R-MAT scale 22, edge factor 16
+(4,194,304 vertices, 134,214,068 entries), every strategy bit-exact against
+the oracle, and properties that hold at any size (one label per reached
+vertex, every edge spans at most one level, every reached vertex but the
+source has a neighbour one level up)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def s22():
+    import back40computing_b200 as b
+    return b.rmat(22, 16, 0.57, 0.19, 0.19, seed=1, undirected=True)
+
+
+def _level_properties(g, labels, src):
+    row = g.row_offsets.astype(np.int64)
+    col = g.column_indices
+    u = np.repeat(np.arange(g.nodes), np.diff(row))
+    lu, lv = labels[u], labels[col]
+    reached = lu >= 0
+    assert labels[src] == 0
+    assert np.all(lv[reached] >= 0)                       # a reached vertex's neighbours are reached
+    assert np.all(np.abs(lu[reached] - lv[reached]) <= 1)  # edges span at most one level
+    has_parent = np.zeros(g.nodes, bool)
+    up = reached & (lv == lu - 1)
+    has_parent[u[up]] = True
+    r = labels > 0
+    assert np.all(has_parent[r])                           # every reached vertex has a parent one level up
+
+
+def test_rmat22_all_strategies_bit_exact(cuda_device, oracle, s22):
+    import back40computing_b200 as b
+    g = s22
+    prob = b.CsrProblem(False).from_graph(g)
+    for k, s in enumerate(g.sample_sources(2, 2)):
+        ref, _ = oracle.bfs(g, int(s))
+        for strategy in (0, 1, 2, 3):
+            en = b.make_enactor(strategy)
+            b.check(prob.Reset(en.GetFrontierType(), 1.3))
+            b.check(en.EnactSearch(prob, int(s)))
+            labels = prob.labels()
+            assert oracle.first_mismatch(labels, ref) == -1, (strategy, int(s))
+            if k == 0 and strategy == 0:
+                _level_properties(g, labels, int(s))
+
+
+def test_rmat22_predecessors_valid(cuda_device, oracle, s22):
+    import back40computing_b200 as b
+    g = s22
+    s = int(g.sample_sources(1, 9)[0])
+    ref, _ = oracle.bfs(g, s)
+    prob = b.CsrProblem(True).from_graph(g)
+    for strategy in (0, 1):
+        en = b.make_enactor(strategy)
+        b.check(prob.Reset(en.GetFrontierType(), 1.3))
+        b.check(en.EnactSearch(prob, s))
+        assert oracle.check_predecessors(g, prob.labels(), ref)[0] == -1, strategy
