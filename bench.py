@@ -73,6 +73,9 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true", help="skip the 1024-search batched leg")
     ap.add_argument("--no-served", action="store_true", help="skip the Poisson-trace serving leg")
     ap.add_argument("--no-lattices", action="store_true", help="skip the grid2d / grid3d single-search leg")
+    ap.add_argument("--batched-max-scale", type=int, default=20, help="largest R-MAT scale of the batched set")
+    ap.add_argument("--batched-policy", default="tuned", choices=["tuned", "default"],
+                    help="autotuned multi-search policy, or the library defaults")
     ap.add_argument("--verify", type=int, default=2, help="sources checked against the oracle")
     ap.add_argument("--sources", type=int, default=NUM_SOURCES, help="sources per step (64 for the bench line)")
     return ap.parse_args()
@@ -289,15 +292,15 @@ def reference_arm(args):
 # Batched and served legs (multi-search kernel vs back-to-back single searches)
 # ------------------------------------------------------------------------------------------
 
-def batched_set(seed=4):
-    """64 graphs: R-MAT with scale uniform in 12..20 and edge factor uniform in
-    8..32, every fourth an Erdos-Renyi G(n, 16/(n-1)) of the same n; 16 seeded
-    sources each (1024 searches)."""
+def batched_set(seed=4, max_scale=20):
+    """64 graphs: R-MAT with scale uniform in 12..max_scale (20 for the bench
+    line) and edge factor uniform in 8..32, every fourth an Erdos-Renyi
+    G(n, 16/(n-1)) of the same n; 16 seeded sources each (1024 searches)."""
     from back40computing_b200 import graphs
     rng = np.random.default_rng(seed)
     gs, desc = [], []
     for i in range(64):
-        scale = int(rng.integers(12, 21))
+        scale = min(int(rng.integers(12, 21)), max_scale)
         ef = int(rng.integers(8, 33))
         n = 1 << scale
         if i % 4 == 3:
@@ -375,7 +378,7 @@ def batched_leg(b, torch, stream, args):
     the same searches as back-to-back EnactSearch calls; device time, labels
     compared by checksum for every search."""
     from back40computing_b200.batch import BfsBatch
-    gs, desc, gids, srcs = batched_set()
+    gs, desc, gids, srcs = batched_set(max_scale=args.batched_max_scale)
     n = len(gids)
     seq = SequentialSearches(b, gs, stream)
     crc_seq = np.zeros(n, np.int64)
@@ -405,7 +408,8 @@ def batched_leg(b, torch, stream, args):
     # The multi-search policy picked by the autotuner for this workload (its
     # B200 result ships with the package; a different workload is tuned here).
     from back40computing_b200 import tune
-    policy = tune.tune_batch(gs, gids, srcs, cache=tune.TuneCache(None, seed=tune.SHIPPED))
+    policy = (tune.tune_batch(gs, gids, srcs, cache=tune.TuneCache(None, seed=tune.SHIPPED))
+              if args.batched_policy == "tuned" else dict(tune.DEFAULT_POLICY))
     batch = BfsBatch()
     tune.apply_batch_policy(batch, policy)
     batch.set_stream(stream.cuda_stream)
@@ -424,7 +428,8 @@ def batched_leg(b, torch, stream, args):
     batch.close()
     s_ms, b_ms = float(np.median(seq_ms)), float(np.median(bat_ms))
     return {
-        "workload": "64 graphs (48 R-MAT scale 12..20 ef 8..32, 16 Erdos-Renyi mean degree 16), 16 sources each",
+        "workload": f"64 graphs (48 R-MAT scale 12..{args.batched_max_scale} ef 8..32, 16 Erdos-Renyi mean degree 16), "
+                    "16 sources each",
         "searches": n, "graph_edges_total": int(sum(g.edges for g in gs)),
         "queries_per_s": n / (b_ms / 1e3), "gteps": float(edges.sum()) / (b_ms / 1e3) / 1e9,
         "ms_per_batch": b_ms,
