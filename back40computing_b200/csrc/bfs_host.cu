@@ -745,11 +745,13 @@ extern "C" int b40c_enactor_create(int strategy, int instrument, int debug, b40c
     b40c_enactor *e = new (std::nothrow) b40c_enactor();
     if (!e) return set_error(B40C_ERR_MEMORY_ALLOCATION, "enactor allocation");
     e->strategy = strategy;
-    // Measured defaults on R-MAT graphs: expand-contract gathers lists of
-    // 128+ edges with warps, the edge-frontier strategies lists of 64+.
+    // Measured defaults: expand-contract runs 512-thread CTAs and gathers
+    // lists of 128+ edges with warps; the edge-frontier strategies run
+    // 256-thread CTAs and gather lists of 64+.
     // Expand-contract switches direction with the published alpha = 14,
     // beta = 24 (Beamer, Asanovic and Patterson, SC 2012).
     if (strategy == B40C_EXPAND_CONTRACT) {
+        e->threads = 512;  // measured best for expand-contract on R-MAT and lattices alike
         e->warp_th = 128;
         e->do_alpha = 14;
         e->do_beta = 24;

@@ -441,10 +441,12 @@ __device__ __forceinline__ unsigned next_run(unsigned nruns, unsigned *steal) {
 // an atomic per discovery group would make the counters a hot spot).
 template <bool MP>
 __device__ __forceinline__ void count_discovered(WarpSmem<MP> &ws, int n, long long deg) {
-    const int nt = warp_sum(n);
-    const long long dt = warp_sum_ll(deg);
-    if (lane_id() == 0) {
-        ws.disc_n += unsigned(nt);
+    // Degrees of distinct vertices of one graph sum to less than its int32
+    // edge count, so 32-bit warp reductions (one instruction each) suffice.
+    const unsigned nt = __reduce_add_sync(0xffffffffu, unsigned(n));
+    const unsigned dt = __reduce_add_sync(0xffffffffu, unsigned(deg));
+    if (lane_id() == 0 && nt) {
+        ws.disc_n += nt;
         ws.disc_m += (unsigned long long)dt;
     }
 }

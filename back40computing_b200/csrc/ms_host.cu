@@ -54,7 +54,7 @@ struct GraphRes {
 struct b40c_batch {
     int device = 0;
     bool mark_pred = false;
-    int threads = 256, warp_th = 128, cta_th = 1024;
+    int threads = 512, warp_th = 128, cta_th = 1024;  // 512-thread CTAs: measured best for the mixed batch
     unsigned cull_flags = CULL_HISTORY;
     unsigned do_alpha = 14, do_beta = 24;  // direction-optimizing (published alpha, beta); 0: top-down only
     unsigned long long wait_ns = 5000000000ull;

@@ -104,7 +104,7 @@ struct SlotUse {
 struct b40c_server {
     int device = 0;
     bool mark_pred = false;
-    int threads = 256, warp_th = 128, cta_th = 1024;
+    int threads = 512, warp_th = 128, cta_th = 1024;  // 512-thread CTAs: measured best for the mixed batch
     unsigned cull_flags = CULL_HISTORY;
     unsigned long long wait_ns = 5000000000ull;
     int epoch_levels = 8;

@@ -32,7 +32,7 @@ WARP_THRESHOLDS = (32, 64, 128, 256)
 CTA_THRESHOLDS = (512, 1024, 4096)
 DIRECTIONS = ((0, 0), (14, 24), (6, 24))  # (alpha, beta); (0, 0) = top-down only
 # The library's defaults for expand-contract searches and batches.
-DEFAULT_POLICY = {"cta_threads": 256, "warp_gather_threshold": 128, "cta_gather_threshold": 1024,
+DEFAULT_POLICY = {"cta_threads": 512, "warp_gather_threshold": 128, "cta_gather_threshold": 1024,
                   "alpha": 14, "beta": 24}
 
 DEFAULT_CACHE = Path(os.environ.get("B40C_TUNE_CACHE", Path.home() / ".cache" / "b40c_bfs_tune.json"))

@@ -445,7 +445,8 @@ def lattice_leg(b, torch, stream, args):
     """The lattice workloads: grid2d 1024 x 1024 from its centre (1,048,576
     vertices, 4,190,208 entries) and grid3d 256^3 from vertex 0 (16,777,216
     vertices, 100,270,080 entries; 766 levels): single searches with each
-    strategy, device time, labels checked against the oracle once."""
+    strategy in the persistent kernel and as per-level launches, device
+    time, labels checked against the oracle once."""
     from back40computing_b200 import graphs
     sys.path.insert(0, str(ROOT / "oracle"))
     from oracle import Oracle
@@ -476,6 +477,16 @@ def lattice_leg(b, torch, stream, args):
                 ms.append(ev[0].elapsed_time(ev[1]))
             t = float(np.median(ms))
             row[STRATEGY_NAMES[strat]] = {"ms": t, "gteps": E / (t / 1e3) / 1e9, "us_per_level": t * 1e3 / (row["depth"] + 1)}
+            if strat != 3:  # the same search as per-level launches (a CUDA graph with a conditional loop)
+                it_ms = []
+                for _ in range(3):
+                    b.check(prob.ResetAsync(ft, 1.3))
+                    ev[0].record(stream)
+                    b.check(en.EnactSearchAsync(prob, src, 0, 2))
+                    ev[1].record(stream)
+                    b.check(en.Sync())
+                    it_ms.append(ev[0].elapsed_time(ev[1]))
+                row[STRATEGY_NAMES[strat]]["per_level_launches_ms"] = float(np.median(it_ms[1:]))
             del en
         prob.close()
         out[name] = row

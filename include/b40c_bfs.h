@@ -134,7 +134,8 @@ int b40c_enactor_last_elapsed_ms(b40c_enactor_t *enactor, float *ms);
 /* Stream (a cudaStream_t) for later searches; NULL = the enactor's own stream. */
 int b40c_enactor_set_stream(b40c_enactor_t *enactor, void *stream);
 /* Tuning policy (the reference's compile-time KernelPolicy, kernel_policy.cuh:61-87,
- * WARP_GATHER_THRESHOLD / CTA_GATHER_THRESHOLD): cta_threads in {128,256,512};
+ * WARP_GATHER_THRESHOLD / CTA_GATHER_THRESHOLD): cta_threads in {128,256,512}
+ * (default 512 for expand-contract, 256 for the others);
  * lists of at least cta_gather_threshold edges (default 1024) are cut into
  * chunks of 16 * cta_threads edges, each gathered by a whole CTA; lists of at
  * least warp_gather_threshold edges (default 64) into chunks of 512 edges,

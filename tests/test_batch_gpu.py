@@ -56,7 +56,7 @@ def test_batch_predecessors_valid(cuda_device, oracle, mixed_graphs):
     _check(oracle, batch, mixed_graphs, gids, srcs, mark_pred=True)
 
 
-@pytest.mark.parametrize("policy", [dict(cta_threads=128), dict(cta_threads=512),
+@pytest.mark.parametrize("policy", [dict(cta_threads=128), dict(cta_threads=256), dict(cta_threads=512),
                                     dict(warp_gather_threshold=8, cta_gather_threshold=64),
                                     dict(warp_gather_threshold=100000, cta_gather_threshold=100000),
                                     dict(cull_flags=0), dict(cull_flags=3)],

@@ -99,6 +99,7 @@ def test_rmat16_vs_oracle(cuda_device, oracle, rmat16, strategy, variant):
 # most lists to the CTA and grid-wide (big-list) phases; culls on and off.
 POLICIES = [
     dict(cta_threads=128),
+    dict(cta_threads=256),
     dict(cta_threads=512),
     dict(warp_gather_threshold=4, cta_gather_threshold=16),
     dict(warp_gather_threshold=1, cta_gather_threshold=1),

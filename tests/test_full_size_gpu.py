@@ -60,3 +60,19 @@ def test_rmat22_predecessors_valid(cuda_device, oracle, s22):
         b.check(prob.Reset(en.GetFrontierType(), 1.3))
         b.check(en.EnactSearch(prob, s))
         assert oracle.check_predecessors(g, prob.labels(), ref)[0] == -1, strategy
+
+
+def test_grid3d_256_fused_and_per_level(cuda_device, oracle):
+    """The high-diameter case: grid3d 256^3 from the corner (765 levels), every
+    strategy in the persistent kernel and in per-level launches, bit-exact."""
+    import back40computing_b200 as b
+    g = b.grid3d(256)
+    ref, _ = oracle.bfs(g, 0)
+    assert int(ref.max()) == 765
+    prob = b.CsrProblem(False).from_graph(g)
+    for strategy in (0, 1, 2, 3):
+        for variant in (1, 2):
+            en = b.make_enactor(strategy)
+            b.check(prob.Reset(en.GetFrontierType(), 1.3))
+            b.check(en.EnactFusedSearch(prob, 0) if variant == 1 else en.EnactIterativeSearch(prob, 0))
+            assert oracle.first_mismatch(prob.labels(), ref) == -1, (strategy, variant)
