@@ -138,7 +138,8 @@ int b40c_enactor_set_stream(b40c_enactor_t *enactor, void *stream);
  * (default 512 for expand-contract, 256 for the others);
  * lists of at least cta_gather_threshold edges (default 1024) are cut into
  * chunks of 16 * cta_threads edges, each gathered by a whole CTA; lists of at
- * least warp_gather_threshold edges (default 64) into chunks of 512 edges,
+ * least warp_gather_threshold edges (default 128 for expand-contract, 64 for
+ * the others) into chunks of 512 edges,
  * each gathered by one warp; chunks are shared by the whole grid; shorter
  * lists are gathered by a warp prefix sum.  cull_flags: bit0 warp-level cull
  * (__match_any_sync), bit1 history cull through a per-CTA shared-memory cache
