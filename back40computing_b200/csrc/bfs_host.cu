@@ -74,6 +74,8 @@ struct b40c_problem {
     cudaStream_t own_stream = nullptr;
     int symmetric = -1;                    // -1 unknown, 0 no, 1 yes (checked on first use)
     unsigned long long *d_sym = nullptr;   // 4 hash sums of the symmetry check
+    unsigned *d_mask_snap = nullptr;       // predecessor-label bottom-up levels: visited-mask copy
+    size_t mask_snap_cap = 0;
 };
 
 struct b40c_enactor {
@@ -156,6 +158,9 @@ void free_problem_device(b40c_problem *p) {
     cudaFree(p->d_sym);
     p->d_sym = nullptr;
     p->symmetric = -1;
+    cudaFree(p->d_mask_snap);
+    p->d_mask_snap = nullptr;
+    p->mask_snap_cap = 0;
 }
 
 // Whether every entry v of row u has an entry u in row v (a symmetric,
@@ -360,10 +365,19 @@ int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size,
     // The hybrid switches between its two bodies inside one persistent launch;
     // like the reference's EnactorHybrid it has a single way to run a search.
     if (variant == B40C_VARIANT_DEFAULT || e->strategy == B40C_HYBRID) variant = B40C_VARIANT_FUSED;
-    // Bottom-up levels: fused expand-contract, depth labels, symmetric graph.
-    if (e->strategy == B40C_EXPAND_CONTRACT && variant == B40C_VARIANT_FUSED && !p->mark_pred && e->do_alpha) {
+    // Bottom-up levels: fused expand-contract on a symmetric graph; with
+    // predecessor labels they probe a copy of the visited mask.
+    if (e->strategy == B40C_EXPAND_CONTRACT && variant == B40C_VARIANT_FUSED && e->do_alpha) {
         if ((rc = ensure_symmetry_known(p))) return rc;
         if (p->symmetric == 1) {
+            if (p->mark_pred && p->mask_snap_cap < p->mask_bytes) {
+                cudaFree(p->d_mask_snap);
+                p->d_mask_snap = nullptr;
+                p->mask_snap_cap = 0;
+                CUDA_TRY(cudaMalloc(&p->d_mask_snap, p->mask_bytes), "cudaMalloc visited-mask copy");
+                p->mask_snap_cap = p->mask_bytes;
+            }
+            bp.mask_snap = p->d_mask_snap;
             bp.do_alpha = e->do_alpha;
             bp.do_beta = e->do_beta;
         }

@@ -635,7 +635,8 @@ __device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, u
 // marked visited but never labelled: on a symmetric graph no list leads to
 // them, and later bottom-up levels skip them.  The discovered vertices are
 // counted and placed for level it+1 exactly as top-down discovery places
-// them, so either direction can run next.  Depth labels only.
+// them, so either direction can run next.  With predecessor labels the
+// probe tests a snapshot of the visited mask instead (see bu_step).
 constexpr int BU_WORDS = 4;  // = the 4 lists per lane that place4 and stage4 take
 constexpr int BU_PROBE = 2;
 static_assert(BU_WORDS == 4, "bottom-up steps hand 4 vertices per lane to place4 / stage4");
@@ -654,6 +655,7 @@ __device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0,
     for (int j = 0; j < BU_WORDS; j++) any_open |= mw[j] != FULL;
     if (!any_open) return;  // warp-uniform
     int v[BU_WORDS], st[BU_WORDS], ln[BU_WORDS];
+    int par[MP ? BU_WORDS : 1];  // predecessor labels: the parent found
     unsigned open = 0, scan = 0, found = 0;
 #pragma unroll
     for (int j = 0; j < BU_WORDS; j++) {
@@ -694,7 +696,18 @@ __device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0,
                 if (((scan >> j) & 1u) && k + e < ln[j]) {
                     const unsigned x = (unsigned)u[j][e];
                     if (x < (unsigned)p.nodes) {
-                        if (__ldca(p.labels + x) == it) found |= 1u << j;
+                        if constexpr (MP) {
+                            // labels hold predecessors: the probe reads the
+                            // snapshot of the visited mask taken at the level's
+                            // start; a visited neighbour of an unvisited vertex
+                            // has depth exactly it (symmetric graph).
+                            if (!((found >> j) & 1u) && ((__ldca(p.mask_snap + (x >> 5)) >> (x & 31u)) & 1u)) {
+                                found |= 1u << j;
+                                par[j] = int(x);
+                            }
+                        } else {
+                            if (__ldca(p.labels + x) == it) found |= 1u << j;
+                        }
                     } else {
                         atomicOr(&c->error, ERR_BAD_VERTEX);
                     }
@@ -717,7 +730,7 @@ __device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0,
         if (lane == 0 && (fb | zb)) __stcg(p.mask + w0 + j, mw[j] | fb | zb);
         if (lane == 0 && zb) atomicAdd(&c->zmarked, unsigned(__popc(zb)));
         if (f) {
-            p.labels[v[j]] = it + 1;
+            p.labels[v[j]] = MP ? par[j] : it + 1;
             nfound++;
             dfound += ln[j];
         }
@@ -727,10 +740,17 @@ __device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0,
     stage4(ws, found & ~placed, v, q_out, qlen_out, p.qcap, &c->error);
 }
 
+// Copies the visited mask into mask_snap (predecessor-label bottom-up
+// levels probe the copy); a grid barrier must follow before it is read.
+__device__ __forceinline__ void snapshot_mask(const BfsParams &p) {
+    const unsigned nwords = (unsigned(p.nodes) + 31u) >> 5;
+    for (unsigned w = blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += gridDim.x * blockDim.x)
+        p.mask_snap[w] = ld_cg(p.mask + w);
+}
+
 // open: an estimate of the vertices still unvisited.
 template <int THREADS, bool MP>
 __device__ void bu_level(const BfsParams &p, int it, Smem<THREADS, MP> &sm, unsigned open) {
-    static_assert(!MP, "bottom-up levels test depth labels");
     Counters *c = p.ctr;
     int *q_out = p.queue[(it + 1) & 1];
     unsigned *qlen_out = &c->qlen[(it + 1) & 3];
@@ -997,18 +1017,19 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
         const unsigned long long mf = p.do_alpha ? __ldcg(&c->mf[it & 3]) : 0ull;
         if (stop_level_loop(p, it, L + nch + nw)) break;
         bool bottom_up = false;
-        if (!MP && p.do_alpha) bottom_up = dir.next(p, nf, mf);
+        if (p.do_alpha) bottom_up = dir.next(p, nf, mf);
         if (leader()) {
             ring_prepare(c, it);
             c->total_queued += L;
             log_phase(p, it, L, nch, nw, bottom_up ? 1u : 0u);
         }
-        if constexpr (!MP) {
-            if (bottom_up) {
-                const unsigned done = dir.visited + ld_cg(&c->zmarked);
-                bu_level<THREADS, MP>(p, it, sm, done < unsigned(p.nodes) ? unsigned(p.nodes) - done : 0u);
+        if (bottom_up) {
+            if constexpr (MP) {  // predecessor labels: probes read a snapshot of the visited mask
+                snapshot_mask(p);
+                if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
             }
-            else ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
+            const unsigned done = dir.visited + ld_cg(&c->zmarked);
+            bu_level<THREADS, MP>(p, it, sm, done < unsigned(p.nodes) ? unsigned(p.nodes) - done : 0u);
         } else {
             ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
         }

@@ -37,6 +37,7 @@ struct BfsParams {
     const int *col;          // edges (+4 padding entries for 16-byte tail loads)
     int *labels;             // nodes: depth, or predecessor when mark_pred
     unsigned *mask;          // visited bitmask, bit (v & 31) of word v >> 5
+    unsigned *mask_snap;     // predecessor labels, bottom-up levels: copy of mask at the level's start
     int *queue[2];           // frontier ping-pong
     int *pred_queue[2];      // predecessor ping-pong (edge frontiers, mark_pred)
     int4 *chunks[2];         // CTA chunks of neighbour lists, ping-pong by phase: {start, len, pred, 0}

@@ -366,15 +366,18 @@ def test_direction_optimizing_skips_directed_graphs(cuda_device, oracle):
         assert not any(r["bottom_up"] for r in log)
 
 
-def test_direction_optimizing_with_predecessors_stays_top_down(cuda_device, oracle, rmat16):
+@pytest.mark.parametrize("alpha", [1, 14])
+def test_direction_optimizing_with_predecessors(cuda_device, oracle, rmat16, alpha):
+    """Predecessor labels: bottom-up levels probe a copy of the visited mask and
+    record the parent they find; every predecessor must be valid."""
     b = bfs_mod()
     g = rmat16
-    s = int(g.sample_sources(1, 23)[0])
-    ref, _ = oracle.bfs(g, s)
     prob = b.CsrProblem(True).from_graph(g)
-    preds, _, log = _ec_search(prob, g, s, 1)
-    assert oracle.check_predecessors(g, preds, ref)[0] == -1
-    assert not any(r["bottom_up"] for r in log)
+    for s in g.sample_sources(3, 23):
+        ref, _ = oracle.bfs(g, int(s))
+        preds, _, log = _ec_search(prob, g, s, alpha)
+        assert oracle.check_predecessors(g, preds, ref)[0] == -1
+        assert any(r["bottom_up"] for r in log)
 
 
 def test_direction_switch_arguments(cuda_device):
