@@ -526,52 +526,56 @@ template <int THREADS, bool MP>
 __device__ void ms_directions(const MsParams &p, int L, MsSmem<THREADS, MP> &sm) {
     __syncthreads();
     const unsigned char *in = p.alive + size_t(L & 3) * size_t(p.nslots);
-    const int per = (p.nslots + THREADS - 1) / THREADS;
-    const int s0 = min(p.nslots, int(threadIdx.x) * per), s1 = min(p.nslots, s0 + per);
-    unsigned mine = 0;
-    for (int s = s0; s < s1; s++) {
-        const size_t at = size_t(L & 3) * size_t(p.nslots) + size_t(s);
-        const size_t clr = size_t((L + 2) & 3) * size_t(p.nslots) + size_t(s);
-        p.nf[clr] = 0u;
-        p.mf[clr] = 0ull;
-        bool bottom_up = false;
-        if (!MP && p.state[s].active && in[s]) {
-            const MsSlot d = load_slot(p, s);
-            const MsGraph g = p.graphs[d.graph];
-            MsDir dr = p.dir[size_t((L + 1) & 1) * size_t(p.nslots) + size_t(s)];  // state after level L-1
-            const unsigned nf = p.nf[at];
-            const unsigned long long mf = p.mf[at];
-            dr.explored += mf;
-            dr.visited += nf;
-            if (g.symmetric) {
-                const unsigned long long total = (unsigned long long)g.edges;
-                const unsigned long long unexplored = total > dr.explored ? total - dr.explored : 0ull;
-                if (!dr.bottom_up) bottom_up = mf * p.do_alpha > unexplored;
-                else bottom_up = !((unsigned long long)nf * p.do_beta < (unsigned long long)d.nodes && nf < dr.prev_nf);
+    const MsDir *prev = p.dir + size_t((L + 1) & 1) * size_t(p.nslots);  // state after level L-1
+    MsDir *next = p.dir + size_t(L & 1) * size_t(p.nslots);
+    unsigned carry = 0;
+    // Rounds of THREADS consecutive slots (coalesced loads), each closed by a
+    // block-wide exclusive scan of the bottom-up steps.
+    for (int r0 = 0; r0 < p.nslots; r0 += THREADS) {
+        const int s = r0 + int(threadIdx.x);
+        unsigned steps = 0;
+        if (s < p.nslots) {
+            const size_t at = size_t(L & 3) * size_t(p.nslots) + size_t(s);
+            const size_t clr = size_t((L + 2) & 3) * size_t(p.nslots) + size_t(s);
+            const bool live = !MP && in[s] && p.state[s].active;
+            bool bottom_up = false;
+            if (live) {
+                MsDir dr = prev[s];
+                const unsigned nf = p.nf[at];
+                const unsigned long long mf = p.mf[at];
+                dr.explored += mf;
+                dr.visited += nf;
+                if (dr.symmetric) {
+                    const unsigned long long total = (unsigned long long)dr.edges;
+                    const unsigned long long unexplored = total > dr.explored ? total - dr.explored : 0ull;
+                    if (!dr.bottom_up) bottom_up = mf * p.do_alpha > unexplored;
+                    else bottom_up = !((unsigned long long)nf * p.do_beta < (unsigned long long)dr.nodes && nf < dr.prev_nf);
+                }
+                dr.prev_nf = nf;
+                dr.bottom_up = bottom_up ? 1 : 0;
+                next[s] = dr;
+                if (bottom_up) steps = ((unsigned(dr.nodes) + 31u) / 32u + 3u) / 4u;
             }
-            dr.prev_nf = nf;
-            dr.bottom_up = bottom_up ? 1 : 0;
-            p.dir[size_t(L & 1) * size_t(p.nslots) + size_t(s)] = dr;
-            if (bottom_up) mine += ((unsigned(d.nodes) + 31u) / 32u + 3u) / 4u;
+            p.nf[clr] = 0u;
+            p.mf[clr] = 0ull;
+            p.bu[s] = bottom_up ? 1 : 0;
         }
-        p.bu[s] = bottom_up ? 1 : 0;
-    }
-    // exclusive scan of the per-thread step counts, then the per-slot prefix
-    const unsigned incl = (unsigned)warp_inclusive_scan(int(mine));
-    if (lane_id() == 31) sm.warp_tot[threadIdx.x >> 5] = incl;
-    __syncthreads();
-    unsigned base = 0;
-    for (int w = 0; w < int(threadIdx.x >> 5); w++) base += sm.warp_tot[w];
-    unsigned run = base + incl - mine;
-    for (int s = s0; s < s1; s++) {
-        p.bu_prefix[s] = run;
-        if (p.bu[s]) {
-            const MsSlot d = load_slot(p, s);
-            run += ((unsigned(d.nodes) + 31u) / 32u + 3u) / 4u;
+        const unsigned incl = (unsigned)warp_inclusive_scan(int(steps));
+        if (lane_id() == 31) sm.warp_tot[threadIdx.x >> 5] = incl;
+        __syncthreads();
+        unsigned base = carry, round_total = 0;
+        for (int w = 0; w < THREADS / 32; w++) {
+            if (w < int(threadIdx.x >> 5)) base += sm.warp_tot[w];
+            round_total += sm.warp_tot[w];
         }
+        if (s < p.nslots) p.bu_prefix[s] = base + incl - steps;
+        carry += round_total;
+        __syncthreads();  // warp_tot is rewritten by the next round
     }
-    if (threadIdx.x == THREADS - 1) p.bu_prefix[p.nslots] = run;
-    if (threadIdx.x == 0) p.ctr->bu_steal[L & 3] = 0u;
+    if (threadIdx.x == 0) {
+        p.bu_prefix[p.nslots] = carry;
+        p.ctr->bu_steal[L & 3] = 0u;
+    }
     __syncthreads();
 }
 
@@ -698,6 +702,9 @@ __global__ void ms_admit_kernel(MsParams p, const int2 *slot_src, int count, int
     const int start = g.row[src], len = g.row[src + 1] - start;
     if (p.do_alpha) {
         MsDir dr = {};
+        dr.nodes = g.nodes;
+        dr.edges = g.edges;
+        dr.symmetric = g.symmetric;
         p.dir[slot] = dr;
         p.dir[size_t(p.nslots) + size_t(slot)] = dr;
         for (int q = 0; q < 4; q++) {

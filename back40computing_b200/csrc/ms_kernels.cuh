@@ -24,7 +24,9 @@ struct MsDir {
     unsigned visited;             // the slot's visited vertices
     unsigned prev_nf;             // its frontier size at the previous level
     int bottom_up;                // 1: the current level runs bottom-up
-    int pad;
+    int nodes;                    // the slot's graph, copied at admission so that the
+    int edges;                    //   per-level decision reads nothing but this record
+    int symmetric;                //   and the slot's counts
 };
 
 struct MsSlot {
