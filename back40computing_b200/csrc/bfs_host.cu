@@ -559,11 +559,16 @@ extern "C" int b40c_problem_from_host(b40c_problem_t *p, int stream_from_host, i
             CUDA_TRY(cudaMalloc(&p->d_row_offsets, sizeof(int) * (size_t(nodes) + 1)), "CsrProblem cudaMalloc d_row_offsets");
             p->row_cap = size_t(nodes) + 1;
         }
-        CUDA_TRY(cudaMemset(p->d_col + edges, 0, 4 * sizeof(int)), "cudaMemset column padding");
+        // The uploads are ordered on the problem's stream, ahead of the device
+        // CSR check below (a plain cudaMemcpy from pageable memory may return
+        // before its DMA lands, and the problem's stream does not wait for it).
+        cudaStream_t s = problem_stream(p);
+        CUDA_TRY(cudaMemsetAsync(p->d_col + edges, 0, 4 * sizeof(int), s), "cudaMemset column padding");
         if (edges)
-            CUDA_TRY(cudaMemcpy(p->d_col, h_col, sizeof(int) * size_t(edges), cudaMemcpyHostToDevice),
+            CUDA_TRY(cudaMemcpyAsync(p->d_col, h_col, sizeof(int) * size_t(edges), cudaMemcpyHostToDevice, s),
                      "CsrProblem cudaMemcpy d_column_indices");
-        CUDA_TRY(cudaMemcpy(p->d_row_offsets, h_row, sizeof(int) * (size_t(nodes) + 1), cudaMemcpyHostToDevice),
+        CUDA_TRY(cudaMemcpyAsync(p->d_row_offsets, h_row, sizeof(int) * (size_t(nodes) + 1), cudaMemcpyHostToDevice,
+                                 s),
                  "CsrProblem cudaMemcpy d_row_offsets");
     }
     if ((rc = device_check_csr(p, h_row, h_col))) {
