@@ -365,9 +365,11 @@ int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size,
     // The hybrid switches between its two bodies inside one persistent launch;
     // like the reference's EnactorHybrid it has a single way to run a search.
     if (variant == B40C_VARIANT_DEFAULT || e->strategy == B40C_HYBRID) variant = B40C_VARIANT_FUSED;
-    // Bottom-up levels: fused expand-contract on a symmetric graph; with
-    // predecessor labels they probe a copy of the visited mask.
-    if (e->strategy == B40C_EXPAND_CONTRACT && variant == B40C_VARIANT_FUSED && e->do_alpha) {
+    // Bottom-up levels: fused expand-contract on a symmetric graph held on the
+    // device (their scattered column reads would cross PCIe one entry at a time
+    // from a stream_from_host graph); with predecessor labels they probe a copy
+    // of the visited mask.
+    if (e->strategy == B40C_EXPAND_CONTRACT && variant == B40C_VARIANT_FUSED && e->do_alpha && !p->mapped) {
         if ((rc = ensure_symmetry_known(p))) return rc;
         if (p->symmetric == 1) {
             if (p->mark_pred && p->mask_snap_cap < p->mask_bytes) {

@@ -166,8 +166,9 @@ int b40c_enactor_level_log(b40c_enactor_t *enactor, int max_records, int64_t *t_
  * edges exceed the unvisited vertices' edges / alpha, and returns to top-down
  * once the frontier holds fewer than nodes / beta vertices and shrinks
  * (Beamer, Asanovic and Patterson, SC 2012).  Defaults alpha = 14, beta = 24;
- * alpha = 0 turns it off.  It applies to fused searches on symmetric graphs,
- * checked once per graph on the device; other searches stay top-down.  Depth
+ * alpha = 0 turns it off.  It applies to fused searches on symmetric graphs
+ * held on the device (not stream_from_host), checked once per graph; other
+ * searches stay top-down.  Depth
  * labels, search depth and total_queued are those of top-down; predecessor
  * labels are valid predecessors (bottom-up levels record the parent they
  * find). */
