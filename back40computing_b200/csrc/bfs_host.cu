@@ -76,6 +76,9 @@ struct b40c_problem {
     unsigned long long *d_sym = nullptr;   // 4 hash sums of the symmetry check
     unsigned *d_mask_snap = nullptr;       // predecessor-label bottom-up levels: visited-mask copy
     size_t mask_snap_cap = 0;
+    unsigned long long *d_heavy = nullptr;  // bottom-up levels: per vertex, its neighbour of highest degree
+    size_t heavy_cap = 0;
+    bool heavy_ready = false;               // d_heavy holds the current graph's keys
 };
 
 struct b40c_enactor {
@@ -161,6 +164,10 @@ void free_problem_device(b40c_problem *p) {
     cudaFree(p->d_mask_snap);
     p->d_mask_snap = nullptr;
     p->mask_snap_cap = 0;
+    cudaFree(p->d_heavy);
+    p->d_heavy = nullptr;
+    p->heavy_cap = 0;
+    p->heavy_ready = false;
 }
 
 // Whether every entry v of row u has an entry u in row v (a symmetric,
@@ -178,6 +185,29 @@ int ensure_symmetry_known(b40c_problem *p) {
     CUDA_TRY(cudaMemcpyAsync(h, p->d_sym, sizeof(h), cudaMemcpyDeviceToHost, s), "symmetry sums copy");
     CUDA_TRY(cudaStreamSynchronize(s), "symmetry check");
     p->symmetric = (h[0] == h[1] && h[2] == h[3]) ? 1 : 0;
+    return B40C_SUCCESS;
+}
+
+// Per vertex, its neighbour of highest degree (launch_heavy_neighbour), which
+// bottom-up levels probe before reading a list.  Built once per graph on the
+// problem's stream, with a host wait, like the symmetry check.
+int ensure_heavy_known(b40c_problem *p) {
+    if (p->heavy_ready) return B40C_SUCCESS;
+    cudaStream_t s = problem_stream(p);
+    if (p->heavy_cap < size_t(p->nodes)) {
+        cudaFree(p->d_heavy);
+        p->d_heavy = nullptr;
+        p->heavy_cap = 0;
+        CUDA_TRY(cudaMalloc(&p->d_heavy, sizeof(unsigned long long) * size_t(p->nodes)),
+                 "cudaMalloc heaviest-neighbour keys");
+        p->heavy_cap = size_t(p->nodes);
+    }
+    CUDA_TRY(cudaMemsetAsync(p->d_heavy, 0, sizeof(unsigned long long) * size_t(p->nodes), s),
+             "heaviest-neighbour keys clear");
+    CUDA_TRY(launch_heavy_neighbour(p->d_row_offsets, p->d_col, int(p->nodes), p->edges, p->d_heavy, s),
+             "heaviest-neighbour launch");
+    CUDA_TRY(cudaStreamSynchronize(s), "heaviest-neighbour keys");
+    p->heavy_ready = true;
     return B40C_SUCCESS;
 }
 
@@ -379,7 +409,9 @@ int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size,
                 CUDA_TRY(cudaMalloc(&p->d_mask_snap, p->mask_bytes), "cudaMalloc visited-mask copy");
                 p->mask_snap_cap = p->mask_bytes;
             }
+            if ((rc = ensure_heavy_known(p))) return rc;
             bp.mask_snap = p->d_mask_snap;
+            bp.heavy = p->d_heavy;
             bp.do_alpha = e->do_alpha;
             bp.do_beta = e->do_beta;
         }
@@ -542,6 +574,7 @@ extern "C" int b40c_problem_from_host(b40c_problem_t *p, int stream_from_host, i
     p->edges = edges;
     p->reset_once = false;
     p->symmetric = -1;
+    p->heavy_ready = false;
     if (p->mapped) {
         if ((rc = map_host(p, h_row, sizeof(int) * (size_t(nodes) + 1), (void **)&p->d_row_offsets))) return rc;
         if ((rc = map_host(p, h_col, sizeof(int) * size_t(edges), (void **)&p->d_col))) return rc;

@@ -628,9 +628,10 @@ __device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, u
 // makes it a depth-(it+1) vertex.
 //
 // A warp takes BU_WORDS consecutive mask words per step; lane j owns vertex
-// 32w + j of each word w and scans its list BU_PROBE entries per round until a
-// parent turns up; rounds are software-pipelined (the entries of round k+1 are
-// loaded before round k's probes are tested).  A word has one writer in the
+// 32w + j of each word w, probes its heaviest neighbour first (from a dense
+// per-vertex array) and, when that is not a parent, scans its list BU_PROBE
+// entries per round until a parent turns up; rounds are software-pipelined
+// (the entries of round k+1 are loaded before round k's probes are tested).  A word has one writer in the
 // level, so its new bits are a plain store.  Vertices without edges are
 // marked visited but never labelled: on a symmetric graph no list leads to
 // them, and later bottom-up levels skip them.  The discovered vertices are
@@ -657,68 +658,122 @@ __device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0,
     int v[BU_WORDS], st[BU_WORDS], ln[BU_WORDS];
     int par[MP ? BU_WORDS : 1];  // predecessor labels: the parent found
     unsigned open = 0, scan = 0, found = 0;
+    // Every load of a phase is issued before any result is tested, and a lane
+    // without work reads entry 0 (a line the whole warp shares) instead of
+    // branching around its load: a load behind a branch, or behind a possible
+    // atomic, would wait for the one before it, and the rounds are bound by
+    // memory latency.
+    int r0[BU_WORDS], r1[BU_WORDS];
+    unsigned long long hk[BU_WORDS];  // heaviest neighbour: (degree << 32) | id, 0 = none
 #pragma unroll
     for (int j = 0; j < BU_WORDS; j++) {
         v[j] = int((w0 + j) * 32u) + lane;
-        st[j] = 0;
-        ln[j] = 0;
-        if (v[j] < p.nodes && !((mw[j] >> lane) & 1u)) {
-            open |= 1u << j;
-            row_range(p, v[j], st[j], ln[j]);
-        }
+        if (v[j] < p.nodes && !((mw[j] >> lane) & 1u)) open |= 1u << j;
+        const int vv = ((open >> j) & 1u) ? v[j] : 0;
+        r0[j] = __ldg(p.row_offsets + vv);
+        r1[j] = __ldg(p.row_offsets + vv + 1);
+        hk[j] = p.heavy ? __ldg(p.heavy + vv) : 0ull;
     }
 #pragma unroll
-    for (int j = 0; j < BU_WORDS; j++)
-        if (((open >> j) & 1u) && ln[j] > 0) scan |= 1u << j;
+    for (int j = 0; j < BU_WORDS; j++) {
+        st[j] = r0[j];
+        ln[j] = ((open >> j) & 1u) ? r1[j] - r0[j] : 0;
+    }
     // Probes are ordinary (L1-cached) label loads: the depth-it labels they
     // look for were written before the level's grid barrier, whose
     // release/acquire orders them before these loads; labels written during
-    // this level are it+1 and never match.
-    int u[BU_WORDS][BU_PROBE];
-#pragma unroll
-    for (int j = 0; j < BU_WORDS; j++)
-#pragma unroll
-        for (int e = 0; e < BU_PROBE; e++)
-            u[j][e] = ((scan >> j) & 1u) && e < ln[j] ? __ldg(p.col + st[j] + e) : -1;
-    for (int k = 0; __any_sync(FULL, scan != 0u); k += BU_PROBE) {
-        int un[BU_WORDS][BU_PROBE];
-#pragma unroll
-        for (int j = 0; j < BU_WORDS; j++)
-#pragma unroll
-            for (int e = 0; e < BU_PROBE; e++) {
-                const int kk = k + BU_PROBE + e;
-                un[j][e] = ((scan >> j) & 1u) && kk < ln[j] ? __ldg(p.col + st[j] + kk) : -1;
-            }
+    // this level are it+1 and never match.  With predecessor labels the probe
+    // reads the snapshot of the visited mask taken at the level's start: a
+    // visited neighbour of an unvisited vertex has depth exactly it
+    // (symmetric graph).
+    //
+    // First each vertex probes its heaviest neighbour, read from a dense
+    // per-vertex array (coalesced); only the vertices it does not settle read
+    // their list, whose first entry is a scattered DRAM access.
+    {
+        unsigned hact = 0;
+        int hp[BU_WORDS];
 #pragma unroll
         for (int j = 0; j < BU_WORDS; j++) {
+            const unsigned x = unsigned(hk[j]);
+            const bool a = ((open >> j) & 1u) && ln[j] > 0 && hk[j] != 0ull && x < (unsigned)p.nodes;
+            if (a) hact |= 1u << j;
+            const unsigned xs = a ? x : 0u;
+            if constexpr (MP) hp[j] = int(__ldca(p.mask_snap + (xs >> 5)));
+            else hp[j] = __ldca(p.labels + xs);
+        }
 #pragma unroll
-            for (int e = 0; e < BU_PROBE; e++) {
-                if (((scan >> j) & 1u) && k + e < ln[j]) {
-                    const unsigned x = (unsigned)u[j][e];
-                    if (x < (unsigned)p.nodes) {
-                        if constexpr (MP) {
-                            // labels hold predecessors: the probe reads the
-                            // snapshot of the visited mask taken at the level's
-                            // start; a visited neighbour of an unvisited vertex
-                            // has depth exactly it (symmetric graph).
-                            if (!((found >> j) & 1u) && ((__ldca(p.mask_snap + (x >> 5)) >> (x & 31u)) & 1u)) {
-                                found |= 1u << j;
-                                par[j] = int(x);
-                            }
-                        } else {
-                            if (__ldca(p.labels + x) == it) found |= 1u << j;
-                        }
-                    } else {
-                        atomicOr(&c->error, ERR_BAD_VERTEX);
+        for (int j = 0; j < BU_WORDS; j++) {
+            if ((hact >> j) & 1u) {
+                const unsigned x = unsigned(hk[j]);
+                if constexpr (MP) {
+                    if (((unsigned)hp[j] >> (x & 31u)) & 1u) {
+                        found |= 1u << j;
+                        par[j] = int(x);
                     }
+                } else {
+                    if (hp[j] == it) found |= 1u << j;
                 }
             }
-            if (((found >> j) & 1u) || k + BU_PROBE >= ln[j]) scan &= ~(1u << j);
+            // a list of one entry was settled by the probe of that entry
+            if (((open >> j) & 1u) && !((found >> j) & 1u) && ln[j] > int((hact >> j) & 1u)) scan |= 1u << j;
         }
+    }
+    // Entry 0 of the column array exists whenever some lane has a list to scan.
+    if (__any_sync(FULL, scan != 0u)) {
+        int u[BU_WORDS][BU_PROBE];
 #pragma unroll
         for (int j = 0; j < BU_WORDS; j++)
 #pragma unroll
-            for (int e = 0; e < BU_PROBE; e++) u[j][e] = un[j][e];
+            for (int e = 0; e < BU_PROBE; e++)
+                u[j][e] = __ldg(p.col + (((scan >> j) & 1u) && e < ln[j] ? st[j] + e : 0));
+        for (int k = 0; __any_sync(FULL, scan != 0u); k += BU_PROBE) {
+            int un[BU_WORDS][BU_PROBE];
+#pragma unroll
+            for (int j = 0; j < BU_WORDS; j++)
+#pragma unroll
+                for (int e = 0; e < BU_PROBE; e++) {
+                    const int kk = k + BU_PROBE + e;
+                    un[j][e] = __ldg(p.col + (((scan >> j) & 1u) && kk < ln[j] ? st[j] + kk : 0));
+                }
+            unsigned act = 0, bad = 0;  // bit j * BU_PROBE + e: entry e of list j probed / out of range
+            int pb[BU_WORDS][BU_PROBE];
+#pragma unroll
+            for (int j = 0; j < BU_WORDS; j++)
+#pragma unroll
+                for (int e = 0; e < BU_PROBE; e++) {
+                    const unsigned x = (unsigned)u[j][e];
+                    const bool a = ((scan >> j) & 1u) && k + e < ln[j];
+                    const bool ok = a && x < (unsigned)p.nodes;
+                    if (ok) act |= 1u << (j * BU_PROBE + e);
+                    if (a && !ok) bad = 1u;
+                    const unsigned xs = ok ? x : 0u;
+                    if constexpr (MP) pb[j][e] = int(__ldca(p.mask_snap + (xs >> 5)));
+                    else pb[j][e] = __ldca(p.labels + xs);
+                }
+#pragma unroll
+            for (int j = 0; j < BU_WORDS; j++) {
+#pragma unroll
+                for (int e = 0; e < BU_PROBE; e++) {
+                    if (!((act >> (j * BU_PROBE + e)) & 1u) || ((found >> j) & 1u)) continue;
+                    const unsigned x = (unsigned)u[j][e];
+                    if constexpr (MP) {
+                        if (((unsigned)pb[j][e] >> (x & 31u)) & 1u) {
+                            found |= 1u << j;
+                            par[j] = int(x);
+                        }
+                    } else {
+                        if (pb[j][e] == it) found |= 1u << j;
+                    }
+                }
+                if (((found >> j) & 1u) || k + BU_PROBE >= ln[j]) scan &= ~(1u << j);
+            }
+            if (bad) atomicOr(&c->error, ERR_BAD_VERTEX);
+#pragma unroll
+            for (int j = 0; j < BU_WORDS; j++)
+#pragma unroll
+                for (int e = 0; e < BU_PROBE; e++) u[j][e] = un[j][e];
+        }
     }
     int nfound = 0;
     long long dfound = 0;
@@ -1326,6 +1381,61 @@ __global__ void symmetry_hash_kernel(const int *row_offsets, const int *col, int
         for (int j = 0; j < 4; j++) atomicAdd(sums + j, h[j]);
 }
 
+// keys[v] = the largest (deg(u) << 32) | u over the entries u of row v: its
+// neighbour of highest degree, which bottom-up levels probe before reading the
+// list (the highest-degree vertices are reached first, so on graphs with a
+// skewed degree distribution that one neighbour is nearly always the parent
+// when there is one).  Runs of HEAVY_RUN entries per lane, found and walked
+// as in the symmetry check; a lane folds each row's best key into keys[row]
+// with one atomicMax per row it touches, so a hub's list costs one atomic per
+// run.  Out-of-range entries are skipped (the CSR check rejects them first).
+constexpr int HEAVY_RUN = 64;
+
+__global__ void heavy_neighbour_kernel(const int *row_offsets, const int *col, int nodes, long long edges,
+                                       unsigned long long *keys) {
+    const long long W = grid_warps();
+    for (long long c = global_warp(); c * 32 * HEAVY_RUN < edges; c += W) {
+        const long long k0 = (c * 32 + lane_id()) * HEAVY_RUN;
+        if (k0 >= edges) continue;
+        const long long k1 = min(edges, k0 + HEAVY_RUN);
+        int lo = 0, hi = nodes;  // last row lo with row_offsets[lo] <= k0
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(row_offsets + mid) <= k0) lo = mid;
+            else hi = mid;
+        }
+        int r = lo;
+        long long next = __ldg(row_offsets + r + 1);
+        unsigned long long best = 0;
+        for (long long k = k0; k < k1; k += 4) {
+            int u[4], d0[4], d1[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) u[j] = k + j < k1 ? __ldg(col + k + j) : -1;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int uu = (unsigned)u[j] < (unsigned)nodes ? u[j] : 0;
+                d0[j] = __ldg(row_offsets + uu);
+                d1[j] = __ldg(row_offsets + uu + 1);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (k + j >= k1) break;
+                while (k + j >= next) {  // entry k + j belongs to a later row
+                    if (best) atomicMax(keys + r, best);
+                    best = 0;
+                    next = __ldg(row_offsets + (++r) + 1);
+                }
+                if ((unsigned)u[j] < (unsigned)nodes) {
+                    const unsigned long long key =
+                        ((unsigned long long)(unsigned)(d1[j] - d0[j]) << 32) | (unsigned)u[j];
+                    best = key > best ? key : best;
+                }
+            }
+        }
+        if (best) atomicMax(keys + r, best);
+    }
+}
+
 // CSR checks on the device: out[0] = the first row v whose offsets decrease
 // (row[v+1] < row[v]), out[1] = the first entry outside [0, nodes); both stay
 // ~0 when there is none (out must start at ~0).
@@ -1466,6 +1576,16 @@ cudaError_t launch_symmetry_hash(const int *row_offsets, const int *col, int nod
     if (!e) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e) return e;
     symmetry_hash_kernel<<<sms * 8, 256, 0, stream>>>(row_offsets, col, nodes, edges, sums);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_heavy_neighbour(const int *row_offsets, const int *col, int nodes, long long edges,
+                                   unsigned long long *keys, cudaStream_t stream) {
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (!e) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e) return e;
+    heavy_neighbour_kernel<<<sms * 8, 256, 0, stream>>>(row_offsets, col, nodes, edges, keys);
     return cudaGetLastError();
 }
 

@@ -64,6 +64,9 @@ struct BfsParams {
     unsigned do_alpha;
     unsigned do_beta;
     long long edges;  // CSR entries (for the unvisited-edge count)
+    // Bottom-up levels: per vertex, its neighbour of highest degree as
+    // (degree << 32) | id (0: no neighbours); probed before the list is read.
+    const unsigned long long *heavy;
     // INSTRUMENT: per CTA of a fused kernel, the %globaltimer ns it spent in
     // level work (barrier waits excluded), written at the kernel's end; NULL: off.
     unsigned long long *cta_busy;
@@ -92,6 +95,11 @@ cudaError_t level_grid_limit(const KernelConfig &kc, int *grid);
 // start at zero.
 cudaError_t launch_symmetry_hash(const int *row_offsets, const int *col, int nodes, long long edges,
                                  unsigned long long *sums, cudaStream_t stream);
+// Per vertex v, the neighbour u of highest degree as (deg(u) << 32) | u (the
+// largest key, so ties go to the larger id); 0 for a vertex without
+// neighbours.  keys[0..nodes) must start at zero.
+cudaError_t launch_heavy_neighbour(const int *row_offsets, const int *col, int nodes, long long edges,
+                                   unsigned long long *keys, cudaStream_t stream);
 // CSR validity on the device: out[0] = first row whose offsets decrease,
 // out[1] = first column entry outside [0, nodes); ~0 when none.  out[0..1]
 // must start at ~0.

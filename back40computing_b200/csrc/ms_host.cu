@@ -47,6 +47,7 @@ struct GraphRes {
     int nodes = 0;
     long long edges = 0;
     int symmetric = 0;
+    unsigned long long *d_heavy = nullptr;  // symmetric graphs: heaviest neighbour per vertex
 };
 
 }  // namespace
@@ -202,6 +203,7 @@ extern "C" int b40c_batch_destroy(b40c_batch_t *b) {
     for (auto &g : b->graphs) {
         cudaFree(g.d_row);
         cudaFree(g.d_col);
+        cudaFree(g.d_heavy);
     }
     cudaFree(b->d_graphs);
     cudaFree(b->d_slots);
@@ -255,12 +257,15 @@ extern "C" int b40c_batch_add_graph(b40c_batch_t *b, int nodes, int edges, const
     CUDA_TRY(cudaMemset(g.d_col + edges, 0, 4 * sizeof(int)), "column padding");
     if (edges) CUDA_TRY(cudaMemcpy(g.d_col, h_col, sizeof(int) * size_t(edges), cudaMemcpyHostToDevice), "upload");
     CUDA_TRY(ms_graph_symmetric(g.d_row, g.d_col, nodes, edges, &g.symmetric), "graph symmetry check");
+    if (g.symmetric)
+        CUDA_TRY(ms_graph_heavy(g.d_row, g.d_col, nodes, edges, &g.d_heavy), "heaviest-neighbour keys");
     b->graphs.push_back(g);
     // Refresh the device graph table.
     std::vector<MsGraph> table(b->graphs.size());
     for (size_t i = 0; i < b->graphs.size(); i++)
         table[i] = MsGraph{b->graphs[i].d_row, b->graphs[i].d_col, b->graphs[i].nodes,
-                           int(b->graphs[i].edges + 4), int(b->graphs[i].edges), b->graphs[i].symmetric};
+                           int(b->graphs[i].edges + 4), int(b->graphs[i].edges), b->graphs[i].symmetric,
+                           b->graphs[i].d_heavy};
     int rc = grow(&b->d_graphs, &b->graphs_cap, table.size(), "batch graph table");
     if (rc) return rc;
     CUDA_TRY(cudaMemcpy(b->d_graphs, table.data(), sizeof(MsGraph) * table.size(), cudaMemcpyHostToDevice),

@@ -393,8 +393,9 @@ __device__ void ms_level(const MsParams &p, int L, unsigned nq_in, unsigned nch,
 // Bottom-up step of slot s (direction-optimizing BFS, Beamer, Asanovic and
 // Patterson, SC 2012; the single-search bu_step of bfs_kernels.cu with slot
 // offsets): mask words w0 .. w0+3 of the slot; lane j owns vertex 32w + j of
-// each word and scans its list 2 entries per round, software-pipelined, for a
-// neighbour at the slot's depth L - start_level.  Label probes are ordinary
+// each word, probes its heaviest neighbour and, when that is not a parent,
+// scans its list 2 entries per round, software-pipelined, for a neighbour at
+// the slot's depth L - start_level.  Label probes are ordinary
 // (L1-cached) loads, ordered after the labels they look for by the grid
 // barriers before the level.  A word has one writer in the level.
 template <int THREADS, bool MP>
@@ -412,17 +413,36 @@ __device__ __forceinline__ void ms_bu_step(const MsParams &p, int L, int s, unsi
     if (mw[0] == FULL && mw[1] == FULL && mw[2] == FULL && mw[3] == FULL) return;  // warp-uniform
     int v[4], st[4], ln[4];
     unsigned open = 0, scan = 0, found = 0;
+    // Row offsets and the heaviest neighbour of every open vertex, loaded
+    // together (a closed lane reads entry 0); the heaviest neighbour is probed
+    // first, and only the vertices it does not settle read their list.
+    int r0[4], r1[4];
+    unsigned long long hk[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         v[j] = int((w0 + j) * 32u) + lane;
-        st[j] = 0;
-        ln[j] = 0;
-        if (v[j] < d.nodes && !((mw[j] >> lane) & 1u)) {
-            open |= 1u << j;
-            st[j] = __ldg(g.row + v[j]);
-            ln[j] = __ldg(g.row + v[j] + 1) - st[j];
-            if (ln[j] > 0) scan |= 1u << j;
-        }
+        if (v[j] < d.nodes && !((mw[j] >> lane) & 1u)) open |= 1u << j;
+        const int vv = ((open >> j) & 1u) ? v[j] : 0;
+        r0[j] = __ldg(g.row + vv);
+        r1[j] = __ldg(g.row + vv + 1);
+        hk[j] = g.heavy ? __ldg(g.heavy + vv) : 0ull;
+    }
+    unsigned hact = 0;
+    int hp[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        st[j] = r0[j];
+        ln[j] = ((open >> j) & 1u) ? r1[j] - r0[j] : 0;
+        const unsigned x = unsigned(hk[j]);
+        const bool a = ((open >> j) & 1u) && ln[j] > 0 && hk[j] != 0ull && x < (unsigned)d.nodes;
+        if (a) hact |= 1u << j;
+        hp[j] = __ldca(labels + (a ? x : 0u));
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (((hact >> j) & 1u) && hp[j] == depth) found |= 1u << j;
+        // a list of one entry was settled by the probe of that entry
+        if (((open >> j) & 1u) && !((found >> j) & 1u) && ln[j] > int((hact >> j) & 1u)) scan |= 1u << j;
     }
     int u[4][2];
 #pragma unroll
@@ -774,6 +794,22 @@ cudaError_t ms_graph_symmetric(const int *d_row, const int *d_col, int nodes, lo
     cudaFree(d);
     if (!e) *symmetric = (h[0] == h[1] && h[2] == h[3]) ? 1 : 0;
     return e;
+}
+
+cudaError_t ms_graph_heavy(const int *d_row, const int *d_col, int nodes, long long edges, unsigned long long **keys) {
+    *keys = nullptr;
+    if (nodes <= 0) return cudaSuccess;
+    unsigned long long *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(unsigned long long) * size_t(nodes));
+    if (!e) e = cudaMemset(d, 0, sizeof(unsigned long long) * size_t(nodes));
+    if (!e) e = launch_heavy_neighbour(d_row, d_col, nodes, edges, d, 0);
+    if (!e) e = cudaStreamSynchronize(0);
+    if (e) {
+        cudaFree(d);
+        return e;
+    }
+    *keys = d;
+    return cudaSuccess;
 }
 
 cudaError_t ms_grid_limit(const MsKernelConfig &kc, int *grid) {

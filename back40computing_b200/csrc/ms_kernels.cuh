@@ -15,6 +15,9 @@ struct MsGraph {
     int vec_end;     // 16-byte column loads are safe below this index
     int edges;
     int symmetric;   // 1: every entry has its reverse (bottom-up levels allowed)
+    // symmetric graphs: per vertex, its neighbour of highest degree as
+    // (degree << 32) | id (0: none), probed by bottom-up levels first
+    const unsigned long long *heavy;
 };
 
 // Direction-optimizing state of one search slot, updated at the start of
@@ -91,6 +94,9 @@ struct MsKernelConfig {
 // Whether a resident graph is symmetric (the hash check of
 // launch_symmetry_hash; allocates and frees a 32-byte buffer, waits).
 cudaError_t ms_graph_symmetric(const int *d_row, const int *d_col, int nodes, long long edges, int *symmetric);
+// Allocates and fills the heaviest-neighbour keys of a resident graph
+// (launch_heavy_neighbour), waiting for them; *keys = nullptr when nodes == 0.
+cudaError_t ms_graph_heavy(const int *d_row, const int *d_col, int nodes, long long edges, unsigned long long **keys);
 // Largest co-resident grid of the multi-search kernel.
 cudaError_t ms_grid_limit(const MsKernelConfig &kc, int *grid);
 // Cooperative launch: runs levels from Counters::cur_it until no search has

@@ -90,6 +90,7 @@ struct ResidentGraph {
     int nodes = 0;
     long long edges = 0;
     int symmetric = 0;
+    unsigned long long *d_heavy = nullptr;  // symmetric graphs: heaviest neighbour per vertex
 };
 
 struct SlotUse {
@@ -276,6 +277,7 @@ extern "C" int b40c_server_destroy(b40c_server_t *s) {
     for (auto &g : s->graphs) {
         cudaFree(g.d_row);
         cudaFree(g.d_col);
+        cudaFree(g.d_heavy);
     }
     cudaFree(s->d_graphs);
     cudaFree(s->d_slots);
@@ -328,11 +330,13 @@ extern "C" int b40c_server_add_graph(b40c_server_t *s, int nodes, int edges, con
     CUDA_TRY(cudaMemset(g.d_col + edges, 0, 4 * sizeof(int)), "column padding");
     if (edges) CUDA_TRY(cudaMemcpy(g.d_col, h_col, sizeof(int) * size_t(edges), cudaMemcpyHostToDevice), "upload");
     CUDA_TRY(ms_graph_symmetric(g.d_row, g.d_col, nodes, edges, &g.symmetric), "graph symmetry check");
+    if (g.symmetric)
+        CUDA_TRY(ms_graph_heavy(g.d_row, g.d_col, nodes, edges, &g.d_heavy), "heaviest-neighbour keys");
     s->graphs.push_back(g);
     std::vector<MsGraph> table(s->graphs.size());
     for (size_t i = 0; i < s->graphs.size(); i++)
         table[i] = MsGraph{s->graphs[i].d_row, s->graphs[i].d_col, s->graphs[i].nodes, int(s->graphs[i].edges + 4),
-                           int(s->graphs[i].edges), s->graphs[i].symmetric};
+                           int(s->graphs[i].edges), s->graphs[i].symmetric, s->graphs[i].d_heavy};
     cudaFree(s->d_graphs);
     s->d_graphs = nullptr;
     CUDA_TRY(cudaMalloc(&s->d_graphs, sizeof(MsGraph) * table.size()), "server graph table");

@@ -354,6 +354,33 @@ def test_direction_optimizing_low_alpha_runs_most_levels_bottom_up(cuda_device, 
         assert any(r["bottom_up"] for r in en.level_log())
 
 
+@pytest.mark.parametrize("mark_pred", [False, True])
+def test_direction_optimizing_after_reupload(cuda_device, oracle, mark_pred):
+    """Bottom-up levels probe each vertex's heaviest neighbour, kept per graph:
+    after FromHostProblem uploads another graph of the same size into the same
+    problem, searches still match the oracle (a stale table would name
+    non-neighbours).  grid2d has equal degrees, so its heaviest neighbour is
+    often not a parent and the lists are scanned."""
+    b = bfs_mod()
+    graphs = [b.rmat(14, 8, seed=31), b.rmat(14, 8, seed=32), b.grid2d(128)]
+    prob = b.CsrProblem(mark_pred)
+    en = b.EnactorExpandContract()
+    en.set_direction_optimizing(1, 1)
+    en.set_level_log(True)
+    for gi, g in enumerate(graphs):
+        prob.from_graph(g)
+        for s in g.sample_sources(2, 23):
+            ref, _ = oracle.bfs(g, int(s))
+            b.check(prob.Reset(en.GetFrontierType(), 1.0))
+            b.check(en.EnactSearch(prob, int(s)))
+            if mark_pred:
+                assert oracle.check_predecessors(g, prob.labels(), ref)[0] == -1
+            else:
+                assert oracle.first_mismatch(prob.labels(), ref) == -1
+            if gi < 2:
+                assert any(r["bottom_up"] for r in en.level_log())
+
+
 def test_direction_optimizing_skips_directed_graphs(cuda_device, oracle):
     """A directed graph fails the symmetry check and is searched top-down only."""
     b = bfs_mod()
