@@ -61,6 +61,7 @@ struct WarpSmem {
     unsigned nbuf;
     unsigned disc_n;             // direction-optimizing counts of this warp's discoveries
     unsigned long long disc_m;   // in the current level, added to the counters at its end
+    unsigned bfound[4];          // bottom-up window scans: vertex 32j + lane found a parent
 };
 
 template <int THREADS, bool MP>
@@ -628,18 +629,17 @@ __device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, u
 // makes it a depth-(it+1) vertex.
 //
 // A warp takes BU_WORDS consecutive mask words per step; lane j owns vertex
-// 32w + j of each word w, probes its heaviest neighbour first (from a dense
-// per-vertex array) and, when that is not a parent, scans its list BU_PROBE
-// entries per round until a parent turns up; rounds are software-pipelined
-// (the entries of round k+1 are loaded before round k's probes are tested).  A word has one writer in the
-// level, so its new bits are a plain store.  Vertices without edges are
+// 32w + j of each word w and probes its heaviest neighbour first (from a
+// dense per-vertex array); the lists of the vertices that probe does not
+// settle are then scanned by the whole warp, a window of entries at a time,
+// until each finds a parent or ends.  A word has one writer in the level, so
+// its new bits are a plain store.  Vertices without edges are
 // marked visited but never labelled: on a symmetric graph no list leads to
 // them, and later bottom-up levels skip them.  The discovered vertices are
 // counted and placed for level it+1 exactly as top-down discovery places
 // them, so either direction can run next.  With predecessor labels the
 // probe tests a snapshot of the visited mask instead (see bu_step).
 constexpr int BU_WORDS = 4;  // = the 4 lists per lane that place4 and stage4 take
-constexpr int BU_PROBE = 2;
 static_assert(BU_WORDS == 4, "bottom-up steps hand 4 vertices per lane to place4 / stage4");
 
 // One bottom-up step: visited-mask words w0 .. w0 + BU_WORDS - 1.
@@ -719,61 +719,82 @@ __device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0,
             if (((open >> j) & 1u) && !((found >> j) & 1u) && ln[j] > int((hact >> j) & 1u)) scan |= 1u << j;
         }
     }
-    // Entry 0 of the column array exists whenever some lane has a list to scan.
+    // The lists the heaviest neighbour did not settle are scanned by the whole
+    // warp in windows of WINDOW entries (4 per lane): every unsettled vertex
+    // puts its next entries, in vertex order, into the warp's window, so
+    // consecutive lanes read consecutive column entries (coalesced loads) and
+    // a window's probes all go out at once.  A vertex whose parent turns up
+    // takes no further entries.  A step then costs about one window (one
+    // column load and one probe in sequence) instead of a round per pair of
+    // entries of its longest list.  Entry 0 of the column array exists
+    // whenever some lane has a list to scan.
     if (__any_sync(FULL, scan != 0u)) {
-        int u[BU_WORDS][BU_PROBE];
-#pragma unroll
-        for (int j = 0; j < BU_WORDS; j++)
-#pragma unroll
-            for (int e = 0; e < BU_PROBE; e++)
-                u[j][e] = __ldg(p.col + (((scan >> j) & 1u) && e < ln[j] ? st[j] + e : 0));
-        for (int k = 0; __any_sync(FULL, scan != 0u); k += BU_PROBE) {
-            int un[BU_WORDS][BU_PROBE];
-#pragma unroll
-            for (int j = 0; j < BU_WORDS; j++)
-#pragma unroll
-                for (int e = 0; e < BU_PROBE; e++) {
-                    const int kk = k + BU_PROBE + e;
-                    un[j][e] = __ldg(p.col + (((scan >> j) & 1u) && kk < ln[j] ? st[j] + kk : 0));
-                }
-            unsigned act = 0, bad = 0;  // bit j * BU_PROBE + e: entry e of list j probed / out of range
-            int pb[BU_WORDS][BU_PROBE];
-#pragma unroll
-            for (int j = 0; j < BU_WORDS; j++)
-#pragma unroll
-                for (int e = 0; e < BU_PROBE; e++) {
-                    const unsigned x = (unsigned)u[j][e];
-                    const bool a = ((scan >> j) & 1u) && k + e < ln[j];
-                    const bool ok = a && x < (unsigned)p.nodes;
-                    if (ok) act |= 1u << (j * BU_PROBE + e);
-                    if (a && !ok) bad = 1u;
-                    const unsigned xs = ok ? x : 0u;
-                    if constexpr (MP) pb[j][e] = int(__ldca(p.mask_snap + (xs >> 5)));
-                    else pb[j][e] = __ldca(p.labels + xs);
-                }
+        int done[BU_WORDS] = {0, 0, 0, 0};
+        unsigned bad = 0;
+        if (lane < BU_WORDS) ws.bfound[lane] = 0u;
+        __syncwarp();
+        for (;;) {
+            int excl[BU_WORDS], rem[BU_WORDS], total = 0;
 #pragma unroll
             for (int j = 0; j < BU_WORDS; j++) {
-#pragma unroll
-                for (int e = 0; e < BU_PROBE; e++) {
-                    if (!((act >> (j * BU_PROBE + e)) & 1u) || ((found >> j) & 1u)) continue;
-                    const unsigned x = (unsigned)u[j][e];
-                    if constexpr (MP) {
-                        if (((unsigned)pb[j][e] >> (x & 31u)) & 1u) {
-                            found |= 1u << j;
-                            par[j] = int(x);
-                        }
-                    } else {
-                        if (pb[j][e] == it) found |= 1u << j;
-                    }
-                }
-                if (((found >> j) & 1u) || k + BU_PROBE >= ln[j]) scan &= ~(1u << j);
+                // at most a window's worth per vertex counts, so sums stay small
+                rem[j] = ((scan >> j) & 1u) ? min(ln[j] - done[j], WINDOW) : 0;
+                const int incl = warp_inclusive_scan(rem[j]);
+                excl[j] = total + incl - rem[j];
+                total += __shfl_sync(FULL, incl, 31);
             }
-            if (bad) atomicOr(&c->error, ERR_BAD_VERTEX);
+            if (total == 0) break;  // warp-uniform
 #pragma unroll
-            for (int j = 0; j < BU_WORDS; j++)
+            for (int j = 0; j < BU_WORDS; j++) {
+                const int hi = min(excl[j] + rem[j], WINDOW);
+                for (int i = excl[j]; i < hi; i++) {
+                    ws.gofs[i] = st[j] + done[j] + (i - excl[j]);
+                    ws.surv[i] = j * 32 + lane;
+                }
+                done[j] += max(0, hi - excl[j]);
+            }
+            __syncwarp();
+            const int cw = min(WINDOW, total);
+            int x[4], own[4], pb[4];
 #pragma unroll
-                for (int e = 0; e < BU_PROBE; e++) u[j][e] = un[j][e];
+            for (int m = 0; m < 4; m++) {
+                const int idx = m * 32 + lane;
+                x[m] = __ldg(p.col + (idx < cw ? ws.gofs[idx] : 0));
+                own[m] = idx < cw ? ws.surv[idx] : -1;
+            }
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                const bool a = own[m] >= 0 && (unsigned)x[m] < (unsigned)p.nodes;
+                if (own[m] >= 0 && !a) bad = 1u;
+                const unsigned xs = a ? (unsigned)x[m] : 0u;
+                if constexpr (MP) pb[m] = int(__ldca(p.mask_snap + (xs >> 5)));
+                else pb[m] = __ldca(p.labels + xs);
+                if (!a) own[m] = -1;
+            }
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                if (own[m] < 0) continue;
+                const unsigned xu = (unsigned)x[m];
+                bool hit;
+                if constexpr (MP) hit = ((unsigned)pb[m] >> (xu & 31u)) & 1u;
+                else hit = pb[m] == it;
+                if (hit) {
+                    atomicOr(&ws.bfound[own[m] >> 5], 1u << (own[m] & 31));
+                    if constexpr (MP) ws.gpred[own[m]] = int(xu);  // any parent found will do
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < BU_WORDS; j++) {
+                if (((scan >> j) & 1u) && ((ws.bfound[j] >> lane) & 1u)) {
+                    found |= 1u << j;
+                    if constexpr (MP) par[j] = ws.gpred[j * 32 + lane];
+                }
+                if (((found >> j) & 1u) || done[j] >= ln[j]) scan &= ~(1u << j);
+            }
+            __syncwarp();
         }
+        if (bad) atomicOr(&c->error, ERR_BAD_VERTEX);
     }
     int nfound = 0;
     long long dfound = 0;
@@ -817,9 +838,9 @@ __device__ void bu_level(const BfsParams &p, int it, Smem<THREADS, MP> &sm, unsi
     // warp is free (a step's cost depends on how long its lists scan, so a
     // static split leaves most warps waiting at the level's barrier for a few
     // slow ones); a warp asks for its next step when it starts one, hiding the
-    // atomic's latency.  Once few are open, most steps only read full mask
-    // words, and a static interleave spares the counter its atomics.
-    const bool dynamic = nsteps > W && (unsigned long long)open * 8ull > (unsigned long long)p.nodes;
+    // atomic's latency.  Once fewer than a quarter are open, most steps are
+    // cheap and alike, and a static interleave spares the counter its atomics.
+    const bool dynamic = nsteps > W && (unsigned long long)open * 4ull > (unsigned long long)p.nodes;
     for (unsigned step = global_warp(); step < nsteps;) {
         unsigned nxt = 0;
         if (dynamic && lane_id() == 0) nxt = atomicAdd(&c->steal[it & 3], 1u);
