@@ -62,6 +62,7 @@ struct WarpSmem {
     unsigned disc_n;             // direction-optimizing counts of this warp's discoveries
     unsigned long long disc_m;   // in the current level, added to the counters at its end
     unsigned bfound[4];          // bottom-up window scans: vertex 32j + lane found a parent
+    unsigned segstart[4];        // bottom-up window scans: window positions where a list starts
 };
 
 template <int THREADS, bool MP>
@@ -721,7 +722,7 @@ __device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0,
     }
     // The lists the heaviest neighbour did not settle are scanned by the whole
     // warp in windows of WINDOW entries (4 per lane): every unsettled vertex
-    // puts its next entries, in vertex order, into the warp's window, so
+    // lays its next entries, in vertex order, into the warp's window, so
     // consecutive lanes read consecutive column entries (coalesced loads) and
     // a window's probes all go out at once.  A vertex whose parent turns up
     // takes no further entries.  A step then costs about one window (one
@@ -744,23 +745,43 @@ __device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0,
                 total += __shfl_sync(FULL, incl, 31);
             }
             if (total == 0) break;  // warp-uniform
+            // Each vertex with entries in the window starts a segment there:
+            // segment k (in vertex order) records its column base and owner,
+            // and a bitmap marks the window position where it starts, so a
+            // position finds its segment by counting the starts up to it.
+            if (lane < BU_WORDS) ws.segstart[lane] = 0u;
+            __syncwarp();
+            int nseg = 0;
 #pragma unroll
             for (int j = 0; j < BU_WORDS; j++) {
-                const int hi = min(excl[j] + rem[j], WINDOW);
-                for (int i = excl[j]; i < hi; i++) {
-                    ws.gofs[i] = st[j] + done[j] + (i - excl[j]);
-                    ws.surv[i] = j * 32 + lane;
+                const bool seg = rem[j] > 0 && excl[j] < WINDOW;
+                const unsigned b = __ballot_sync(FULL, seg);
+                if (seg) {
+                    const int k = nseg + __popc(b & lanemask_lt());
+                    ws.gofs[k] = st[j] + done[j] - excl[j];
+                    ws.surv[k] = j * 32 + lane;
+                    atomicOr(&ws.segstart[excl[j] >> 5], 1u << (excl[j] & 31));
+                    done[j] += min(rem[j], WINDOW - excl[j]);
                 }
-                done[j] += max(0, hi - excl[j]);
+                nseg += __popc(b);
             }
             __syncwarp();
             const int cw = min(WINDOW, total);
+            unsigned sw[BU_WORDS];
+            int before[BU_WORDS];  // segment starts in the words before word w
+#pragma unroll
+            for (int w = 0; w < BU_WORDS; w++) {
+                sw[w] = ws.segstart[w];
+                before[w] = w ? before[w - 1] + __popc(sw[w - 1]) : 0;
+            }
             int x[4], own[4], pb[4];
 #pragma unroll
             for (int m = 0; m < 4; m++) {
-                const int idx = m * 32 + lane;
-                x[m] = __ldg(p.col + (idx < cw ? ws.gofs[idx] : 0));
-                own[m] = idx < cw ? ws.surv[idx] : -1;
+                const int idx = m * 32 + lane;  // word m of the bitmap, bit lane
+                const int k = before[m] + __popc(sw[m] & ((2u << lane) - 1u)) - 1;
+                const bool in = idx < cw;
+                x[m] = __ldg(p.col + (in ? ws.gofs[k] + idx : 0));
+                own[m] = in ? ws.surv[k] : -1;
             }
 #pragma unroll
             for (int m = 0; m < 4; m++) {
