@@ -30,6 +30,8 @@ SIGNATURES = {
     "b40c_problem_reset_async": (c_int, [c_void_p, c_int, c_double]),
     "b40c_problem_extract_results": (c_int, [c_void_p, c_void_p]),
     "b40c_problem_extract_results_async": (c_int, [c_void_p, c_void_p]),
+    "b40c_problem_set_label_buffers": (c_int, [c_void_p, c_int]),
+    "b40c_problem_sync": (c_int, [c_void_p]),
     "b40c_problem_from_host_ids64": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_int]),
     "b40c_problem_extract_results_ids64": (c_int, [c_void_p, c_void_p]),
     "b40c_problem_info": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_int64), POINTER(c_void_p),

@@ -153,6 +153,16 @@ class CsrProblem:
     def set_stream(self, stream_handle: int | None) -> None:
         check(lib().b40c_problem_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)))
 
+    def set_label_buffers(self, count: int) -> None:
+        """count = 2: Reset alternates two label arrays and ExtractResultsAsync
+        copies on a side stream, overlapping the next search (no reference
+        counterpart; the reference keeps one d_labels array)."""
+        check(lib().b40c_problem_set_label_buffers(self._h, int(count)))
+
+    def Sync(self) -> int:
+        """Waits for the problem's stream and its side-stream label copies."""
+        return lib().b40c_problem_sync(self._h)
+
 
 class _Enactor:
     STRATEGY: Strategy

@@ -79,6 +79,16 @@ struct b40c_problem {
     unsigned long long *d_heavy = nullptr;  // bottom-up levels: per vertex, its neighbour of highest degree
     size_t heavy_cap = 0;
     bool heavy_ready = false;               // d_heavy holds the current graph's keys
+    // Two label buffers (b40c_problem_set_label_buffers): each Reset switches
+    // to the other one, and ExtractResultsAsync copies on a side stream, so
+    // the copy of one search's labels to the host overlaps the next search.
+    int label_buffers = 1;
+    int *d_labels_alt = nullptr;
+    size_t labels_alt_cap = 0;
+    bool use_alt = false;                        // the current labels are in d_labels_alt
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t after_search = nullptr;          // problem-stream point a side copy waits for
+    cudaEvent_t copied[2] = {nullptr, nullptr};  // the last side copy out of d_labels / d_labels_alt
 };
 
 struct b40c_enactor {
@@ -110,12 +120,16 @@ struct b40c_enactor {
     int busy_grid = 0;  // CTAs of the last instrumented fused search (0: none)
     bool have_stats = false;
     bool timing_pending = false;
-    // cached per-level graph
-    cudaGraphExec_t gexec = nullptr;
-    cudaGraph_t graph = nullptr;
-    BfsParams gparams{};
-    KernelConfig gkc{};
-    int ggrid = 0;
+    // Cached per-level graphs, two of them (a problem with two label buffers
+    // alternates its labels pointer between searches); the most recently used
+    // one is entry 0.
+    struct LevelGraph {
+        cudaGraphExec_t exec = nullptr;
+        cudaGraph_t graph = nullptr;
+        BfsParams params{};
+        KernelConfig kc{};
+        int grid = 0;
+    } lg[2];
 };
 
 namespace {
@@ -123,6 +137,13 @@ namespace {
 constexpr int LEVEL_LOG_CAP = 4096;
 
 cudaStream_t problem_stream(b40c_problem *p) { return p->stream ? p->stream : p->own_stream; }
+// The label buffer the last Reset initialised: searches write it, extracts read it.
+int *cur_labels(const b40c_problem *p) { return p->use_alt ? p->d_labels_alt : p->d_labels; }
+// Waits for everything queued on the problem: its stream and side-stream label copies.
+void sync_problem(b40c_problem *p) {
+    cudaStreamSynchronize(problem_stream(p));
+    if (p->copy_stream) cudaStreamSynchronize(p->copy_stream);
+}
 cudaStream_t enactor_stream(b40c_enactor *e) { return e->stream ? e->stream : e->own_stream; }
 
 // The ends of the row offsets, checked on the host; the rest of the CSR
@@ -148,10 +169,12 @@ void free_problem_device(b40c_problem *p) {
     p->d_col = nullptr;
     p->col_cap = p->row_cap = 0;
     cudaFree(p->d_labels);
+    cudaFree(p->d_labels_alt);
     cudaFree(p->d_mask);
-    p->d_labels = nullptr;
+    p->d_labels = p->d_labels_alt = nullptr;
     p->d_mask = nullptr;
-    p->labels_cap = p->mask_cap = 0;
+    p->labels_cap = p->labels_alt_cap = p->mask_cap = 0;
+    p->use_alt = false;
     for (int i = 0; i < 2; i++) {
         cudaFree(p->d_queue[i]);
         cudaFree(p->d_pred[i]);
@@ -332,7 +355,7 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
     bp = BfsParams{};
     bp.row_offsets = p->d_row_offsets;
     bp.col = p->d_col;
-    bp.labels = p->d_labels;
+    bp.labels = cur_labels(p);
     bp.mask = p->d_mask;
     for (int i = 0; i < 2; i++) {
         bp.queue[i] = p->d_queue[i];
@@ -371,7 +394,7 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
 
 int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size, int variant) {
     if (!e || !p) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor or problem");
-    if (!p->d_col || !p->d_labels || !p->reset_once)
+    if (!p->d_col || !cur_labels(p) || !p->reset_once)
         return set_error(B40C_ERR_ILLEGAL_STATE, "problem needs FromHostProblem and Reset before a search");
     if (src < 0 || src >= p->nodes)
         return set_error(B40C_ERR_INVALID_VALUE, "source %d outside [0, %lld)", src, (long long)p->nodes);
@@ -441,23 +464,33 @@ int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size,
         int limit = 0;
         CUDA_TRY(level_grid_limit(kc, &limit), "occupancy query");
         int grid = max_grid_size > 0 ? std::min(max_grid_size, limit) : limit;
-        BfsParams key = bp;
-        key.cond_handle = e->gparams.cond_handle;
-        bool reuse = e->gexec && e->ggrid == grid && e->gkc.strategy == kc.strategy &&
-                     e->gkc.threads == kc.threads && e->gkc.mark_pred == kc.mark_pred &&
-                     std::memcmp(&key, &e->gparams, sizeof(BfsParams)) == 0;
-        if (!reuse) {
-            if (e->gexec) cudaGraphExecDestroy(e->gexec);
-            if (e->graph) cudaGraphDestroy(e->graph);
-            e->gexec = nullptr;
-            e->graph = nullptr;
-            BfsParams gp = bp;
-            CUDA_TRY(build_level_graph(gp, kc, grid, &e->gexec, &e->graph), "building the per-level BFS graph");
-            e->gparams = gp;
-            e->gkc = kc;
-            e->ggrid = grid;
+        // A cached graph serves any source: only the init kernel, launched
+        // outside the graph, reads it.
+        int hit = -1;
+        for (int k = 0; k < 2 && hit < 0; k++) {
+            const auto &g = e->lg[k];
+            BfsParams key = bp;
+            key.cond_handle = g.params.cond_handle;
+            key.src = g.params.src;
+            if (g.exec && g.grid == grid && g.kc.strategy == kc.strategy && g.kc.threads == kc.threads &&
+                g.kc.mark_pred == kc.mark_pred && std::memcmp(&key, &g.params, sizeof(BfsParams)) == 0)
+                hit = k;
         }
-        CUDA_TRY(cudaGraphLaunch(e->gexec, s), "cudaGraphLaunch");
+        if (hit < 0) {  // build into entry 1 (the older one), then make it the newest
+            auto &g = e->lg[1];
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            if (g.graph) cudaGraphDestroy(g.graph);
+            g.exec = nullptr;
+            g.graph = nullptr;
+            BfsParams gp = bp;
+            CUDA_TRY(build_level_graph(gp, kc, grid, &g.exec, &g.graph), "building the per-level BFS graph");
+            g.params = gp;
+            g.kc = kc;
+            g.grid = grid;
+            hit = 1;
+        }
+        if (hit == 1) std::swap(e->lg[0], e->lg[1]);
+        CUDA_TRY(cudaGraphLaunch(e->lg[0].exec, s), "cudaGraphLaunch");
     } else {
         return set_error(B40C_ERR_INVALID_VALUE, "unknown variant %d", variant);
     }
@@ -533,8 +566,12 @@ extern "C" int b40c_problem_destroy(b40c_problem_t *p) {
     clear_error();
     if (!p) return B40C_SUCCESS;
     cudaSetDevice(p->device);
-    cudaStreamSynchronize(problem_stream(p));
+    sync_problem(p);
     free_problem_device(p);
+    if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+    if (p->after_search) cudaEventDestroy(p->after_search);
+    for (cudaEvent_t ev : p->copied)
+        if (ev) cudaEventDestroy(ev);
     if (p->own_stream) cudaStreamDestroy(p->own_stream);
     delete p;
     return B40C_SUCCESS;
@@ -552,7 +589,7 @@ extern "C" int b40c_problem_from_host(b40c_problem_t *p, int stream_from_host, i
     int rc = check_csr_ends(nodes, edges, h_row);
     if (rc) return rc;
     CUDA_TRY(cudaSetDevice(p->device), "cudaSetDevice");
-    cudaStreamSynchronize(problem_stream(p));
+    sync_problem(p);
     const bool was_mapped = p->mapped;
     p->mapped = stream_from_host != 0 && edges > 0;
     if (p->mapped || was_mapped) {
@@ -563,6 +600,11 @@ extern "C" int b40c_problem_from_host(b40c_problem_t *p, int stream_from_host, i
             cudaFree(p->d_labels);
             p->d_labels = nullptr;
             p->labels_cap = 0;
+        }
+        if (p->labels_alt_cap < size_t(nodes)) {
+            cudaFree(p->d_labels_alt);
+            p->d_labels_alt = nullptr;
+            p->labels_alt_cap = 0;
         }
         if (p->mask_cap < size_t((nodes + 31) / 32) * 4) {
             cudaFree(p->d_mask);
@@ -621,10 +663,17 @@ static int problem_reset(b40c_problem *p, int frontier_type, double queue_sizing
     if (!(queue_sizing > 0.0)) queue_sizing = 1.3;  // test_bfs.cu:802 default
     CUDA_TRY(cudaSetDevice(p->device), "cudaSetDevice");
     cudaStream_t s = problem_stream(p);
-    if (!p->d_labels) {
-        CUDA_TRY(cudaMalloc(&p->d_labels, sizeof(int) * size_t(p->nodes)), "CsrProblem cudaMalloc d_labels");
-        p->labels_cap = size_t(p->nodes);
+    // With two label buffers every Reset moves to the other one; a side copy
+    // still reading it (ExtractResultsAsync two searches ago) finishes first.
+    if (p->label_buffers == 2) p->use_alt = !p->use_alt;
+    int *&labels = p->use_alt ? p->d_labels_alt : p->d_labels;
+    size_t &labels_cap = p->use_alt ? p->labels_alt_cap : p->labels_cap;
+    if (!labels) {
+        CUDA_TRY(cudaMalloc(&labels, sizeof(int) * size_t(p->nodes)), "CsrProblem cudaMalloc d_labels");
+        labels_cap = size_t(p->nodes);
     }
+    if (p->label_buffers == 2 && p->copied[p->use_alt ? 1 : 0])
+        CUDA_TRY(cudaStreamWaitEvent(s, p->copied[p->use_alt ? 1 : 0], 0), "wait for the label copy");
     // ceil(nodes / 8) bytes as the reference (csr_problem.cuh:581-583), rounded to whole words.
     p->mask_bytes = size_t((p->nodes + 31) / 32) * 4;
     if (!p->d_mask) {
@@ -676,7 +725,7 @@ static int problem_reset(b40c_problem *p, int frontier_type, double queue_sizing
         }
     }
     // labels := -1, visited mask := 0 (csr_problem.cuh:719-745).
-    CUDA_TRY(cudaMemsetAsync(p->d_labels, 0xff, sizeof(int) * size_t(p->nodes), s), "labels memset");
+    CUDA_TRY(cudaMemsetAsync(labels, 0xff, sizeof(int) * size_t(p->nodes), s), "labels memset");
     CUDA_TRY(cudaMemsetAsync(p->d_mask, 0, p->mask_bytes, s), "visited mask memset");
     p->reset_once = true;
     if (sync) CUDA_TRY(cudaStreamSynchronize(s), "Reset");
@@ -693,14 +742,33 @@ extern "C" int b40c_problem_reset_async(b40c_problem_t *p, int frontier_type, do
     return problem_reset(p, frontier_type, queue_sizing, false);
 }
 
+// Enqueues the copy of the current labels to h_labels: on the problem's
+// stream, or with two label buffers on the side stream behind the problem
+// stream's work so far (the next Reset and search then overlap it).
+static int enqueue_extract(b40c_problem *p, int *h_labels) {
+    if (!p || !h_labels) return set_error(B40C_ERR_INVALID_VALUE, "ExtractResults: NULL argument");
+    int *labels = cur_labels(p);
+    if (!labels) return set_error(B40C_ERR_ILLEGAL_STATE, "ExtractResults before Reset");
+    const size_t bytes = sizeof(int) * size_t(p->nodes);
+    if (p->label_buffers == 2) {
+        CUDA_TRY(cudaEventRecord(p->after_search, problem_stream(p)), "cudaEventRecord");
+        CUDA_TRY(cudaStreamWaitEvent(p->copy_stream, p->after_search, 0), "cudaStreamWaitEvent");
+        CUDA_TRY(cudaMemcpyAsync(h_labels, labels, bytes, cudaMemcpyDeviceToHost, p->copy_stream),
+                 "CsrProblem cudaMemcpyAsync d_labels");
+        CUDA_TRY(cudaEventRecord(p->copied[p->use_alt ? 1 : 0], p->copy_stream), "cudaEventRecord");
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(h_labels, labels, bytes, cudaMemcpyDeviceToHost, problem_stream(p)),
+                 "CsrProblem cudaMemcpyAsync d_labels");
+    }
+    return B40C_SUCCESS;
+}
+
 extern "C" int b40c_problem_extract_results(b40c_problem_t *p, int *h_labels) {
     clear_error();
-    if (!p || !h_labels) return set_error(B40C_ERR_INVALID_VALUE, "ExtractResults: NULL argument");
-    if (!p->d_labels) return set_error(B40C_ERR_ILLEGAL_STATE, "ExtractResults before Reset");
-    cudaStream_t s = problem_stream(p);
-    CUDA_TRY(cudaMemcpyAsync(h_labels, p->d_labels, sizeof(int) * size_t(p->nodes), cudaMemcpyDeviceToHost, s),
-             "CsrProblem cudaMemcpy d_labels");
-    CUDA_TRY(cudaStreamSynchronize(s), "ExtractResults");
+    int rc = enqueue_extract(p, h_labels);
+    if (rc) return rc;
+    if (p->label_buffers == 2) CUDA_TRY(cudaEventSynchronize(p->copied[p->use_alt ? 1 : 0]), "ExtractResults");
+    else CUDA_TRY(cudaStreamSynchronize(problem_stream(p)), "ExtractResults");
     return B40C_SUCCESS;
 }
 
@@ -744,7 +812,7 @@ extern "C" int b40c_problem_from_host_ids64(b40c_problem_t *p, int stream_from_h
 extern "C" int b40c_problem_extract_results_ids64(b40c_problem_t *p, long long *h_labels) {
     clear_error();
     if (!p || !h_labels) return set_error(B40C_ERR_INVALID_VALUE, "ExtractResults: NULL argument");
-    if (!p->d_labels) return set_error(B40C_ERR_ILLEGAL_STATE, "ExtractResults before Reset");
+    if (!cur_labels(p)) return set_error(B40C_ERR_ILLEGAL_STATE, "ExtractResults before Reset");
     std::vector<int> tmp(size_t(p->nodes));
     int rc = b40c_problem_extract_results(p, tmp.data());
     if (rc) return rc;
@@ -754,11 +822,46 @@ extern "C" int b40c_problem_extract_results_ids64(b40c_problem_t *p, long long *
 
 extern "C" int b40c_problem_extract_results_async(b40c_problem_t *p, int *h_labels) {
     clear_error();
-    if (!p || !h_labels) return set_error(B40C_ERR_INVALID_VALUE, "ExtractResults: NULL argument");
-    if (!p->d_labels) return set_error(B40C_ERR_ILLEGAL_STATE, "ExtractResults before Reset");
-    CUDA_TRY(cudaMemcpyAsync(h_labels, p->d_labels, sizeof(int) * size_t(p->nodes), cudaMemcpyDeviceToHost,
-                             problem_stream(p)),
-             "CsrProblem cudaMemcpyAsync d_labels");
+    return enqueue_extract(p, h_labels);
+}
+
+extern "C" int b40c_problem_set_label_buffers(b40c_problem_t *p, int count) {
+    clear_error();
+    if (!p || (count != 1 && count != 2))
+        return set_error(B40C_ERR_INVALID_VALUE, "set_label_buffers: count must be 1 or 2");
+    CUDA_TRY(cudaSetDevice(p->device), "cudaSetDevice");
+    sync_problem(p);
+    if (count == 2 && !p->copy_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking), "label copy stream");
+        CUDA_TRY(cudaEventCreateWithFlags(&p->after_search, cudaEventDisableTiming), "cudaEventCreate");
+        for (cudaEvent_t &ev : p->copied) CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    if (count == 1 && p->use_alt && p->d_labels_alt) {
+        // Keep the current labels readable: move them into the buffer that stays.
+        if (!p->d_labels) {
+            CUDA_TRY(cudaMalloc(&p->d_labels, sizeof(int) * size_t(p->nodes)), "CsrProblem cudaMalloc d_labels");
+            p->labels_cap = size_t(p->nodes);
+        }
+        CUDA_TRY(cudaMemcpy(p->d_labels, p->d_labels_alt, sizeof(int) * size_t(p->nodes), cudaMemcpyDeviceToDevice),
+                 "label buffer copy");
+        p->use_alt = false;
+    }
+    if (count == 1) {
+        p->use_alt = false;
+        cudaFree(p->d_labels_alt);
+        p->d_labels_alt = nullptr;
+        p->labels_alt_cap = 0;
+    }
+    p->label_buffers = count;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_problem_sync(b40c_problem_t *p) {
+    clear_error();
+    if (!p) return set_error(B40C_ERR_INVALID_VALUE, "NULL problem");
+    CUDA_TRY(cudaSetDevice(p->device), "cudaSetDevice");
+    CUDA_TRY(cudaStreamSynchronize(problem_stream(p)), "problem stream");
+    if (p->copy_stream) CUDA_TRY(cudaStreamSynchronize(p->copy_stream), "label copy stream");
     return B40C_SUCCESS;
 }
 
@@ -770,7 +873,7 @@ extern "C" int b40c_problem_info(b40c_problem_t *p, int64_t *nodes, int64_t *edg
     if (edges) *edges = p->edges;
     if (d_row_offsets) *d_row_offsets = p->d_row_offsets;
     if (d_column_indices) *d_column_indices = p->d_col;
-    if (d_labels) *d_labels = p->d_labels;
+    if (d_labels) *d_labels = cur_labels(p);
     if (d_visited_mask) *d_visited_mask = p->d_mask;
     return B40C_SUCCESS;
 }
@@ -831,8 +934,10 @@ extern "C" int b40c_enactor_destroy(b40c_enactor_t *e) {
     if (!e) return B40C_SUCCESS;
     cudaSetDevice(e->device);
     cudaStreamSynchronize(enactor_stream(e));
-    if (e->gexec) cudaGraphExecDestroy(e->gexec);
-    if (e->graph) cudaGraphDestroy(e->graph);
+    for (auto &g : e->lg) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
     cudaFree(e->d_ctr);
     cudaFree(e->d_chunks[0]);
     cudaFree(e->d_chunks[1]);

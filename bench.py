@@ -694,31 +694,48 @@ def main():
         prob = b.CsrProblem(False)
         prob.set_stream(stream.cuda_stream)
 
-        def e2e_step(record):
+        def e2e_step(record, pipelined):
             b.check(prob.FromHostProblem(False, g.nodes, g.edges, col_p.numpy(), row_p.numpy(), 1))
             for i, s in enumerate(sources):
-                b.check(prob.Reset(ft, 1.3))
-                b.check(en.EnactSearch(prob, int(s)))
                 out = outs[i & 1].numpy()
-                b.check(prob.ExtractResults(out))
+                if pipelined:  # two label buffers: the copy of search i overlaps search i + 1
+                    b.check(prob.ResetAsync(ft, 1.3))
+                    b.check(en.EnactSearchAsync(prob, int(s)))
+                    b.check(prob.ExtractResultsAsync(out))
+                else:
+                    b.check(prob.Reset(ft, 1.3))
+                    b.check(en.EnactSearch(prob, int(s)))
+                    b.check(prob.ExtractResults(out))
                 if record:
+                    b.check(prob.Sync())
                     E[i] = int(deg[out > -1].sum())
+            if pipelined:
+                b.check(en.Sync())
+                b.check(prob.Sync())
 
-        e2e_step(True)
-        barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            e2e_step(False)
-        torch.cuda.synchronize()
-        secs = time.perf_counter() - t0
-        secs, e2e_edges = reduce_replicas(secs, float(E.sum()) * args.steps, world, dev)
+        def e2e_time(pipelined):
+            prob.set_label_buffers(2 if pipelined else 1)
+            e2e_step(True, pipelined)
+            barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                e2e_step(False, pipelined)
+            torch.cuda.synchronize()
+            return reduce_replicas(time.perf_counter() - t0, float(E.sum()) * args.steps, world, dev)
+
+        secs_sync, edges_sync = e2e_time(False)
+        secs, e2e_edges = e2e_time(True)
         e2e = {"value": e2e_edges / secs / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": int(4 * (g.nodes + 1) + 4 * g.edges + 4 * nsrc),
                "d2h_bytes_per_step": int(4 * g.nodes * nsrc),
                "ms_per_step": secs / args.steps * 1e3,
-               "step": "FromHostProblem (CSR from pinned host memory) + 64 x (Reset, EnactSearch, "
-                       "ExtractResults to pinned host memory), synchronous public API"}
+               "step": "FromHostProblem (CSR from pinned host memory) + 64 x (ResetAsync, EnactSearchAsync, "
+                       "ExtractResultsAsync to pinned host memory) with two label buffers, then Sync",
+               "synchronous_api": {"value": edges_sync / secs_sync / 1e9, "unit": UNIT,
+                                   "ms_per_step": secs_sync / args.steps * 1e3,
+                                   "step": "the same with the synchronous Reset, EnactSearch, ExtractResults "
+                                           "and one label buffer"}}
         prob.close()
         del en
 

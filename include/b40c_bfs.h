@@ -80,8 +80,20 @@ int b40c_problem_reset(b40c_problem_t *problem, int frontier_type, double queue_
 int b40c_problem_reset_async(b40c_problem_t *problem, int frontier_type, double queue_sizing);
 /* ExtractResults(h_label) (:255-273): copies nodes labels to the host. */
 int b40c_problem_extract_results(b40c_problem_t *problem, int *h_labels);
-/* Enqueues the label copy on the problem's stream without waiting. */
+/* Enqueues the label copy on the problem's stream without waiting.  With two
+ * label buffers (below) the copy goes to a side stream instead; wait for it
+ * with b40c_problem_sync. */
 int b40c_problem_extract_results_async(b40c_problem_t *problem, int *h_labels);
+/* No reference counterpart (the reference keeps one d_labels array,
+ * csr_problem.cuh:116).  count = 2: each Reset switches between two label
+ * arrays, and ExtractResultsAsync copies the last search's labels on a side
+ * stream, so that copy overlaps the next Reset and search; the device label
+ * pointer (b40c_problem_info) then changes with every Reset.  count = 1 (the
+ * default): one array, as in the reference.  Costs 4 bytes per vertex more. */
+int b40c_problem_set_label_buffers(b40c_problem_t *problem, int count);
+/* Waits for all work queued on the problem: its stream and side-stream label
+ * copies. */
+int b40c_problem_sync(b40c_problem_t *problem);
 /* 8-byte vertex ids with int sizes, the reference's g500 configuration
  * (VertexId = long long, SizeT = int; test/bfs/test_bfs.cu:1068-1093):
  * the column ids are checked and narrowed to the device's int32 layout (every

@@ -237,6 +237,58 @@ def test_async_back_to_back(cuda_device, oracle, rmat16):
             assert oracle.first_mismatch(out, ref) == -1
 
 
+@pytest.mark.parametrize("variant", [0, 2])
+def test_two_label_buffers_pipeline(cuda_device, oracle, rmat16, variant):
+    """Two label buffers: each Reset switches buffers and ExtractResultsAsync
+    copies on a side stream while the next search runs. Every copied array
+    must equal the oracle, with fused and per-level (graph) searches, the
+    latter cached per buffer. Switching back to one buffer keeps the last
+    search's labels."""
+    b = bfs_mod()
+    g = rmat16
+    sources = [int(s) for s in g.sample_sources(7, 41)]
+    for strategy in STRATEGIES:
+        if strategy == 3 and variant == 2:
+            continue  # the hybrid runs fused only
+        prob = b.CsrProblem(False).from_graph(g)
+        prob.set_label_buffers(2)
+        en = b.make_enactor(strategy)
+        outs = [np.full(g.nodes, 7, np.int32) for _ in sources]
+        ptrs = set()
+        for s, out in zip(sources, outs):
+            b.check(prob.ResetAsync(en.GetFrontierType(), 1.3))
+            ptrs.add(prob.device_pointers()["d_labels"])
+            b.check(en.EnactSearchAsync(prob, s, 0, variant))
+            b.check(prob.ExtractResultsAsync(out))
+        b.check(en.Sync())
+        b.check(prob.Sync())
+        assert len(ptrs) == 2
+        for s, out in zip(sources, outs):
+            ref, _ = oracle.bfs(g, s)
+            assert oracle.first_mismatch(out, ref) == -1, (strategy, s)
+        # synchronous calls in the two-buffer mode, then back to one buffer
+        ref, _ = oracle.bfs(g, sources[0])
+        enact = en.EnactIterativeSearch if variant == 2 else en.EnactSearch
+        b.check(prob.Reset(en.GetFrontierType(), 1.3))
+        b.check(enact(prob, sources[0]))
+        assert oracle.first_mismatch(prob.labels(), ref) == -1
+        prob.set_label_buffers(1)
+        assert oracle.first_mismatch(prob.labels(), ref) == -1
+        b.check(prob.Reset(en.GetFrontierType(), 1.3))
+        b.check(enact(prob, sources[1]))
+        ref1, _ = oracle.bfs(g, sources[1])
+        assert oracle.first_mismatch(prob.labels(), ref1) == -1
+        prob.close()
+
+
+def test_label_buffers_argument_check(cuda_device):
+    b = bfs_mod()
+    prob = b.CsrProblem(False)
+    with pytest.raises(b.BfsError):
+        prob.set_label_buffers(3)
+    prob.close()
+
+
 def test_stream_from_host(cuda_device, oracle):
     b = bfs_mod()
     g = b.rmat(12, 8, seed=3)
