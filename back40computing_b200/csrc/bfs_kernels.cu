@@ -65,10 +65,20 @@ struct WarpSmem {
     unsigned segstart[4];        // bottom-up window scans: window positions where a list starts
 };
 
+// The counts a fused kernel's phase starts from.
+struct LevelCounts {
+    unsigned L;        // input vertex or edge frontier queue length
+    unsigned nch, nw;  // CTA and warp chunks of neighbour lists input to the phase
+    unsigned nf;       // direction switch: vertices discovered for the phase
+    unsigned zmarked;  // direction switch: vertices without edges marked so far
+    unsigned long long mf;  // direction switch: their edges
+};
+
 template <int THREADS, bool MP>
 struct Smem {
     WarpSmem<MP> w[THREADS / 32];
     unsigned long long vcache[VCACHE];  // (mask word index << 32) | word value
+    LevelCounts lc;
     unsigned flag;
 };
 
@@ -1097,6 +1107,26 @@ struct DirectionChoice {
     }
 };
 
+// Reads the counts phase q starts from once per CTA and shares them through
+// shared memory (a load per thread would send every warp of the grid to the
+// same few L2 lines at each phase's start).  Called by all threads after the
+// grid barrier that ends the previous phase; ends with __syncthreads.
+template <int THREADS, bool MP>
+__device__ __forceinline__ LevelCounts read_counts(Counters *c, int q, bool dir, Smem<THREADS, MP> &sm) {
+    if (threadIdx.x == 0) {
+        LevelCounts v;
+        v.L = ld_cg(&c->qlen[q & 3]);
+        v.nch = ld_cg(&c->big[q & 3]);
+        v.nw = ld_cg(&c->wch[q & 3]);
+        v.nf = dir ? ld_cg(&c->nf[q & 3]) : 0u;
+        v.zmarked = dir ? ld_cg(&c->zmarked) : 0u;
+        v.mf = dir ? __ldcg(&c->mf[q & 3]) : 0ull;
+        sm.lc = v;
+    }
+    __syncthreads();
+    return sm.lc;
+}
+
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(BfsParams p) {
     Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
@@ -1108,13 +1138,11 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
     int it = 0;
     for (;;) {
         clk.start(p);
-        const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]), nw = ld_cg(&c->wch[it & 3]);
-        // the direction counts are loaded with the queue counts (one round trip)
-        const unsigned nf = p.do_alpha ? ld_cg(&c->nf[it & 3]) : 0u;
-        const unsigned long long mf = p.do_alpha ? __ldcg(&c->mf[it & 3]) : 0ull;
+        const LevelCounts lc = read_counts(c, it, p.do_alpha != 0u, sm);
+        const unsigned L = lc.L, nch = lc.nch, nw = lc.nw;
         if (stop_level_loop(p, it, L + nch + nw)) break;
         bool bottom_up = false;
-        if (p.do_alpha) bottom_up = dir.next(p, nf, mf);
+        if (p.do_alpha) bottom_up = dir.next(p, lc.nf, lc.mf);
         if (leader()) {
             ring_prepare(c, it);
             c->total_queued += L;
@@ -1125,7 +1153,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
                 snapshot_mask(p);
                 if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
             }
-            const unsigned done = dir.visited + ld_cg(&c->zmarked);
+            const unsigned done = dir.visited + lc.zmarked;
             bu_level<THREADS, MP>(p, it, sm, done < unsigned(p.nodes) ? unsigned(p.nodes) - done : 0u);
         } else {
             ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
@@ -1148,7 +1176,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
     int it = 0;
     for (;;) {
         clk.start(p);
-        const unsigned L = ld_cg(&c->qlen[it & 3]), nch = ld_cg(&c->big[it & 3]), nw = ld_cg(&c->wch[it & 3]);
+        const LevelCounts lc = read_counts(c, it, false, sm);
+        const unsigned L = lc.L, nch = lc.nch, nw = lc.nw;
         if (stop_level_loop(p, it, L + nch + nw)) break;
         if (leader()) {
             ring_prepare(c, it);
@@ -1178,8 +1207,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
     int it = 0, qi = 0;
     for (;;) {
         clk.start(p);
-        unsigned L = ld_cg(&c->qlen[qi & 3]);
-        const unsigned nch = ld_cg(&c->big[qi & 3]), nw = ld_cg(&c->wch[qi & 3]);
+        const LevelCounts lc = read_counts(c, qi, false, sm);
+        unsigned L = lc.L;
+        const unsigned nch = lc.nch, nw = lc.nw;
         if (stop_level_loop(p, it, L + nch + nw)) break;
         if (leader()) {
             ring_prepare(c, qi);
@@ -1191,7 +1221,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         clk.start(p);
         qi++;
-        L = ld_cg(&c->qlen[qi & 3]);
+        L = read_counts(c, qi, false, sm).L;
         if (L == 0u) break;  // no vertex discovered: the reference stops without ++
         if (leader()) {
             ring_prepare(c, qi);
@@ -1227,8 +1257,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
     int it = 0, q = 0;
     for (;;) {
         clk.start(p);
-        unsigned L = ld_cg(&c->qlen[q & 3]);
-        const unsigned nch = ld_cg(&c->big[q & 3]), nw = ld_cg(&c->wch[q & 3]);
+        const LevelCounts lc = read_counts(c, q, false, sm);
+        unsigned L = lc.L;
+        const unsigned nch = lc.nch, nw = lc.nw;
         if (stop_level_loop(p, it, L + nch + nw)) break;
         if (leader()) {
             ring_prepare(c, q);
@@ -1250,7 +1281,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
         if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
         clk.start(p);
         q++;
-        L = ld_cg(&c->qlen[q & 3]);
+        L = read_counts(c, q, false, sm).L;
         if (L == 0u) break;  // no vertex discovered: stop without ++, as two-phase does
         if (leader()) {
             ring_prepare(c, q);
@@ -1514,11 +1545,15 @@ static KernelFn fused_fn(int strategy) {
     }
 }
 
+// 1024-thread CTAs exist for expand-contract only (the host rejects them for
+// the other strategies): one CTA per SM halves the CTAs that meet at every
+// level's grid barrier, against two 512-thread CTAs.
 template <bool MP>
 static KernelFn fused_fn_t(int threads, int strategy) {
     switch (threads) {
     case 128: return fused_fn<128, MP>(strategy);
     case 512: return fused_fn<512, MP>(strategy);
+    case 1024: return strategy == STRATEGY_EXPAND_CONTRACT ? ec_fused_kernel<1024, MP> : nullptr;
     default: return fused_fn<256, MP>(strategy);
     }
 }
@@ -1528,6 +1563,7 @@ static size_t smem_bytes_t(int threads) {
     switch (threads) {
     case 128: return sizeof(Smem<128, MP>);
     case 512: return sizeof(Smem<512, MP>);
+    case 1024: return sizeof(Smem<1024, MP>);
     default: return sizeof(Smem<256, MP>);
     }
 }
@@ -1569,6 +1605,11 @@ static LevelFns level_fns_t(int threads, int strategy) {
     switch (threads) {
     case 128: return level_fns<128, MP>(strategy);
     case 512: return level_fns<512, MP>(strategy);
+    case 1024: {
+        LevelFns f{};
+        if (strategy == STRATEGY_EXPAND_CONTRACT) f.level_a = ec_level_kernel<1024, MP>;
+        return f;
+    }
     default: return level_fns<256, MP>(strategy);
     }
 }
@@ -1592,8 +1633,10 @@ static cudaError_t grid_for(const void *fn, int threads, size_t smem, int *grid)
 }
 
 cudaError_t launch_search_init(const BfsParams &p, const KernelConfig &kc, cudaStream_t stream) {
-    const int cta_chunk = kc.threads == 128 ? chunk_edges<128>() : kc.threads == 512 ? chunk_edges<512>()
-                                                                                       : chunk_edges<256>();
+    const int cta_chunk = kc.threads == 128    ? chunk_edges<128>()
+                          : kc.threads == 512  ? chunk_edges<512>()
+                          : kc.threads == 1024 ? chunk_edges<1024>()
+                                               : chunk_edges<256>();
     search_init_kernel<<<1, 64, 0, stream>>>(p, kc.strategy, kc.mark_pred ? 1 : 0, cta_chunk);
     return cudaGetLastError();
 }

@@ -43,6 +43,7 @@ struct MsSmem {
     MsWarp<MP> w[THREADS / 32];
     unsigned long long vcache[VCACHE];  // (global mask word << 32) | word value
     unsigned warp_tot[THREADS / 32];    // bookkeeping scan of bottom-up steps
+    unsigned lc[4];                     // a level's counts, read once per CTA: queue, chunks, warp chunks, retired
     unsigned flag;
     unsigned last;                      // grid_barrier_serial: this CTA arrived last
 };
@@ -642,9 +643,19 @@ __global__ void __launch_bounds__(THREADS, MS_MIN_BLOCKS(THREADS)) ms_fused_kern
     const int L_end = p.max_levels > 0 ? L + p.max_levels : 0x7fffffff;
     const int L_first = L;
     for (;;) {
-        const unsigned nq = ld_cg(&c->qlen[L & 3]), nch = ld_cg(&c->big[L & 3]), nw = ld_cg(&c->wch[L & 3]);
-        // Searches retired at the previous level's start (final before the barrier).
-        const bool retired_before = L > L_first && ld_cg(&c->retired[(L - 1) & 3]) != 0u;
+        // The level's counts, loaded by one thread and shared (a load per
+        // thread would send every warp of the grid to the same L2 lines).
+        // Retired: searches retired at the previous level's start (final
+        // before the barrier).
+        if (threadIdx.x == 0) {
+            sm.lc[0] = ld_cg(&c->qlen[L & 3]);
+            sm.lc[1] = ld_cg(&c->big[L & 3]);
+            sm.lc[2] = ld_cg(&c->wch[L & 3]);
+            sm.lc[3] = L > L_first ? ld_cg(&c->retired[(L - 1) & 3]) : 0u;
+        }
+        __syncthreads();
+        const unsigned nq = sm.lc[0], nch = sm.lc[1], nw = sm.lc[2];
+        const bool retired_before = sm.lc[3] != 0u;
         const bool empty = nq + nch + nw == 0u;
         if (blockIdx.x == 0) ms_bookkeeping(p, L, empty);
         if (empty || L >= L_end || (p.stop_on_retire && retired_before)) break;
@@ -675,8 +686,8 @@ __global__ void __launch_bounds__(THREADS, MS_MIN_BLOCKS(THREADS)) ms_fused_kern
             if (p.do_alpha) {
                 MsWarp<MP> &ws = sm.w[threadIdx.x >> 5];
                 ms_bu_level<THREADS, MP>(p, L, ws);
-            const unsigned n = ws.nbuf;
-            if (n) ms_flush(ws, n, p.queue[(L + 1) & 1], &c->qlen[(L + 1) & 3], p.qcap, &c->error);
+                const unsigned n = ws.nbuf;
+                if (n) ms_flush(ws, n, p.queue[(L + 1) & 1], &c->qlen[(L + 1) & 3], p.qcap, &c->error);
                 if (lane_id() == 0) ws.nbuf = 0;
                 __syncwarp();
             }
