@@ -1036,10 +1036,8 @@ extern "C" int b40c_enactor_set_policy(b40c_enactor_t *e, int cta_threads, int w
                                        int cull_flags) {
     clear_error();
     if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
-    if (cta_threads && cta_threads != 128 && cta_threads != 256 && cta_threads != 512 &&
-        !(cta_threads == 1024 && e->strategy == B40C_EXPAND_CONTRACT))
-        return set_error(B40C_ERR_INVALID_VALUE,
-                         "cta_threads must be 128, 256 or 512 (or 1024 for expand-contract)");
+    if (cta_threads && cta_threads != 128 && cta_threads != 256 && cta_threads != 512)
+        return set_error(B40C_ERR_INVALID_VALUE, "cta_threads must be 128, 256 or 512");
     if (warp_th < 0 || cta_th < 0 || cull_flags < -1 || cull_flags > 3)
         return set_error(B40C_ERR_INVALID_VALUE, "invalid policy field");
     if (cta_threads) e->threads = cta_threads;

@@ -1545,15 +1545,11 @@ static KernelFn fused_fn(int strategy) {
     }
 }
 
-// 1024-thread CTAs exist for expand-contract only (the host rejects them for
-// the other strategies): one CTA per SM halves the CTAs that meet at every
-// level's grid barrier, against two 512-thread CTAs.
 template <bool MP>
 static KernelFn fused_fn_t(int threads, int strategy) {
     switch (threads) {
     case 128: return fused_fn<128, MP>(strategy);
     case 512: return fused_fn<512, MP>(strategy);
-    case 1024: return strategy == STRATEGY_EXPAND_CONTRACT ? ec_fused_kernel<1024, MP> : nullptr;
     default: return fused_fn<256, MP>(strategy);
     }
 }
@@ -1563,7 +1559,6 @@ static size_t smem_bytes_t(int threads) {
     switch (threads) {
     case 128: return sizeof(Smem<128, MP>);
     case 512: return sizeof(Smem<512, MP>);
-    case 1024: return sizeof(Smem<1024, MP>);
     default: return sizeof(Smem<256, MP>);
     }
 }
@@ -1605,11 +1600,6 @@ static LevelFns level_fns_t(int threads, int strategy) {
     switch (threads) {
     case 128: return level_fns<128, MP>(strategy);
     case 512: return level_fns<512, MP>(strategy);
-    case 1024: {
-        LevelFns f{};
-        if (strategy == STRATEGY_EXPAND_CONTRACT) f.level_a = ec_level_kernel<1024, MP>;
-        return f;
-    }
     default: return level_fns<256, MP>(strategy);
     }
 }
@@ -1633,10 +1623,8 @@ static cudaError_t grid_for(const void *fn, int threads, size_t smem, int *grid)
 }
 
 cudaError_t launch_search_init(const BfsParams &p, const KernelConfig &kc, cudaStream_t stream) {
-    const int cta_chunk = kc.threads == 128    ? chunk_edges<128>()
-                          : kc.threads == 512  ? chunk_edges<512>()
-                          : kc.threads == 1024 ? chunk_edges<1024>()
-                                               : chunk_edges<256>();
+    const int cta_chunk = kc.threads == 128 ? chunk_edges<128>() : kc.threads == 512 ? chunk_edges<512>()
+                                                                                       : chunk_edges<256>();
     search_init_kernel<<<1, 64, 0, stream>>>(p, kc.strategy, kc.mark_pred ? 1 : 0, cta_chunk);
     return cudaGetLastError();
 }
