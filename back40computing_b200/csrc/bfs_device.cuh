@@ -138,6 +138,36 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
+// The counts a fused kernel's phase starts from.
+struct LevelCounts {
+    unsigned L;             // input vertex or edge frontier queue length
+    unsigned nch, nw;       // CTA and warp chunks of neighbour lists input to the phase
+    unsigned nf;            // direction switch: vertices discovered for the phase
+    unsigned zmarked;       // direction switch: vertices without edges marked so far
+    unsigned long long mf;  // direction switch: their edges
+};
+
+// Loads the counts phase q starts from (dir: with the direction counts).
+__device__ __forceinline__ LevelCounts load_counts(const Counters *c, int q, bool dir) {
+    LevelCounts v;
+    v.L = __ldcg(&c->qlen[q & 3]);
+    v.nch = __ldcg(&c->big[q & 3]);
+    v.nw = __ldcg(&c->wch[q & 3]);
+    v.nf = dir ? __ldcg(&c->nf[q & 3]) : 0u;
+    v.zmarked = dir ? __ldcg(&c->zmarked) : 0u;
+    v.mf = dir ? __ldcg(&c->mf[q & 3]) : 0ull;
+    return v;
+}
+
+// What a grid barrier loads for the phase after it: the counts of phase q,
+// into the CTA's shared copy *out.
+struct NextCounts {
+    LevelCounts *out;
+    int q;
+    bool dir;
+};
+__device__ __forceinline__ NextCounts next_counts(LevelCounts *out, int q, bool dir) { return NextCounts{out, q, dir}; }
+
 // ---- grid barrier ----------------------------------------------------------------
 // All CTAs of a cooperative launch call this the same number of times.  Each
 // CTA's thread 0 arrives with an acq_rel add on a 64-bit count of all
@@ -147,9 +177,13 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 // less).  A waiting CTA spins with an acquire load until then, the error word
 // becomes non-zero, or wait_ns of %globaltimer time pass (then
 // ERR_BARRIER_TIMEOUT is raised and the CTA leaves the wait).  Returns false
-// on any raised error, identically for every thread of the CTA.
+// on any raised error, identically for every thread of the CTA.  With `next`,
+// the waiting thread also loads the next phase's counts into the CTA's shared
+// copy, in the same round trip as the error word: every thread reads them
+// after the barrier, and no warp has to go to L2 for them.
 __device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wait_ns,
-                                             unsigned *smem_flag, unsigned expected) {
+                                             unsigned *smem_flag, unsigned expected,
+                                             const NextCounts *next = nullptr) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned long long arrived = atom_add_acqrel_gpu_u64(&c->bar_total, 1ull);
@@ -167,6 +201,7 @@ __device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wai
                 if (ns < 128) ns <<= 1;
             }
         }
+        if (next) *next->out = load_counts(c, next->q, next->dir);
         *smem_flag = ld_relaxed_gpu(&c->error);
     }
     __syncthreads();
@@ -175,6 +210,10 @@ __device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wai
 __device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wait_ns,
                                              unsigned *smem_flag) {
     return grid_barrier(c, wait_ns, smem_flag, gridDim.x);
+}
+__device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wait_ns, unsigned *smem_flag,
+                                             NextCounts next) {
+    return grid_barrier(c, wait_ns, smem_flag, gridDim.x, &next);
 }
 
 // The same barrier with a serial section: the CTA whose arrival completes the

@@ -65,15 +65,6 @@ struct WarpSmem {
     unsigned segstart[4];        // bottom-up window scans: window positions where a list starts
 };
 
-// The counts a fused kernel's phase starts from.
-struct LevelCounts {
-    unsigned L;        // input vertex or edge frontier queue length
-    unsigned nch, nw;  // CTA and warp chunks of neighbour lists input to the phase
-    unsigned nf;       // direction switch: vertices discovered for the phase
-    unsigned zmarked;  // direction switch: vertices without edges marked so far
-    unsigned long long mf;  // direction switch: their edges
-};
-
 template <int THREADS, bool MP>
 struct Smem {
     WarpSmem<MP> w[THREADS / 32];
@@ -1107,22 +1098,13 @@ struct DirectionChoice {
     }
 };
 
-// Reads the counts phase q starts from once per CTA and shares them through
-// shared memory (a load per thread would send every warp of the grid to the
-// same few L2 lines at each phase's start).  Called by all threads after the
-// grid barrier that ends the previous phase; ends with __syncthreads.
+// The counts a fused kernel's first phase starts from, read once per CTA and
+// shared through shared memory (a load per thread would send every warp of
+// the grid to the same few L2 lines).  Later phases get theirs from the grid
+// barrier before them (next_counts), in the waiting thread's last round trip.
 template <int THREADS, bool MP>
 __device__ __forceinline__ LevelCounts read_counts(Counters *c, int q, bool dir, Smem<THREADS, MP> &sm) {
-    if (threadIdx.x == 0) {
-        LevelCounts v;
-        v.L = ld_cg(&c->qlen[q & 3]);
-        v.nch = ld_cg(&c->big[q & 3]);
-        v.nw = ld_cg(&c->wch[q & 3]);
-        v.nf = dir ? ld_cg(&c->nf[q & 3]) : 0u;
-        v.zmarked = dir ? ld_cg(&c->zmarked) : 0u;
-        v.mf = dir ? __ldcg(&c->mf[q & 3]) : 0ull;
-        sm.lc = v;
-    }
+    if (threadIdx.x == 0) sm.lc = load_counts(c, q, dir);
     __syncthreads();
     return sm.lc;
 }
@@ -1136,9 +1118,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
     DirectionChoice dir;
     BusyClock clk;
     int it = 0;
+    const bool dcounts = p.do_alpha != 0u;
+    LevelCounts lc = read_counts(c, 0, dcounts, sm);
     for (;;) {
         clk.start(p);
-        const LevelCounts lc = read_counts(c, it, p.do_alpha != 0u, sm);
         const unsigned L = lc.L, nch = lc.nch, nw = lc.nw;
         if (stop_level_loop(p, it, L + nch + nw)) break;
         bool bottom_up = false;
@@ -1159,7 +1142,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
             ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
         }
         clk.stop(p);
-        if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, it + 1, dcounts))) break;
+        lc = sm.lc;
         it++;
     }
     clk.flush(p);
@@ -1174,9 +1158,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
     Counters *c = p.ctr;
     BusyClock clk;
     int it = 0;
+    LevelCounts lc = read_counts(c, 0, false, sm);
     for (;;) {
         clk.start(p);
-        const LevelCounts lc = read_counts(c, it, false, sm);
         const unsigned L = lc.L, nch = lc.nch, nw = lc.nw;
         if (stop_level_loop(p, it, L + nch + nw)) break;
         if (leader()) {
@@ -1186,7 +1170,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
         }
         ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, pol);
         clk.stop(p);
-        if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, it + 1, false))) break;
+        lc = sm.lc;
         it++;
     }
     clk.flush(p);
@@ -1205,9 +1190,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
     Counters *c = p.ctr;
     BusyClock clk;
     int it = 0, qi = 0;
+    LevelCounts lc = read_counts(c, 0, false, sm);
     for (;;) {
         clk.start(p);
-        const LevelCounts lc = read_counts(c, qi, false, sm);
         unsigned L = lc.L;
         const unsigned nch = lc.nch, nw = lc.nw;
         if (stop_level_loop(p, it, L + nch + nw)) break;
@@ -1218,10 +1203,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
         }
         tp_contract<THREADS, MP>(p, it, qi, L, nch, nw, sm, pol);
         clk.stop(p);
-        if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, qi + 1, false))) break;
         clk.start(p);
         qi++;
-        L = read_counts(c, qi, false, sm).L;
+        L = sm.lc.L;
         if (L == 0u) break;  // no vertex discovered: the reference stops without ++
         if (leader()) {
             ring_prepare(c, qi);
@@ -1229,7 +1214,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
         }
         tp_expand<THREADS, MP>(p, qi, L, sm, pol);
         clk.stop(p);
-        if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, qi + 1, false))) break;
+        lc = sm.lc;
         qi++;
         it++;
     }
@@ -1255,9 +1241,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
     const unsigned long long saturation = 4ull * THREADS * gridDim.x;
     BusyClock clk;
     int it = 0, q = 0;
+    LevelCounts lc = read_counts(c, 0, false, sm);
     for (;;) {
         clk.start(p);
-        const LevelCounts lc = read_counts(c, q, false, sm);
         unsigned L = lc.L;
         const unsigned nch = lc.nch, nw = lc.nw;
         if (stop_level_loop(p, it, L + nch + nw)) break;
@@ -1271,17 +1257,18 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
         if (edges <= saturation) {
             ce_level<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
             clk.stop(p);
-            if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+            if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, q + 1, false))) break;
+            lc = sm.lc;
             q++;
             it++;
             continue;
         }
         tp_contract<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
         clk.stop(p);
-        if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, q + 1, false))) break;
         clk.start(p);
         q++;
-        L = read_counts(c, q, false, sm).L;
+        L = sm.lc.L;
         if (L == 0u) break;  // no vertex discovered: stop without ++, as two-phase does
         if (leader()) {
             ring_prepare(c, q);
@@ -1289,7 +1276,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
         }
         tp_expand<THREADS, MP>(p, q, L, sm, pol);
         clk.stop(p);
-        if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
+        if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, q + 1, false))) break;
+        lc = sm.lc;
         q++;
         it++;
     }
