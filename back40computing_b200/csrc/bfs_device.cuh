@@ -144,17 +144,20 @@ struct LevelCounts {
     unsigned nch, nw;       // CTA and warp chunks of neighbour lists input to the phase
     unsigned nf;            // direction switch: vertices discovered for the phase
     unsigned zmarked;       // direction switch: vertices without edges marked so far
+    unsigned retired;       // multi-search: searches retired at the previous phase's start
     unsigned long long mf;  // direction switch: their edges
 };
 
-// Loads the counts phase q starts from (dir: with the direction counts).
-__device__ __forceinline__ LevelCounts load_counts(const Counters *c, int q, bool dir) {
+// Loads the counts phase q starts from (dir: with the direction counts;
+// retired: with the multi-search retirements of phase q - 1).
+__device__ __forceinline__ LevelCounts load_counts(const Counters *c, int q, bool dir, bool retired = false) {
     LevelCounts v;
     v.L = __ldcg(&c->qlen[q & 3]);
     v.nch = __ldcg(&c->big[q & 3]);
     v.nw = __ldcg(&c->wch[q & 3]);
     v.nf = dir ? __ldcg(&c->nf[q & 3]) : 0u;
     v.zmarked = dir ? __ldcg(&c->zmarked) : 0u;
+    v.retired = retired ? __ldcg(&c->retired[(q - 1) & 3]) : 0u;
     v.mf = dir ? __ldcg(&c->mf[q & 3]) : 0ull;
     return v;
 }
@@ -165,8 +168,11 @@ struct NextCounts {
     LevelCounts *out;
     int q;
     bool dir;
+    bool retired;
 };
-__device__ __forceinline__ NextCounts next_counts(LevelCounts *out, int q, bool dir) { return NextCounts{out, q, dir}; }
+__device__ __forceinline__ NextCounts next_counts(LevelCounts *out, int q, bool dir, bool retired = false) {
+    return NextCounts{out, q, dir, retired};
+}
 
 // ---- grid barrier ----------------------------------------------------------------
 // All CTAs of a cooperative launch call this the same number of times.  Each
@@ -201,7 +207,7 @@ __device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wai
                 if (ns < 128) ns <<= 1;
             }
         }
-        if (next) *next->out = load_counts(c, next->q, next->dir);
+        if (next) *next->out = load_counts(c, next->q, next->dir, next->retired);
         *smem_flag = ld_relaxed_gpu(&c->error);
     }
     __syncthreads();
@@ -220,9 +226,12 @@ __device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wai
 // count runs serial() with all its threads (it may use __syncthreads) before
 // it publishes the new generation, so serial() sees everything every CTA did
 // before the barrier and every CTA sees its results after it.
+// With `next`, thread 0 of every CTA loads the next phase's counts after the
+// barrier, with the error word, as grid_barrier does.
 template <class F>
 __device__ __forceinline__ bool grid_barrier_serial(Counters *c, unsigned long long wait_ns, unsigned *smem_flag,
-                                                    unsigned *smem_last, const F &serial) {
+                                                    unsigned *smem_last, const F &serial,
+                                                    const NextCounts *next = nullptr) {
     __syncthreads();
     unsigned gen = 0;
     if (threadIdx.x == 0) {
@@ -251,7 +260,10 @@ __device__ __forceinline__ bool grid_barrier_serial(Counters *c, unsigned long l
             if (ns < 256) ns <<= 1;
         }
     }
-    if (threadIdx.x == 0) *smem_flag = ld_relaxed_gpu(&c->error);
+    if (threadIdx.x == 0) {
+        if (next) *next->out = load_counts(c, next->q, next->dir, next->retired);
+        *smem_flag = ld_relaxed_gpu(&c->error);
+    }
     __syncthreads();
     return *smem_flag == 0u;
 }

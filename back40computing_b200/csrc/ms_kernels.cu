@@ -43,7 +43,7 @@ struct MsSmem {
     MsWarp<MP> w[THREADS / 32];
     unsigned long long vcache[VCACHE];  // (global mask word << 32) | word value
     unsigned warp_tot[THREADS / 32];    // bookkeeping scan of bottom-up steps
-    unsigned lc[4];                     // a level's counts, read once per CTA: queue, chunks, warp chunks, retired
+    LevelCounts lc;                     // a level's counts, read once per CTA
     unsigned flag;
     unsigned last;                      // grid_barrier_serial: this CTA arrived last
 };
@@ -642,20 +642,16 @@ __global__ void __launch_bounds__(THREADS, MS_MIN_BLOCKS(THREADS)) ms_fused_kern
     int L = c->cur_it;
     const int L_end = p.max_levels > 0 ? L + p.max_levels : 0x7fffffff;
     const int L_first = L;
+    // A level's counts are loaded by one thread per CTA and shared (a load per
+    // thread would send every warp of the grid to the same L2 lines): for the
+    // first level here, for the others by the grid barrier before them.
+    // Retired: searches retired at the previous level's start (final before
+    // the barrier).
+    if (threadIdx.x == 0) sm.lc = load_counts(c, L, false);
+    __syncthreads();
     for (;;) {
-        // The level's counts, loaded by one thread and shared (a load per
-        // thread would send every warp of the grid to the same L2 lines).
-        // Retired: searches retired at the previous level's start (final
-        // before the barrier).
-        if (threadIdx.x == 0) {
-            sm.lc[0] = ld_cg(&c->qlen[L & 3]);
-            sm.lc[1] = ld_cg(&c->big[L & 3]);
-            sm.lc[2] = ld_cg(&c->wch[L & 3]);
-            sm.lc[3] = L > L_first ? ld_cg(&c->retired[(L - 1) & 3]) : 0u;
-        }
-        __syncthreads();
-        const unsigned nq = sm.lc[0], nch = sm.lc[1], nw = sm.lc[2];
-        const bool retired_before = sm.lc[3] != 0u;
+        const unsigned nq = sm.lc.L, nch = sm.lc.nch, nw = sm.lc.nw;
+        const bool retired_before = sm.lc.retired != 0u;
         const bool empty = nq + nch + nw == 0u;
         if (blockIdx.x == 0) ms_bookkeeping(p, L, empty);
         if (empty || L >= L_end || (p.stop_on_retire && retired_before)) break;
@@ -692,10 +688,12 @@ __global__ void __launch_bounds__(THREADS, MS_MIN_BLOCKS(THREADS)) ms_fused_kern
                 __syncwarp();
             }
         }
+        const NextCounts next = next_counts(&sm.lc, L + 1, false, true);
         if (p.do_alpha) {
-            if (!grid_barrier_serial(c, p.wait_ns, &sm.flag, &sm.last, [&] { ms_directions<THREADS, MP>(p, L + 1, sm); }))
+            if (!grid_barrier_serial(c, p.wait_ns, &sm.flag, &sm.last,
+                                     [&] { ms_directions<THREADS, MP>(p, L + 1, sm); }, &next))
                 break;
-        } else if (!grid_barrier(c, p.wait_ns, &sm.flag)) {
+        } else if (!grid_barrier(c, p.wait_ns, &sm.flag, gridDim.x, &next)) {
             break;
         }
         L++;
