@@ -396,7 +396,9 @@ __device__ void ms_level(const MsParams &p, int L, unsigned nq_in, unsigned nch,
 // offsets): mask words w0 .. w0+3 of the slot; lane j owns vertex 32w + j of
 // each word, probes its heaviest neighbour and, when that is not a parent,
 // scans its list 2 entries per round, software-pipelined, for a neighbour at
-// the slot's depth L - start_level.  Label probes are ordinary
+// the slot's depth L - start_level.  Unlike the single search it scans per
+// lane, not by warp windows: the batches' graphs are small and their lists
+// short, and windows measured slower there.  Label probes are ordinary
 // (L1-cached) loads, ordered after the labels they look for by the grid
 // barriers before the level.  A word has one writer in the level.
 template <int THREADS, bool MP>
