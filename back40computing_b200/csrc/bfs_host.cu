@@ -725,8 +725,8 @@ static int problem_reset(b40c_problem *p, int frontier_type, double queue_sizing
         }
     }
     // labels := -1, visited mask := 0 (csr_problem.cuh:719-745).
-    CUDA_TRY(cudaMemsetAsync(labels, 0xff, sizeof(int) * size_t(p->nodes), s), "labels memset");
-    CUDA_TRY(cudaMemsetAsync(p->d_mask, 0, p->mask_bytes, s), "visited mask memset");
+    CUDA_TRY(launch_reset_state(labels, p->nodes, p->d_mask, (long long)(p->mask_bytes / 4), s),
+             "labels and visited mask initialisation");
     p->reset_once = true;
     if (sync) CUDA_TRY(cudaStreamSynchronize(s), "Reset");
     return B40C_SUCCESS;

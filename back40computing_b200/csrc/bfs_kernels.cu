@@ -1497,6 +1497,18 @@ __global__ void heavy_neighbour_kernel(const int *row_offsets, const int *col, i
     }
 }
 
+// Reset's initialisation in one launch: labels := -1 (16-byte stores; the
+// array is cudaMalloc-aligned) and the visited mask := 0.
+__global__ void reset_state_kernel(int *labels, long long n, unsigned *mask, long long mask_words) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n4 = n >> 2;
+    int4 *l4 = reinterpret_cast<int4 *>(labels);
+    for (long long i = t; i < n4; i += stride) l4[i] = make_int4(-1, -1, -1, -1);
+    for (long long i = (n4 << 2) + t; i < n; i += stride) labels[i] = -1;
+    for (long long i = t; i < mask_words; i += stride) mask[i] = 0u;
+}
+
 // CSR checks on the device: out[0] = the first row v whose offsets decrease
 // (row[v+1] < row[v]), out[1] = the first entry outside [0, nodes); both stay
 // ~0 when there is none (out must start at ~0).
@@ -1647,6 +1659,16 @@ cudaError_t launch_heavy_neighbour(const int *row_offsets, const int *col, int n
     if (!e) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e) return e;
     heavy_neighbour_kernel<<<sms * 8, 256, 0, stream>>>(row_offsets, col, nodes, edges, keys);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset_state(int *labels, long long nodes, unsigned *mask, long long mask_words,
+                               cudaStream_t stream) {
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (!e) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e) return e;
+    reset_state_kernel<<<sms * 8, 256, 0, stream>>>(labels, nodes, mask, mask_words);
     return cudaGetLastError();
 }
 

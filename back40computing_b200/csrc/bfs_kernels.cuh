@@ -100,6 +100,10 @@ cudaError_t launch_symmetry_hash(const int *row_offsets, const int *col, int nod
 // neighbours.  keys[0..nodes) must start at zero.
 cudaError_t launch_heavy_neighbour(const int *row_offsets, const int *col, int nodes, long long edges,
                                    unsigned long long *keys, cudaStream_t stream);
+// Reset's state initialisation in one launch: labels[0..nodes) := -1 (labels
+// 16-byte aligned), mask[0..mask_words) := 0.
+cudaError_t launch_reset_state(int *labels, long long nodes, unsigned *mask, long long mask_words,
+                               cudaStream_t stream);
 // CSR validity on the device: out[0] = first row whose offsets decrease,
 // out[1] = first column entry outside [0, nodes); ~0 when none.  out[0..1]
 // must start at ~0.
