@@ -662,7 +662,8 @@ def main():
             "alg_gbs": float(bytes_alg.sum() * args.steps / (np.sum(kern_ms) / 1e3) / 1e9),
             "edges_visited_mean": float(E.mean()),
             "vertices_visited_mean": float(V.mean()),
-            "launches": 2 * args.steps * nsrc,
+            # per search: Reset's initialisation kernel, the init kernel, the fused kernel
+            "launches": 3 * args.steps * nsrc,
             "clocks": clk,
         }
         del en
