@@ -251,6 +251,18 @@ extern "C" int b40c_batch_add_graph(b40c_batch_t *b, int nodes, int edges, const
     GraphRes g;
     g.nodes = nodes;
     g.edges = edges;
+    // Frees the graph's device arrays if a step below fails before the
+    // batch owns them.
+    struct Unwind {
+        GraphRes *g;
+        bool owned = false;
+        ~Unwind() {
+            if (owned) return;
+            cudaFree(g->d_row);
+            cudaFree(g->d_col);
+            cudaFree(g->d_heavy);
+        }
+    } unwind{&g};
     CUDA_TRY(cudaMalloc(&g.d_row, sizeof(int) * (size_t(nodes) + 1)), "batch graph row offsets");
     CUDA_TRY(cudaMalloc(&g.d_col, sizeof(int) * (size_t(edges) + 4)), "batch graph column indices");
     CUDA_TRY(cudaMemcpy(g.d_row, h_row, sizeof(int) * (size_t(nodes) + 1), cudaMemcpyHostToDevice), "upload");
@@ -260,6 +272,7 @@ extern "C" int b40c_batch_add_graph(b40c_batch_t *b, int nodes, int edges, const
     if (g.symmetric)
         CUDA_TRY(ms_graph_heavy(g.d_row, g.d_col, nodes, edges, &g.d_heavy), "heaviest-neighbour keys");
     b->graphs.push_back(g);
+    unwind.owned = true;
     // Refresh the device graph table.
     std::vector<MsGraph> table(b->graphs.size());
     for (size_t i = 0; i < b->graphs.size(); i++)

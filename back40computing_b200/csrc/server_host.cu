@@ -324,6 +324,18 @@ extern "C" int b40c_server_add_graph(b40c_server_t *s, int nodes, int edges, con
     ResidentGraph g;
     g.nodes = nodes;
     g.edges = edges;
+    // Frees the graph's device arrays if a step below fails before the
+    // server owns them.
+    struct Unwind {
+        ResidentGraph *g;
+        bool owned = false;
+        ~Unwind() {
+            if (owned) return;
+            cudaFree(g->d_row);
+            cudaFree(g->d_col);
+            cudaFree(g->d_heavy);
+        }
+    } unwind{&g};
     CUDA_TRY(cudaMalloc(&g.d_row, sizeof(int) * (size_t(nodes) + 1)), "server graph row offsets");
     CUDA_TRY(cudaMalloc(&g.d_col, sizeof(int) * (size_t(edges) + 4)), "server graph column indices");
     CUDA_TRY(cudaMemcpy(g.d_row, h_row, sizeof(int) * (size_t(nodes) + 1), cudaMemcpyHostToDevice), "upload");
@@ -333,6 +345,7 @@ extern "C" int b40c_server_add_graph(b40c_server_t *s, int nodes, int edges, con
     if (g.symmetric)
         CUDA_TRY(ms_graph_heavy(g.d_row, g.d_col, nodes, edges, &g.d_heavy), "heaviest-neighbour keys");
     s->graphs.push_back(g);
+    unwind.owned = true;
     std::vector<MsGraph> table(s->graphs.size());
     for (size_t i = 0; i < s->graphs.size(); i++)
         table[i] = MsGraph{s->graphs[i].d_row, s->graphs[i].d_col, s->graphs[i].nodes, int(s->graphs[i].edges + 4),
