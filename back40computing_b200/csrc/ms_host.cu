@@ -271,18 +271,21 @@ extern "C" int b40c_batch_add_graph(b40c_batch_t *b, int nodes, int edges, const
     CUDA_TRY(ms_graph_symmetric(g.d_row, g.d_col, nodes, edges, &g.symmetric), "graph symmetry check");
     if (g.symmetric)
         CUDA_TRY(ms_graph_heavy(g.d_row, g.d_col, nodes, edges, &g.d_heavy), "heaviest-neighbour keys");
-    b->graphs.push_back(g);
-    unwind.owned = true;
-    // Refresh the device graph table.
-    std::vector<MsGraph> table(b->graphs.size());
+    // Refresh the device graph table with the new graph appended; the batch
+    // owns the graph only once the table holds it, so that a failure here
+    // leaves b->graphs and the device table as they were.
+    std::vector<MsGraph> table(b->graphs.size() + 1);
     for (size_t i = 0; i < b->graphs.size(); i++)
         table[i] = MsGraph{b->graphs[i].d_row, b->graphs[i].d_col, b->graphs[i].nodes,
                            int(b->graphs[i].edges + 4), int(b->graphs[i].edges), b->graphs[i].symmetric,
                            b->graphs[i].d_heavy};
+    table.back() = MsGraph{g.d_row, g.d_col, g.nodes, int(g.edges + 4), int(g.edges), g.symmetric, g.d_heavy};
     int rc = grow(&b->d_graphs, &b->graphs_cap, table.size(), "batch graph table");
     if (rc) return rc;
     CUDA_TRY(cudaMemcpy(b->d_graphs, table.data(), sizeof(MsGraph) * table.size(), cudaMemcpyHostToDevice),
              "graph table upload");
+    b->graphs.push_back(g);
+    unwind.owned = true;
     *graph_id = int(b->graphs.size()) - 1;
     return B40C_SUCCESS;
 }

@@ -1,20 +1,21 @@
 // Breadth-first search that allocates no memory: b40c_enact_search_no_alloc.
 //
-// Some callers cannot call cudaMalloc at search time: code running while a
-// CUDA graph is being captured on its stream, allocators and schedulers that
-// own every byte of the device and forbid allocation behind their back, and
-// real-time loops that cannot pay for the device-wide synchronisation that
-// cudaMalloc/cudaFree may imply.  For them this entry point runs the fused
-// expand-contract search over a CSR and a label array the caller already
-// holds on the device.  The scratch memory the search needs besides those
-// (search counters, visited bitmask, the two frontier queues and the CTA and
-// warp chunk tables) is carved from one file-scope device array of a fixed
-// size, NOALLOC_SCRATCH_BYTES, which every GPU that loads this library holds
-// until the process exits.
+// Some callers cannot call cudaMalloc at search time: frameworks whose
+// allocator owns every byte of the device and forbids allocation behind its
+// back, and real-time loops that cannot pay for the device-wide
+// synchronisation that cudaMalloc/cudaFree may imply.  For them this entry
+// point runs the fused expand-contract search over a CSR and a label array
+// the caller already holds on the device.  The scratch memory the search
+// needs besides those (search counters, visited bitmask, the two frontier
+// queues and the CTA and warp chunk tables) is carved from one file-scope
+// device array of a fixed size, NOALLOC_SCRATCH_BYTES, which every GPU that
+// loads this library holds until the process exits.
 //
 // Host code cannot use the array's name as a device address (on the host it
-// names a host-side stand-in), so the first call on each device looks up the
-// array's device address with cudaGetSymbolAddress and keeps it.
+// names a host-side stand-in), so the first call in each CUDA context looks
+// up the array's device address with cudaGetSymbolAddress and keeps it for
+// that context; a new context (after cudaDeviceReset, or a context the caller
+// made current) gets its own lookup.
 //
 // Every call shares the one array, and a call leaves its contents behind: each
 // call therefore clears the counters and the visited bitmask (they must start
@@ -23,6 +24,7 @@
 // overlaps on the GPU (different streams, or different host threads, on the
 // same device) race on the array and corrupt each other's results.
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -46,6 +48,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 
 std::mutex g_noalloc_mutex;
 void *g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
+unsigned long long g_noalloc_ctx[NOALLOC_MAX_DEVICES] = {};  // context id the address belongs to
 
 size_t round256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -95,13 +98,44 @@ int cuda_fail(cudaError_t e, const char *what) {
         if (_e != cudaSuccess) return cuda_fail(_e, what);  \
     } while (0)
 
-// Device address of the scratch array on the current device, looked up once.
+// Id of the calling thread's current CUDA context (driver entry points found
+// through the runtime, so the library links no libcuda); 0 when unknown.
+unsigned long long current_context_id() {
+    typedef CUresult (*GetCurrentFn)(CUcontext *);
+    typedef CUresult (*GetIdFn)(CUcontext, unsigned long long *);
+    static GetCurrentFn get_current = nullptr;
+    static GetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetIdFn>(f);
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, &id) == CUDA_SUCCESS)
+        return id;
+    return 0;
+}
+
+// Device address of the scratch array in the current context.  It is looked
+// up once per device and context (symbol addresses belong to a context, and a
+// reset device gets a new one); when the context id cannot be read, it is
+// looked up on every call (the lookup allocates nothing).
 int scratch_base(int device, unsigned char **base) {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_base[device]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_noalloc_base[device] || ctx == 0 || g_noalloc_ctx[device] != ctx) {
         void *p = nullptr;
         NA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress of the scratch array");
         g_noalloc_base[device] = p;
+        g_noalloc_ctx[device] = ctx;
     }
     *base = static_cast<unsigned char *>(g_noalloc_base[device]);
     return B40C_SUCCESS;

@@ -344,17 +344,25 @@ extern "C" int b40c_server_add_graph(b40c_server_t *s, int nodes, int edges, con
     CUDA_TRY(ms_graph_symmetric(g.d_row, g.d_col, nodes, edges, &g.symmetric), "graph symmetry check");
     if (g.symmetric)
         CUDA_TRY(ms_graph_heavy(g.d_row, g.d_col, nodes, edges, &g.d_heavy), "heaviest-neighbour keys");
-    s->graphs.push_back(g);
-    unwind.owned = true;
-    std::vector<MsGraph> table(s->graphs.size());
+    // The new device table (old graphs plus this one) is built and uploaded
+    // before it replaces the old one; the server owns the graph only once
+    // that succeeded, so a failure leaves s->graphs and s->d_graphs as they were.
+    std::vector<MsGraph> table(s->graphs.size() + 1);
     for (size_t i = 0; i < s->graphs.size(); i++)
         table[i] = MsGraph{s->graphs[i].d_row, s->graphs[i].d_col, s->graphs[i].nodes, int(s->graphs[i].edges + 4),
                            int(s->graphs[i].edges), s->graphs[i].symmetric, s->graphs[i].d_heavy};
+    table.back() = MsGraph{g.d_row, g.d_col, g.nodes, int(g.edges + 4), int(g.edges), g.symmetric, g.d_heavy};
+    MsGraph *d_table = nullptr;
+    CUDA_TRY(cudaMalloc(&d_table, sizeof(MsGraph) * table.size()), "server graph table");
+    cudaError_t ue = cudaMemcpy(d_table, table.data(), sizeof(MsGraph) * table.size(), cudaMemcpyHostToDevice);
+    if (ue != cudaSuccess) {
+        cudaFree(d_table);
+        CUDA_TRY(ue, "graph table upload");
+    }
     cudaFree(s->d_graphs);
-    s->d_graphs = nullptr;
-    CUDA_TRY(cudaMalloc(&s->d_graphs, sizeof(MsGraph) * table.size()), "server graph table");
-    CUDA_TRY(cudaMemcpy(s->d_graphs, table.data(), sizeof(MsGraph) * table.size(), cudaMemcpyHostToDevice),
-             "graph table upload");
+    s->d_graphs = d_table;
+    s->graphs.push_back(g);
+    unwind.owned = true;
     *graph_id = int(s->graphs.size()) - 1;
     return B40C_SUCCESS;
 }

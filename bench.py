@@ -76,7 +76,8 @@ def parse_args():
     ap.add_argument("--batched-max-scale", type=int, default=20, help="largest R-MAT scale of the batched set")
     ap.add_argument("--batched-policy", default="tuned", choices=["tuned", "default"],
                     help="autotuned multi-search policy, or the library defaults")
-    ap.add_argument("--verify", type=int, default=2, help="sources checked against the oracle")
+    ap.add_argument("--verify", type=int, default=-1,
+                    help="sources of each strategy checked against the oracle during warm-up (-1: all)")
     ap.add_argument("--sources", type=int, default=NUM_SOURCES, help="sources per step (64 for the bench line)")
     return ap.parse_args()
 
@@ -110,6 +111,15 @@ def make_graph(scale, ef):
     return graphs.rmat(scale, ef, 0.57, 0.19, 0.19, seed=1, undirected=True)
 
 
+def bench_config(args, nodes, edges, nsrc, world):
+    """The workload both arms report (identical dicts, so the two lines compare)."""
+    return {"workload": f"BFS rmat-s{args.scale}-ef{args.edge_factor} (a=.57 b=.19 c=.19, seed 1, symmetrized), "
+                        f"{nsrc} sources/step (seed 2)",
+            "nodes": int(nodes), "edges": int(edges), "parallelism": f"replicas x{world}",
+            "l2": ("inputs larger than L2" if 4 * edges > 126e6 else "inputs smaller than L2")
+                  + " (column indices %.0f MB)" % (4 * edges / 1e6)}
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -118,14 +128,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def measured_traffic(scale):
-    """DRAM bytes per launch of the headline kernel from the committed ncu
-    summary (profiles/ec_fused_rmat21_full.md), scaled there to scale 22."""
-    prof = ROOT / "profiles" / "ec_fused_rmat21_full.md"
+def measured_traffic(scale, strategy):
+    """DRAM bytes (read + write) of one launch of a strategy's fused kernel on
+    this workload, from the committed ncu capture (profiles/dram_fused_rmat22.md,
+    lines "traffic_bytes_<strategy>: <bytes>"); None when not captured."""
+    prof = ROOT / "profiles" / "dram_fused_rmat22.md"
     if scale != 22 or not prof.exists():
         return None
+    key = f"traffic_bytes_{STRATEGY_NAMES[strategy]}:"
     for line in prof.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch_rmat22:"):
+        if line.startswith(key):
             return float(line.split(":", 1)[1])
     return None
 
@@ -253,24 +265,25 @@ def run_cpu(g, sources, threads):
 
 
 def reference_arm(args):
+    """The reference's own CPU BFS (SimpleReferenceBfs from oracle/_ref, or the
+    oracle's restatement when it is absent) on every host thread, over the same
+    graph and the same 64 sources per step as the GPU arm.  The graph comes
+    from the oracle's restated generator, so this arm never loads the product
+    library."""
     rank, world, _ = dist_info()
     if rank != 0:
         return
-    g = make_graph(args.scale, args.edge_factor)
-    sources = g.sample_sources(NUM_SOURCES, 2)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle import rmat as oracle_rmat
+    g = oracle_rmat(args.scale, args.edge_factor, 0.57, 0.19, 0.19, seed=1, undirected=True)
+    sources = g.sample_sources(args.sources, 2)
     threads = os.cpu_count() or 1
-    per_step = max(8, threads)
-    idx = 0
     for _ in range(args.warmup):
-        sel = np.take(sources, range(idx, idx + per_step), mode="wrap")
-        idx += per_step
-        run_cpu(g, sel, threads)
+        run_cpu(g, sources, threads)
     edges, secs = 0, 0.0
     kind = "port"
     for _ in range(args.steps):
-        sel = np.take(sources, range(idx, idx + per_step), mode="wrap")
-        idx += per_step
-        e, dt, kind = run_cpu(g, sel, threads)
+        e, dt, kind = run_cpu(g, sources, threads)
         edges += e
         secs += dt
     gteps = edges / secs / 1e9
@@ -278,12 +291,13 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": gteps, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-        "data": "synthetic (seeded R-MAT)",
-        "config": {"workload": f"rmat-s{args.scale}-ef{args.edge_factor} BFS, {per_step} of 64 sources per step",
-                   "nodes": g.nodes, "edges": g.edges},
+        "data": "synthetic (seeded R-MAT, 64 sources)",
+        "config": bench_config(args, g.nodes, g.edges, len(sources), args.gpus),
         "cpu_baseline": {"value": gteps, "unit": UNIT, "cores": threads, "kind": kind,
-                         "sample": f"{per_step} sources per step x {args.steps} steps, one search per host thread"},
+                         "sample": f"all {len(sources)} sources per step x {args.steps} steps, "
+                                   f"one search at a time per host thread"},
         "e2e": {"value": gteps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "graph_sha256": g.sha256(),
     }
     print(json.dumps(line), flush=True)
 
@@ -380,6 +394,17 @@ def batched_leg(b, torch, stream, args):
     from back40computing_b200.batch import BfsBatch
     gs, desc, gids, srcs = batched_set(max_scale=args.batched_max_scale)
     n = len(gids)
+    # crc32 of the oracle's labels of every search.
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle import Oracle
+    orc = Oracle()
+    crc_ref = np.zeros(n, np.int64)
+    for gi, g in enumerate(gs):
+        idx = np.nonzero(gids == gi)[0]
+        refs, _ = orc.bfs_many_labels(g, srcs[idx])
+        for k, i in enumerate(idx):
+            crc_ref[i] = _crc(refs[k])
+        del refs
     seq = SequentialSearches(b, gs, stream)
     crc_seq = np.zeros(n, np.int64)
     edges = np.zeros(n, np.int64)
@@ -400,6 +425,9 @@ def batched_leg(b, torch, stream, args):
         torch.cuda.synchronize()
         return ev[0].elapsed_time(ev[1])
 
+    bad = np.nonzero(crc_seq != crc_ref)[0]
+    if bad.size:
+        raise SystemExit(f"bench: single-search labels differ from the oracle for searches {bad[:8].tolist()}")
     for _ in range(args.warmup):
         time_seq()
     seq_ms = [time_seq() for _ in range(args.steps)]
@@ -416,9 +444,9 @@ def batched_leg(b, torch, stream, args):
     for g in gs:
         batch.add_graph(g)
     batch.run(gids, srcs, use_cuda_graph=True)
-    mismatched = [i for i in range(n) if _crc(batch.labels(i)) != crc_seq[i]]
+    mismatched = [i for i in range(n) if _crc(batch.labels(i)) != crc_ref[i]]
     if mismatched:
-        raise SystemExit(f"bench: batched labels differ from single searches for searches {mismatched[:8]}")
+        raise SystemExit(f"bench: batched labels differ from the oracle for searches {mismatched[:8]}")
     for _ in range(args.warmup):
         batch.run(gids, srcs, use_cuda_graph=True)
     bat_ms = []
@@ -436,7 +464,8 @@ def batched_leg(b, torch, stream, args):
         "sequential_queries_per_s": n / (s_ms / 1e3), "sequential_ms": s_ms,
         "speedup_vs_sequential": s_ms / b_ms,
         "policy": policy,
-        "labels": "identical to single searches (crc32 of all %d label arrays)" % n,
+        "labels": "every search's labels equal the oracle's (crc32 of all %d label arrays, batched and "
+                  "single searches)" % n,
         "timing": "device time, median of %d; sequential = back-to-back async Reset+EnactSearch" % args.steps,
     }
 
@@ -604,8 +633,16 @@ def main():
         if world > 1:
             dist.barrier()
 
+    # Oracle labels of the sources checked during warm-up (every source by
+    # default), computed once on the host threads before any timing.
+    nver = nsrc if args.verify < 0 else min(args.verify, nsrc)
+    refs = None
+    if nver:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        from oracle import Oracle
+        refs, _ = Oracle().bfs_many_labels(g, sources[:nver])
     results = {}
-    verified = []
+    checked = 0
     for strat in strategies:
         en = b.make_enactor(strat)
         en.set_stream(stream.cuda_stream)
@@ -623,8 +660,12 @@ def main():
                     vis = lab > -1
                     V[i] = int(vis.sum())
                     E[i] = int(deg[vis].sum())
-                    if i < args.verify:
-                        verified.append((strat, int(s), lab))
+                    if i < nver:
+                        if not np.array_equal(lab, refs[i]):
+                            bad = int(np.nonzero(lab != refs[i])[0][0])
+                            raise SystemExit(f"bench: labels of strategy {strat} source {int(s)} differ from "
+                                             f"the oracle at vertex {bad}")
+                        checked += 1
             b.check(en.Sync())
         # Timed steps.
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps * nsrc)]
@@ -662,22 +703,14 @@ def main():
             "alg_gbs": float(bytes_alg.sum() * args.steps / (np.sum(kern_ms) / 1e3) / 1e9),
             "edges_visited_mean": float(E.mean()),
             "vertices_visited_mean": float(V.mean()),
+            "verified_sources": min(nver, nsrc),
             # per search: Reset's initialisation kernel, the init kernel, the fused kernel
             "launches": 3 * args.steps * nsrc,
             "clocks": clk,
         }
         del en
 
-    # Labels of the warm-up runs checked bit-exact against the oracle.
-    sys.path.insert(0, str(ROOT / "oracle"))
-    from oracle import Oracle
-    orc = Oracle()
-    ref_cache = {}
-    for strat, s, lab in verified:
-        if s not in ref_cache:
-            ref_cache[s] = orc.bfs(g, s)[0]
-        if orc.first_mismatch(lab, ref_cache[s]) != -1:
-            raise SystemExit(f"bench: labels of strategy {strat} source {s} differ from the oracle")
+    del refs
 
     # End-to-end through the public API with host buffers.
     e2e = None
@@ -766,23 +799,31 @@ def main():
         return
     peak, peak_kind = measured_peaks()
     head = results[HEADLINE]
-    traffic = measured_traffic(args.scale)
+    for st, r in results.items():
+        # DRAM bytes of one launch (ncu, this workload) over the mean launch time.
+        tr = measured_traffic(args.scale, st)
+        r["dram_bytes_per_launch"] = tr
+        r["dram_frac"] = None if tr is None else tr / (r["kernel_ms_mean"] / 1e3) / 1e9 / peak
+        r["alg_frac"] = r["alg_gbs"] / peak
+    traffic = head["dram_bytes_per_launch"]
     line = {
         "metric": METRIC, "value": head["gteps"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded R-MAT, 64 sources)",
-        "config": {"workload": f"BFS rmat-s{args.scale}-ef{args.edge_factor} (a=.57 b=.19 c=.19), "
-                               f"{nsrc} sources/step, strategy {STRATEGY_NAMES[HEADLINE]} "
-                               f"{'fused, direction-optimizing (alpha 14, beta 24)' if args.variant == 1 else 'iterative'}",
-                   "nodes": g.nodes, "edges": g.edges, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (column indices %.0f MB)" % (4 * g.edges / 1e6)},
+        "config": bench_config(args, g.nodes, g.edges, nsrc, world),
+        "headline": f"strategy {STRATEGY_NAMES[HEADLINE]} "
+                    f"{'fused, direction-optimizing (alpha 14, beta 24)' if args.variant == 1 else 'iterative'}",
         "roofline": {"bound": "hbm", "achieved": head["alg_gbs"], "peak": peak, "unit": "GB/s",
                      "frac": head["alg_gbs"] / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "dram_frac": head["dram_frac"],
                      "alg_bytes_per_launch": head["alg_bytes_per_search"],
                      "kernel_ms_mean": head["kernel_ms_mean"],
-                     "note": "achieved = (4E + 20V) per search / fused-kernel time; the direction-optimizing "
-                             "search reads fewer bytes than 4E + 20V (bottom-up levels stop at the first "
-                             "parent), so traffic (ncu DRAM bytes per launch) is below it"},
+                     "note": "achieved = (4E + 20V) per search / fused-kernel time (of measured peak); traffic = "
+                             "ncu DRAM bytes of one launch of the fused kernel on this workload; dram_frac = "
+                             "traffic / mean kernel time / peak. The direction-optimizing search reads far fewer "
+                             "bytes than 4E + 20V (bottom-up levels stop at the first parent)"},
+        "verified": f"{checked} searches (every strategy x {min(nver, nsrc)} sources) bit-exact against the oracle "
+                    f"during warm-up",
         "strategies": {STRATEGY_NAMES[s]: {k: v for k, v in r.items() if k != "clocks"} for s, r in results.items()},
         "gpu_launches": head["launches"],
         "clocks": head["clocks"],

@@ -286,10 +286,10 @@ int b40c_server_run_trace(b40c_server_t *server, int n, const int *graph_ids, co
 int b40c_server_stats(b40c_server_t *server, long long *epochs, long long *max_active);
 
 /* ---- search without allocation (no counterpart in the reference) --------
- * For callers that must not allocate device memory while they search: code
- * that runs while a CUDA graph is being captured on its stream, frameworks
- * whose allocator owns all device memory, and latency-bound loops that cannot
- * afford the synchronisation cudaMalloc/cudaFree may cause.  Runs one fused
+ * For callers that must not allocate device memory while they search:
+ * frameworks whose allocator owns all device memory, and latency-bound loops
+ * that cannot afford the synchronisation cudaMalloc/cudaFree may cause.  Runs
+ * one fused
  * expand-contract search (default policy, depth labels) over a CSR the caller
  * already holds on the current device: d_row_offsets (nodes + 1 entries,
  * non-decreasing from 0 to edges) and d_column_indices (edges entries, each
@@ -300,10 +300,10 @@ int b40c_server_stats(b40c_server_t *server, long long *epochs, long long *max_a
  * queues, chunk tables) comes from one static 32 MiB device array that every
  * GPU loading the library holds until exit; a graph whose scratch would not
  * fit (about 1M vertices with 16M edges fits) is rejected with
- * B40C_ERR_INVALID_VALUE and a message naming both sizes.  The first call on
- * each device looks up that array's device address; make it before any
- * stream capture.  All calls on a device share the array: calls that overlap
- * on the GPU race and corrupt each other's results. */
+ * B40C_ERR_INVALID_VALUE and a message naming both sizes.  The first call in
+ * each device's CUDA context looks up that array's device address; make it
+ * before any stream capture.  All calls on a device share the array: calls
+ * that overlap on the GPU race and corrupt each other's results. */
 int b40c_enact_search_no_alloc(int nodes, int edges, const int *d_row_offsets,
                                const int *d_column_indices, int src, int *d_labels,
                                int *search_depth, void *stream);

@@ -162,3 +162,51 @@ int oracle_bfs_many(int64_t nodes, const int *row_offsets, const int *column_ind
     for (t = 0; t < threads; t++) free(job[t].labels);
     return rc;
 }
+
+/* ---- reference labels of many sources at once (parity checks) ---- */
+typedef struct {
+    int64_t nodes;
+    const int *row_offsets, *column_indices;
+    const int *sources;
+    int num_sources;
+    int stride, first;
+    int *labels; /* num_sources x nodes */
+    int64_t *depths;
+} oracle_labels_job_t;
+
+static void *oracle_labels_worker(void *arg) {
+    oracle_labels_job_t *job = (oracle_labels_job_t *)arg;
+    int s;
+    for (s = job->first; s < job->num_sources; s += job->stride)
+        job->depths[s] = oracle_bfs(job->nodes, job->row_offsets, job->column_indices, job->sources[s],
+                                    job->labels + (size_t)s * (size_t)job->nodes);
+    return NULL;
+}
+
+/* SimpleReferenceBfs from every source, spread over threads host threads:
+ * labels[s * nodes + v] receives source s's labels and depths[s] its
+ * search_depth (as oracle_bfs).  Returns 0. */
+int oracle_bfs_many_labels(int64_t nodes, const int *row_offsets, const int *column_indices,
+                           const int *sources, int num_sources, int threads, int *labels, int64_t *depths) {
+    pthread_t tid[256];
+    oracle_labels_job_t job[256];
+    int t;
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    if (threads > num_sources) threads = num_sources > 0 ? num_sources : 1;
+    for (t = 0; t < threads; t++) {
+        job[t].nodes = nodes;
+        job[t].row_offsets = row_offsets;
+        job[t].column_indices = column_indices;
+        job[t].sources = sources;
+        job[t].num_sources = num_sources;
+        job[t].stride = threads;
+        job[t].first = t;
+        job[t].labels = labels;
+        job[t].depths = depths;
+    }
+    for (t = 0; t < threads; t++) pthread_create(&tid[t], NULL, oracle_labels_worker, &job[t]);
+    for (t = 0; t < threads; t++) pthread_join(tid[t], NULL);
+    return 0;
+}
+

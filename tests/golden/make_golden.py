@@ -6,7 +6,7 @@ oracle/_ref/libref_bfs.so by oracle/Makefile.  Graphs come from the
 reference's builders (grid2d/grid3d/random/rmat, seeded with srand) and from
 this package's generators.  Run from the repository root:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REFERENCE=<reference tree> && python tests/golden/make_golden.py
 
 Each file holds: row_offsets, column_indices, sources, labels (one row per
 source), depths (SimpleReferenceBfs search_depth) and a `builder` string.

@@ -103,3 +103,28 @@ def test_batch_direction_optimizing(cuda_device, oracle, mixed_graphs, alpha, be
     _check(oracle, batch, graphs, gids, srcs)
     batch.run(gids, srcs, use_cuda_graph=True)  # replay
     _check(oracle, batch, graphs, gids, srcs)
+
+
+def test_bench_batched_set_every_search_matches_oracle(cuda_device, oracle):
+    """The bench's batched workload itself: 64 graphs (48 R-MAT of scale 12..20
+    and edge factor 8..32, 16 Erdos-Renyi of mean degree 16), 16 seeded sources
+    each, 1024 searches in one CUDA-graph launch with the tuned policy; every
+    search's labels bit-exact against the oracle."""
+    import bench
+    from back40computing_b200 import tune
+    from back40computing_b200.batch import BfsBatch
+    gs, _, gids, srcs = bench.batched_set(max_scale=20)
+    policy = tune.tune_batch(gs, gids, srcs, cache=tune.TuneCache(None, seed=tune.SHIPPED))
+    batch = BfsBatch()
+    tune.apply_batch_policy(batch, policy)
+    for g in gs:
+        batch.add_graph(g)
+    batch.run(gids, srcs, use_cuda_graph=True)
+    batch.run(gids, srcs, use_cuda_graph=True)  # the replayed graph, as the bench times it
+    for gi, g in enumerate(gs):
+        idx = np.nonzero(gids == gi)[0]
+        refs, _ = oracle.bfs_many_labels(g, srcs[idx])
+        for k, i in enumerate(idx):
+            assert oracle.first_mismatch(batch.labels(int(i)), refs[k]) == -1, (gi, int(i), int(srcs[i]))
+            assert batch.search_depth(int(i)) == int(refs[k].max())
+    batch.close()

@@ -106,3 +106,38 @@ def test_oracle_threads_agree(oracle):
     for s, ev in zip(src, ev1):
         lab, _ = oracle.bfs(g, int(s))
         assert oracle.visit_stats(g, lab)[1] == ev
+
+
+@pytest.mark.parametrize("scale,ef,undirected,seed", [(10, 16, True, 3), (12, 8, False, 5), (16, 16, True, 1)])
+def test_oracle_rmat_matches_product_generator(scale, ef, undirected, seed):
+    """The oracle's restated R-MAT (the CPU legs' input) is the product's graph,
+    byte for byte, and draws the same sources."""
+    import back40computing_b200 as b
+    from oracle import rmat
+    g_oracle = rmat(scale, ef, seed=seed, undirected=undirected)
+    g_prod = b.rmat(scale, ef, 0.57, 0.19, 0.19, seed=seed, undirected=undirected)
+    assert g_oracle.sha256() == g_prod.sha256()
+    assert np.array_equal(g_oracle.sample_sources(64, 2), g_prod.sample_sources(64, 2))
+
+
+def test_oracle_rmat_matches_product_generator_at_bench_size():
+    """The bench workload itself: R-MAT scale 22, edge factor 16, seed 1,
+    symmetrized (134,214,152 entries), and its 64 sources (seed 2)."""
+    import back40computing_b200 as b
+    from oracle import rmat
+    g_oracle = rmat(22, 16, seed=1, undirected=True)
+    g_prod = b.rmat(22, 16, 0.57, 0.19, 0.19, seed=1, undirected=True)
+    assert g_oracle.edges == 134214152
+    assert g_oracle.sha256() == g_prod.sha256()
+    assert np.array_equal(g_oracle.sample_sources(64, 2), g_prod.sample_sources(64, 2))
+
+
+def test_oracle_many_labels_match_single_searches(oracle):
+    from oracle import rmat
+    g = rmat(13, 8, seed=7)
+    src = g.sample_sources(9, 3)
+    labels, depths = oracle.bfs_many_labels(g, src, threads=4)
+    for i, s in enumerate(src):
+        lab, d = oracle.bfs(g, int(s))
+        assert np.array_equal(labels[i], lab)
+        assert depths[i] == d

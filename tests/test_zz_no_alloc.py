@@ -1,8 +1,8 @@
 """b40c_enact_search_no_alloc: the search for callers that must not allocate.
 
-Code that runs while a CUDA graph is being captured, frameworks whose own
-allocator owns all device memory, and latency-bound loops cannot let a search
-call cudaMalloc.  This entry point takes the CSR and the label array from the
+Frameworks whose own allocator owns all device memory, and latency-bound
+loops that cannot pay for the synchronisation an allocation may cause, cannot
+let a search call cudaMalloc.  This entry point takes the CSR and the label array from the
 caller and takes its scratch from a static 32 MiB device array, so these tests
 check that its labels and search depth equal those of the ordinary
 Reset + EnactSearch path (expand-contract), bit for bit, over calls in a row
