@@ -49,10 +49,13 @@ SIGNATURES = {
     "b40c_enactor_set_stream": (c_int, [c_void_p, c_void_p]),
     "b40c_enactor_set_policy": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
     "b40c_enactor_set_level_log": (c_int, [c_void_p, c_int]),
+    "b40c_enactor_level_times": (c_int, [c_void_p, c_int, POINTER(c_int64), POINTER(c_int64), POINTER(c_int)]),
     "b40c_enactor_level_log": (c_int, [c_void_p, c_int, POINTER(c_int64), POINTER(c_int), POINTER(c_int),
                                        POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "b40c_enactor_set_direction_optimizing": (c_int, [c_void_p, c_int, c_int]),
     "b40c_enactor_set_wait_limit_us": (c_int, [c_void_p, c_longlong]),
+    "b40c_enactor_set_l2_persistence": (c_int, [c_void_p, c_int]),
+    "b40c_enactor_set_bottom_up_staging": (c_int, [c_void_p, c_int]),
     "b40c_graph_grid2d": (c_int, [c_int, c_int, POINTER(CsrT)]),
     "b40c_graph_grid3d": (c_int, [c_int, c_int, POINTER(CsrT)]),
     "b40c_graph_rmat": (c_int, [c_int, c_int, c_double, c_double, c_double, c_uint64, c_int, POINTER(CsrT)]),

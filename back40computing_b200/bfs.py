@@ -248,8 +248,11 @@ class _Enactor:
         if n.value == 0:
             return []
         t0 = ts[0]
+        we = (ctypes.c_int64 * max_records)()
+        m = ctypes.c_int()
+        check(lib().b40c_enactor_level_times(self._h, max_records, None, we, ctypes.byref(m)))
         return [{"level": i, "start_ns": ts[i] - t0, "frontier": fr[i], "chunks": ch[i], "wchunks": wc[i],
-                 "bottom_up": bool(bu[i])}
+                 "bottom_up": bool(bu[i]), "work_end_ns": (we[i] - t0) if we[i] else None}
                 for i in range(n.value)]
 
     def set_direction_optimizing(self, alpha: int = 14, beta: int = 24) -> None:
@@ -258,6 +261,14 @@ class _Enactor:
 
     def set_wait_limit_us(self, us: int) -> None:
         check(lib().b40c_enactor_set_wait_limit_us(self._h, int(us)))
+
+    def set_bottom_up_staging(self, enable: bool = True) -> None:
+        """Bottom-up steps stage their inputs in shared memory one step ahead (default off)."""
+        check(lib().b40c_enactor_set_bottom_up_staging(self._h, int(bool(enable))))
+
+    def set_l2_persistence(self, what: int) -> None:
+        """0 off, 1 keep the visited mask L2-resident, 2 the mask and the labels."""
+        check(lib().b40c_enactor_set_l2_persistence(self._h, int(what)))
 
 
 class EnactorExpandContract(_Enactor):

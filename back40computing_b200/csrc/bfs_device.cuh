@@ -46,6 +46,12 @@ struct alignas(256) Counters {
     unsigned pad_b[60];
     unsigned wch[4];     // wch[q&3]: warp chunks of neighbour lists input to phase q
     unsigned pad_w[60];
+    // raw[q&3]: the edge frontier phase q has as the reference defines it --
+    // every neighbour of the vertices the phase before expanded, whether it
+    // sits in the queue, in a chunk, or was dropped by the gather-time cull.
+    // Edge-frontier strategies stop, count total_queued and log by it.
+    unsigned raw[4];
+    unsigned pad_r[60];
     unsigned error;      // ERR_* bits
     int iteration;       // iteration counter at exit (reference d_iteration)
     int cur_it;          // current iteration for per-level (graph-driven) kernels
@@ -116,6 +122,11 @@ __device__ __forceinline__ uint64_t policy_evict_first() {
     asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
     return pol;
 }
+__device__ __forceinline__ uint64_t policy_evict_normal() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
 __device__ __forceinline__ int4 ldg_stream_v4(const int *p, uint64_t pol) {
     int4 v;
     asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
@@ -131,6 +142,41 @@ __device__ __forceinline__ int ldg_stream(const int *p, uint64_t pol) {
     return v;
 }
 
+// ---- bulk copies into shared memory with mbarrier completion (sm_90+) ---------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return unsigned(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// Makes initialised mbarriers visible to the bulk-copy unit.
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+// Global -> shared bulk copy of `bytes` (a multiple of 16; both addresses
+// 16-byte aligned) completing on mbarrier bar.  A plain (non-multicast) copy
+// from this GPU's own memory.
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// Orders the generic-proxy global writes this thread has observed before the
+// bulk (async-proxy) reads it issues next.
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
@@ -145,6 +191,7 @@ struct LevelCounts {
     unsigned nf;            // direction switch: vertices discovered for the phase
     unsigned zmarked;       // direction switch: vertices without edges marked so far
     unsigned retired;       // multi-search: searches retired at the previous phase's start
+    unsigned raw;           // edge-frontier strategies: the phase's edge frontier before culling
     unsigned long long mf;  // direction switch: their edges
 };
 
@@ -158,6 +205,7 @@ __device__ __forceinline__ LevelCounts load_counts(const Counters *c, int q, boo
     v.nf = dir ? __ldcg(&c->nf[q & 3]) : 0u;
     v.zmarked = dir ? __ldcg(&c->zmarked) : 0u;
     v.retired = retired ? __ldcg(&c->retired[(q - 1) & 3]) : 0u;
+    v.raw = __ldcg(&c->raw[q & 3]);
     v.mf = dir ? __ldcg(&c->mf[q & 3]) : 0ull;
     return v;
 }

@@ -100,6 +100,8 @@ struct b40c_enactor {
     unsigned cull_flags = CULL_HISTORY;
     unsigned do_alpha = 0, do_beta = 0;  // direction-optimizing expand-contract (0: top-down only)
     unsigned long long wait_ns = 5000000000ull;
+    int l2_persist = 0;  // b40c_enactor_set_l2_persistence
+    bool stage_bu = false;  // b40c_enactor_set_bottom_up_staging
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     Counters *d_ctr = nullptr;
@@ -217,16 +219,17 @@ int ensure_symmetry_known(b40c_problem *p) {
 int ensure_heavy_known(b40c_problem *p) {
     if (p->heavy_ready) return B40C_SUCCESS;
     cudaStream_t s = problem_stream(p);
-    if (p->heavy_cap < size_t(p->nodes)) {
+    // HEAVY_PAD zero keys past the last vertex: a bottom-up step stages whole
+    // 16-byte units of keys with one bulk copy.
+    const size_t keys = size_t(p->nodes) + HEAVY_PAD;
+    if (p->heavy_cap < keys) {
         cudaFree(p->d_heavy);
         p->d_heavy = nullptr;
         p->heavy_cap = 0;
-        CUDA_TRY(cudaMalloc(&p->d_heavy, sizeof(unsigned long long) * size_t(p->nodes)),
-                 "cudaMalloc heaviest-neighbour keys");
-        p->heavy_cap = size_t(p->nodes);
+        CUDA_TRY(cudaMalloc(&p->d_heavy, sizeof(unsigned long long) * keys), "cudaMalloc heaviest-neighbour keys");
+        p->heavy_cap = keys;
     }
-    CUDA_TRY(cudaMemsetAsync(p->d_heavy, 0, sizeof(unsigned long long) * size_t(p->nodes), s),
-             "heaviest-neighbour keys clear");
+    CUDA_TRY(cudaMemsetAsync(p->d_heavy, 0, sizeof(unsigned long long) * keys, s), "heaviest-neighbour keys clear");
     CUDA_TRY(launch_heavy_neighbour(p->d_row_offsets, p->d_col, int(p->nodes), p->edges, p->d_heavy, s),
              "heaviest-neighbour launch");
     CUDA_TRY(cudaStreamSynchronize(s), "heaviest-neighbour keys");
@@ -351,6 +354,14 @@ int ensure_enactor_buffers(b40c_enactor *e, b40c_problem *p) {
     return B40C_SUCCESS;
 }
 
+// Whether a column array of `edges` entries is streamed with evict_first:
+// when it takes more than a quarter of the device's L2.
+bool stream_column(int device, int64_t edges) {
+    int l2 = 0;
+    if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device) != cudaSuccess || l2 <= 0) return true;
+    return double(edges) * sizeof(int) > 0.25 * double(l2);
+}
+
 int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
     bp = BfsParams{};
     bp.row_offsets = p->d_row_offsets;
@@ -383,6 +394,7 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
     bp.cta_th = std::max(e->cta_th, e->warp_th);
     bp.cull_flags = e->cull_flags;
     bp.edges = p->edges;
+    bp.stream_col = stream_column(p->device, p->edges) ? 1 : 0;
     bp.do_alpha = 0;  // enabled by enqueue_search for searches that can run bottom-up
     bp.do_beta = 0;
     if (qcap < 1) return set_error(B40C_ERR_ILLEGAL_STATE, "frontier queues not allocated: call Reset first");
@@ -391,6 +403,10 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
                          "predecessor queues missing: Reset with this enactor's frontier type");
     return B40C_SUCCESS;
 }
+
+int set_persist_window(b40c_enactor *e, b40c_problem *p, cudaStream_t s, bool on);
+int launch_search(b40c_enactor *e, BfsParams &bp, const KernelConfig &kc, cudaStream_t s, int max_grid_size,
+                  int variant);
 
 int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size, int variant) {
     if (!e || !p) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor or problem");
@@ -435,12 +451,65 @@ int enqueue_search(b40c_enactor *e, b40c_problem *p, int src, int max_grid_size,
             if ((rc = ensure_heavy_known(p))) return rc;
             bp.mask_snap = p->d_mask_snap;
             bp.heavy = p->d_heavy;
+            bp.stage_bu = e->stage_bu ? 1 : 0;  // the problem's row offsets, mask and keys carry the padding
+            kc.stage_bu = e->stage_bu;           // and the launch carries the stage buffers
             bp.do_alpha = e->do_alpha;
             bp.do_beta = e->do_beta;
         }
     }
     if (bp.levels)
         CUDA_TRY(cudaMemsetAsync(bp.levels, 0, sizeof(LevelRecord) * LEVEL_LOG_CAP, s), "level log clear");
+    if (e->l2_persist && (rc = set_persist_window(e, p, s, true))) return rc;
+    rc = launch_search(e, bp, kc, s, max_grid_size, variant);
+    if (e->l2_persist) {
+        const int rc2 = set_persist_window(e, p, s, false);
+        if (!rc) rc = rc2;
+    }
+    return rc;
+}
+
+// The persisting access-policy window of b40c_enactor_set_l2_persistence on
+// stream s: the visited mask (what 1), or the mask and the labels when their
+// two allocations lie side by side (what 2); on = false clears it.
+int set_persist_window(b40c_enactor *e, b40c_problem *p, cudaStream_t s, bool on) {
+    cudaStreamAttrValue v{};
+    if (on) {
+        int max_window = 0, max_persist = 0;
+        CUDA_TRY(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, p->device),
+                 "access-policy window size query");
+        CUDA_TRY(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, p->device),
+                 "persisting L2 size query");
+        char *lo = reinterpret_cast<char *>(p->d_mask);
+        char *hi = lo + p->mask_bytes;
+        if (e->l2_persist == 2) {
+            char *l = reinterpret_cast<char *>(cur_labels(p));
+            char *lh = l + sizeof(int) * size_t(p->nodes);
+            char *a = std::min(lo, l), *z = std::max(hi, lh);
+            const size_t both = size_t(hi - lo) + size_t(lh - l);
+            if (size_t(z - a) <= size_t(max_window) && size_t(z - a) <= both + (size_t(1) << 20)) {
+                lo = a;
+                hi = z;
+            }
+        }
+        const size_t bytes = std::min(size_t(hi - lo), size_t(max_window));
+        size_t limit = 0;
+        CUDA_TRY(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize), "persisting L2 limit query");
+        const size_t want = std::min(bytes, size_t(max_persist));
+        if (limit < want) CUDA_TRY(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want), "persisting L2 limit");
+        v.accessPolicyWindow.base_ptr = lo;
+        v.accessPolicyWindow.num_bytes = bytes;
+        v.accessPolicyWindow.hitRatio = bytes ? std::min(1.0f, float(double(want) / double(bytes))) : 0.f;
+        v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    }
+    CUDA_TRY(cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &v), "access-policy window");
+    return B40C_SUCCESS;
+}
+
+// The launches of one search on stream s (init kernel, then the fused kernel
+// or the per-level graph), bracketed by the enactor's timing events.
+int launch_search(b40c_enactor *e, BfsParams &bp, const KernelConfig &kc, cudaStream_t s, int max_grid_size,
+                  int variant) {
     CUDA_TRY(cudaEventRecord(e->ev0, s), "cudaEventRecord");
     CUDA_TRY(launch_search_init(bp, kc, s), "search init kernel launch");
     if (variant == B40C_VARIANT_FUSED) {
@@ -606,7 +675,7 @@ extern "C" int b40c_problem_from_host(b40c_problem_t *p, int stream_from_host, i
             p->d_labels_alt = nullptr;
             p->labels_alt_cap = 0;
         }
-        if (p->mask_cap < size_t((nodes + 31) / 32) * 4) {
+        if (p->mask_cap < size_t((nodes + 31) / 32) * 4 + MASK_PAD_BYTES) {
             cudaFree(p->d_mask);
             p->d_mask = nullptr;
             p->mask_cap = 0;
@@ -629,18 +698,23 @@ extern "C" int b40c_problem_from_host(b40c_problem_t *p, int stream_from_host, i
             CUDA_TRY(cudaMalloc(&p->d_col, sizeof(int) * (size_t(edges) + 4)), "CsrProblem cudaMalloc d_column_indices");
             p->col_cap = size_t(edges) + 4;
         }
-        if (p->row_cap < size_t(nodes) + 1) {
+        // Row offsets padded with ROW_PAD entries: a bottom-up step stages 132
+        // offsets (whole 16-byte units) with one bulk copy.
+        if (p->row_cap < size_t(nodes) + 1 + ROW_PAD) {
             cudaFree(p->d_row_offsets);
             p->d_row_offsets = nullptr;
             p->row_cap = 0;
-            CUDA_TRY(cudaMalloc(&p->d_row_offsets, sizeof(int) * (size_t(nodes) + 1)), "CsrProblem cudaMalloc d_row_offsets");
-            p->row_cap = size_t(nodes) + 1;
+            CUDA_TRY(cudaMalloc(&p->d_row_offsets, sizeof(int) * (size_t(nodes) + 1 + ROW_PAD)),
+                     "CsrProblem cudaMalloc d_row_offsets");
+            p->row_cap = size_t(nodes) + 1 + ROW_PAD;
         }
         // The uploads are ordered on the problem's stream, ahead of the device
         // CSR check below (a plain cudaMemcpy from pageable memory may return
         // before its DMA lands, and the problem's stream does not wait for it).
         cudaStream_t s = problem_stream(p);
         CUDA_TRY(cudaMemsetAsync(p->d_col + edges, 0, 4 * sizeof(int), s), "cudaMemset column padding");
+        CUDA_TRY(cudaMemsetAsync(p->d_row_offsets + nodes + 1, 0, ROW_PAD * sizeof(int), s),
+                 "cudaMemset row-offset padding");
         if (edges)
             CUDA_TRY(cudaMemcpyAsync(p->d_col, h_col, sizeof(int) * size_t(edges), cudaMemcpyHostToDevice, s),
                      "CsrProblem cudaMemcpy d_column_indices");
@@ -677,8 +751,11 @@ static int problem_reset(b40c_problem *p, int frontier_type, double queue_sizing
     // ceil(nodes / 8) bytes as the reference (csr_problem.cuh:581-583), rounded to whole words.
     p->mask_bytes = size_t((p->nodes + 31) / 32) * 4;
     if (!p->d_mask) {
-        CUDA_TRY(cudaMalloc(&p->d_mask, p->mask_bytes), "CsrProblem cudaMalloc d_visited_mask");
-        p->mask_cap = p->mask_bytes;
+        // padded so that a bottom-up step's 16-byte bulk copy of its 4 words stays inside
+        CUDA_TRY(cudaMalloc(&p->d_mask, p->mask_bytes + MASK_PAD_BYTES), "CsrProblem cudaMalloc d_visited_mask");
+        CUDA_TRY(cudaMemsetAsync(reinterpret_cast<char *>(p->d_mask) + p->mask_bytes, 0, MASK_PAD_BYTES, s),
+                 "visited-mask padding");
+        p->mask_cap = p->mask_bytes + MASK_PAD_BYTES;
     }
     long long n = p->nodes, m = p->edges;
     long long want[2] = {0, 0}, wpred[2] = {0, 0};
@@ -1085,6 +1162,33 @@ extern "C" int b40c_enactor_level_log(b40c_enactor_t *e, int max_records, int64_
     return B40C_SUCCESS;
 }
 
+extern "C" int b40c_enactor_level_times(b40c_enactor_t *e, int max_records, int64_t *t_start_ns,
+                                        int64_t *t_work_end_ns, int *count) {
+    clear_error();
+    if (!e || !count || max_records < 0) return set_error(B40C_ERR_INVALID_VALUE, "invalid argument");
+    *count = 0;
+    if (!e->log_levels || !e->d_levels) return set_error(B40C_ERR_ILLEGAL_STATE, "level log not enabled");
+    if (e->h_ctr && !e->have_stats) {
+        int rc = finish_search(e);
+        if (rc) return rc;
+    }
+    std::vector<LevelRecord> h(LEVEL_LOG_CAP);
+    CUDA_TRY(cudaMemcpy(h.data(), e->d_levels, sizeof(LevelRecord) * LEVEL_LOG_CAP, cudaMemcpyDeviceToHost),
+             "level log copy");
+    int n = 0;
+    while (n < LEVEL_LOG_CAP && h[n].t_start != 0) {
+        n++;
+        if (h[n - 1].frontier == 0u && h[n - 1].chunks == 0u && h[n - 1].wchunks == 0u) break;
+    }
+    n = std::min(n, max_records);
+    for (int i = 0; i < n; i++) {
+        if (t_start_ns) t_start_ns[i] = (int64_t)h[i].t_start;
+        if (t_work_end_ns) t_work_end_ns[i] = (int64_t)h[i].t_work_end;
+    }
+    *count = n;
+    return B40C_SUCCESS;
+}
+
 extern "C" int b40c_enactor_set_direction_optimizing(b40c_enactor_t *e, int alpha, int beta) {
     clear_error();
     if (!e || alpha < 0 || beta < 0 || (alpha > 0 && beta == 0))
@@ -1100,6 +1204,20 @@ extern "C" int b40c_enactor_set_wait_limit_us(b40c_enactor_t *e, long long us) {
     clear_error();
     if (!e || us <= 0) return set_error(B40C_ERR_INVALID_VALUE, "invalid wait limit");
     e->wait_ns = (unsigned long long)us * 1000ull;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_set_bottom_up_staging(b40c_enactor_t *e, int enable) {
+    clear_error();
+    if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
+    e->stage_bu = enable != 0;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_set_l2_persistence(b40c_enactor_t *e, int what) {
+    clear_error();
+    if (!e || what < 0 || what > 2) return set_error(B40C_ERR_INVALID_VALUE, "L2 persistence: what is 0, 1 or 2");
+    e->l2_persist = what;
     return B40C_SUCCESS;
 }
 

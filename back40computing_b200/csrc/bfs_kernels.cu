@@ -58,7 +58,9 @@ struct WarpSmem {
     int gpred[MP ? WINDOW : 1];
     int surv[WINDOW];
     int obuf[OBUF];
+    int opred[MP ? OBUF : 1];    // owners staged with obuf (edge-frontier appends with predecessors)
     unsigned nbuf;
+    unsigned raw_n;              // edge-frontier entries this warp's expansions produced in the phase
     unsigned disc_n;             // direction-optimizing counts of this warp's discoveries
     unsigned long long disc_m;   // in the current level, added to the counters at its end
     unsigned bfound[4];          // bottom-up window scans: vertex 32j + lane found a parent
@@ -72,6 +74,14 @@ struct Smem {
     LevelCounts lc;
     unsigned flag;
 };
+
+// L2 policy of the column stream: evict_first when the column array is large
+// next to L2 (it then passes through once per search and must not push out
+// the mask, labels and row offsets); evict_normal when the whole graph can
+// stay in L2 between searches.
+__device__ __forceinline__ uint64_t column_policy(const BfsParams &p) {
+    return p.stream_col ? policy_evict_first() : policy_evict_normal();
+}
 
 // ---------------------------------------------------------------------------------------
 // Culling and enqueueing, 4 elements per thread
@@ -270,13 +280,6 @@ __device__ __forceinline__ unsigned place4(const BfsParams &p, int q_next, unsig
     return placed;
 }
 
-// One list per lane: place4 with list 0 only.
-template <int THREADS>
-__device__ __forceinline__ bool place1(const BfsParams &p, int q_next, bool has, int start, int len, int pred) {
-    const int st[4] = {start, 0, 0, 0}, ln[4] = {len, 0, 0, 0}, pr[4] = {pred, 0, 0, 0};
-    return place4<THREADS>(p, q_next, has ? 1u : 0u, st, ln, pr) & 1u;
-}
-
 // ---------------------------------------------------------------------------------------
 // Gather strategies
 // ---------------------------------------------------------------------------------------
@@ -296,7 +299,11 @@ __device__ __forceinline__ void gather_chunks(const BfsParams &p, const int4 *ta
     }
 }
 
-__device__ __forceinline__ int global_warp() { return int(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)); }
+// Warp w of the grid is warp w / gridDim.x of CTA w % gridDim.x: consecutive
+// work items (tiles, steps, runs) go to different CTAs, and so to different
+// SMs, so a level with few items still spreads over the whole GPU instead of
+// crowding the issue slots and memory pipes of the first few SMs.
+__device__ __forceinline__ int global_warp() { return int((threadIdx.x >> 5) * gridDim.x + blockIdx.x); }
 __device__ __forceinline__ int grid_warps() { return int(gridDim.x * (blockDim.x >> 5)); }
 
 // Warp chunk phase: warp w of the grid streams warp chunks w, w + W, ...
@@ -342,75 +349,179 @@ __device__ __forceinline__ void gather_chunk_tables(const BfsParams &p, const in
     if (e0 > s0) gather_list<32>(p.col, p.vec_end, s0, e0 - s0, ch.z, 0u, lane_id(), sink, pol);
 }
 
-// Warp- and scan-based gather of one list per lane (start, len, owner pred).
-// With POSITIONAL the warp first reserves room for all its lists in the output
-// queue with one atomicAdd on qlen_out (short lists first, then the others) and
-// the sink receives each element's position.
-template <bool MP, bool POSITIONAL, class Sink>
-__device__ __forceinline__ void warp_lists(const BfsParams &p, WarpSmem<MP> &ws, const Sink &sink, uint64_t pol,
-                                           int start, int len, int pred, unsigned *qlen_out) {
-    const int lane = lane_id();
-    const bool small = len < p.warp_th;
-    const int sl = small ? len : 0;
-    const int si = warp_inclusive_scan(sl);
-    const int small_total = __shfl_sync(FULL, si, 31);
-    const int small_excl = si - sl;
-    unsigned out = 0, small_base = 0;
-    if (POSITIONAL) {
-        const int ml = small ? 0 : len;
-        const int mi = warp_inclusive_scan(ml);
-        const unsigned need = unsigned(small_total) + unsigned(__shfl_sync(FULL, mi, 31));
-        unsigned base = 0;
-        if (need) {
-            if (lane == 0) {
-                base = atomicAdd(qlen_out, need);
-                if ((unsigned long long)base + need > (unsigned long long)p.qcap) {
-                    atomicOr(&p.ctr->error, ERR_OVERFLOW);
-                    base = 0xffffffffu;
-                }
-            }
-            base = __shfl_sync(FULL, base, 0);
-            if (base == 0xffffffffu) return;  // warp-uniform: output dropped on overflow
-        }
-        small_base = base;
-        out = small ? base + unsigned(small_excl) : base + unsigned(small_total) + unsigned(mi - ml);
-    }
-    // warp-based gather of lists >= warp_th
-    unsigned wm;
-    while ((wm = __ballot_sync(FULL, len >= p.warp_th)) != 0u) {
-        const int leader = __ffs(wm) - 1;
-        const int s = __shfl_sync(FULL, start, leader);
-        const int l = __shfl_sync(FULL, len, leader);
-        const int pv = __shfl_sync(FULL, pred, leader);
-        const unsigned o = __shfl_sync(FULL, out, leader);
-        if (lane == leader) len = 0;
-        gather_list<32>(p.col, p.vec_end, s, l, pv, o, lane, sink, pol);
-    }
-    // scan-based gather of the short lists through the warp's window
-    for (int base = 0; base < small_total; base += WINDOW) {
-        const int lo = max(small_excl, base), hi = min(small_excl + sl, base + WINDOW);
-        for (int j = lo; j < hi; j++) {
-            ws.gofs[j - base] = start + (j - small_excl);
-            if (MP) ws.gpred[j - base] = pred;
-        }
-        __syncwarp();
-        const int cnt = min(WINDOW, small_total - base);
-        const int k = lane * 4;
-        unsigned valid = 0;
-        int u[4], pv[4];
+// ---- window gathers of up to 4 lists per lane ------------------------------------------
+// The lists a warp holds (bit j of has marks list j of a lane: column entries
+// [st[j], st[j] + ln[j]), owner pr[j]) are laid out one after the other, list
+// 0 of every lane, then list 1, and so on (list_layout gives each list's first
+// position o[j] and returns the warp's total).  The warp streams that layout in
+// windows of WINDOW positions, 4 per lane (position 32m + lane of the window).
+// Each list that reaches into a window writes one segment record (its column
+// base relative to the window) and marks the position where it starts in a
+// bitmap; a position finds its list by counting the starts up to it.  Lists
+// of any length take the same path, consecutive lanes read consecutive column
+// entries, and a window costs one column load per lane and element whatever
+// the mix of lengths.
+
+__device__ __forceinline__ unsigned list_layout(unsigned has, const int (&ln)[4], int (&o)[4]) {
+    unsigned total = 0;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            u[j] = -1;
-            pv[j] = 0;
-            if (k + j < cnt) {
-                valid |= 1u << j;
-                u[j] = __ldg(p.col + ws.gofs[k + j]);
-                if (MP) pv[j] = ws.gpred[k + j];
+    for (int j = 0; j < 4; j++) {
+        const int l = ((has >> j) & 1u) ? ln[j] : 0;
+        const int incl = warp_inclusive_scan(l);
+        o[j] = int(total) + incl - l;
+        total += unsigned(__shfl_sync(FULL, incl, 31));
+    }
+    return total;
+}
+
+// Window [w0, w0 + WINDOW) of the layout: e[m] = the column index at window
+// position 32m + lane (own[m] its list's owner), for positions below cw =
+// min(WINDOW, total - w0); returns cw.  Ends with the warp's shared records
+// read, so the next window may rewrite them after a __syncwarp.
+template <bool MP>
+__device__ __forceinline__ int window_entries(WarpSmem<MP> &ws, unsigned has, const int (&st)[4],
+                                              const int (&ln)[4], const int (&pr)[4], const int (&o)[4],
+                                              unsigned w0, unsigned total, int (&e)[4], int (&own)[4]) {
+    const int lane = lane_id();
+    if (lane < 4) ws.segstart[lane] = 0u;
+    __syncwarp();
+    int nseg = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int l = ((has >> j) & 1u) ? ln[j] : 0;
+        const bool seg = l > 0 && o[j] < int(w0) + WINDOW && o[j] + l > int(w0);
+        const unsigned b = __ballot_sync(FULL, seg);
+        if (seg) {
+            const int k = nseg + __popc(b & lanemask_lt());
+            const int s0 = max(o[j], int(w0)) - int(w0);
+            ws.gofs[k] = st[j] - o[j] + int(w0);
+            if (MP) ws.gpred[k] = pr[j];
+            atomicOr(&ws.segstart[s0 >> 5], 1u << (s0 & 31));
+        }
+        nseg += __popc(b);
+    }
+    __syncwarp();
+    const int cw = min(WINDOW, int(total - w0));
+    unsigned sw[4];
+    int before[4];  // segment starts in the words before word m
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        sw[m] = ws.segstart[m];
+        before[m] = m ? before[m - 1] + __popc(sw[m - 1]) : 0;
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const int idx = m * 32 + lane;
+        const int k = before[m] + __popc(sw[m] & ((2u << lane) - 1u)) - 1;
+        e[m] = idx < cw ? ws.gofs[k] + idx : -1;
+        own[m] = (MP && idx < cw) ? ws.gpred[k] : 0;
+    }
+    return cw;
+}
+
+// Positional gather: one atomicAdd on qlen_out reserves room in q_out for every
+// entry of the warp's lists, which are then written at their layout positions
+// (the owners into pq_out when MP).  Called by all lanes together.
+template <bool MP>
+__device__ __forceinline__ void gather_positional4(const BfsParams &p, WarpSmem<MP> &ws, unsigned has,
+                                                   const int (&st)[4], const int (&ln)[4], const int (&pr)[4],
+                                                   int *q_out, int *pq_out, unsigned *qlen_out, uint64_t pol) {
+    int o[4];
+    const unsigned total = list_layout(has, ln, o);
+    if (total == 0u) return;  // warp-uniform
+    unsigned base = 0;
+    if (lane_id() == 0) {
+        base = atomicAdd(qlen_out, total);
+        if ((unsigned long long)base + total > (unsigned long long)p.qcap) {
+            atomicOr(&p.ctr->error, ERR_OVERFLOW);
+            base = 0xffffffffu;
+        }
+    }
+    base = __shfl_sync(FULL, base, 0);
+    if (base == 0xffffffffu) return;  // warp-uniform: output dropped on overflow
+    for (unsigned w0 = 0; w0 < total; w0 += WINDOW) {
+        int e[4], own[4], x[4];
+        window_entries<MP>(ws, has, st, ln, pr, o, w0, total, e, own);
+#pragma unroll
+        for (int m = 0; m < 4; m++) x[m] = e[m] >= 0 ? ldg_stream(p.col + e[m], pol) : 0;
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            if (e[m] >= 0) {
+                const unsigned pos = base + w0 + unsigned(m * 32) + lane_id();
+                q_out[pos] = x[m];
+                if (MP) pq_out[pos] = own[m];
             }
         }
-        sink(valid, u, pv, small_base + unsigned(base + k));
         __syncwarp();
     }
+}
+
+// Sink-based gather: every window's elements go to sink (valid bits, 4
+// elements and their owners per lane).  Called by all lanes together.
+template <bool MP, class Sink>
+__device__ __forceinline__ void gather_windows4(const BfsParams &p, WarpSmem<MP> &ws, unsigned has,
+                                                const int (&st)[4], const int (&ln)[4], const int (&pr)[4],
+                                                const Sink &sink, uint64_t pol) {
+    int o[4];
+    const unsigned total = list_layout(has, ln, o);
+    for (unsigned w0 = 0; w0 < total; w0 += WINDOW) {
+        int e[4], own[4], x[4];
+        window_entries<MP>(ws, has, st, ln, pr, o, w0, total, e, own);
+        unsigned valid = 0;
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            x[m] = e[m] >= 0 ? ldg_stream(p.col + e[m], pol) : -1;
+            if (e[m] >= 0) valid |= 1u << m;
+        }
+        __syncwarp();
+        sink(valid, x, own, 0u);
+    }
+}
+
+// Frontier vertices per lane of a warp tile: 4 (tiles of WINDOW vertices, row
+// ranges and lists of four vertices per lane in flight together) once a level
+// has at least two such tiles per warp of the grid, else 1 (tiles of 32), so
+// that a small level still gives every warp of the grid a tile.
+__device__ __forceinline__ unsigned vertices_per_lane(unsigned L) {
+    return (unsigned long long)L >= 2ull * WINDOW * unsigned(grid_warps()) ? 4u : 1u;
+}
+
+// Loads the frontier vertices of warp tile t (per vertices per lane, tile
+// size 32 * per) from q_in; bit j of the result marks v[j].
+__device__ __forceinline__ unsigned load_tile(const int *q_in, unsigned L, unsigned t, unsigned per, int (&v)[4]) {
+    unsigned sel = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const unsigned idx = t * 32u * per + unsigned(j) * 32u + lane_id();
+        v[j] = -1;
+        if (unsigned(j) < per && idx < L) {
+            v[j] = ld_cg(q_in + idx);
+            sel |= 1u << j;
+        }
+    }
+    return sel;
+}
+
+// Row ranges of up to 4 vertices per lane (bit j of sel marks v[j]): every
+// load is issued before any is used (an unselected slot reads row 0, a line
+// the warp shares).  Sets has to the selected vertices with edges.
+__device__ __forceinline__ unsigned row_ranges4(const BfsParams &p, unsigned sel, const int (&v)[4], int (&st)[4],
+                                                int (&ln)[4]) {
+    int r0[4], r1[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int vv = ((sel >> j) & 1u) ? v[j] : 0;
+        r0[j] = __ldg(p.row_offsets + vv);
+        r1[j] = __ldg(p.row_offsets + vv + 1);
+    }
+    unsigned has = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        st[j] = r0[j];
+        ln[j] = ((sel >> j) & 1u) ? r1[j] - r0[j] : 0;
+        if (ln[j] > 0) has |= 1u << j;
+    }
+    return has;
 }
 
 // Warp tiles handed out per atomic: several when there are many per warp.
@@ -437,6 +548,142 @@ __device__ __forceinline__ unsigned next_run(unsigned nruns, unsigned *steal) {
 // warp together with up to 4 elements per lane; bit j of valid marks u[j];
 // output positions (edge-frontier queues) are out0 + j.
 // ---------------------------------------------------------------------------------------
+
+// Edge-frontier appends with their owners (predecessor labels): as stage4,
+// with the owners staged beside the ids and written to pq at the same
+// positions.  Called by all lanes together.
+template <bool MP>
+__device__ __forceinline__ void pair_flush(WarpSmem<MP> &ws, unsigned n, int *q, int *pq, unsigned *qlen,
+                                           long long qcap, unsigned *err) {
+    unsigned base = 0;
+    if (lane_id() == 0) base = atomicAdd(qlen, n);
+    base = __shfl_sync(FULL, base, 0);
+    for (unsigned i = lane_id(); i < n; i += 32) {
+        const unsigned long long pos = (unsigned long long)base + i;
+        if (pos < (unsigned long long)qcap) {
+            q[pos] = ws.obuf[i];
+            if (MP) pq[pos] = ws.opred[i];
+        } else {
+            atomicOr(err, ERR_OVERFLOW);
+        }
+    }
+    __syncwarp();
+}
+
+template <bool MP>
+__device__ __forceinline__ void stage_pairs4(WarpSmem<MP> &ws, unsigned flags, const int (&u)[4], const int (&pr)[4],
+                                             int *q, int *pq, unsigned *qlen, long long qcap, unsigned *err) {
+    const unsigned lt = lanemask_lt();
+    unsigned total = 0, pre[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        unsigned b = __ballot_sync(FULL, (flags >> j) & 1u);
+        pre[j] = total + __popc(b & lt);
+        total += __popc(b);
+    }
+    if (total == 0u) return;  // warp-uniform
+    unsigned n = ws.nbuf;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if ((flags >> j) & 1u) {
+            ws.obuf[n + pre[j]] = u[j];
+            if (MP) ws.opred[n + pre[j]] = pr[j];
+        }
+    }
+    n += total;
+    __syncwarp();
+    if (n > unsigned(OBUF - WINDOW)) {
+        pair_flush(ws, n, q, pq, qlen, qcap, err);
+        n = 0;
+    }
+    if (lane_id() == 0) ws.nbuf = n;
+    __syncwarp();
+}
+
+// Adds the lengths of a lane's lists (bit j of has marks ln[j]) to the warp's
+// raw edge-frontier count of the phase; flush_raw adds the warp's count to
+// the counters once, at the phase's end.
+__device__ __forceinline__ void count_raw(unsigned *raw_n, unsigned has, const int (&ln)[4]) {
+    unsigned l = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) l += ((has >> j) & 1u) ? unsigned(ln[j]) : 0u;
+    l = __reduce_add_sync(FULL, l);
+    if (lane_id() == 0) *raw_n += l;
+}
+template <bool MP>
+__device__ __forceinline__ void flush_raw(const BfsParams &p, WarpSmem<MP> &ws, int q) {
+    if (lane_id() == 0) {
+        if (ws.raw_n) atomicAdd(&p.ctr->raw[q & 3], ws.raw_n);
+        ws.raw_n = 0u;
+    }
+    __syncwarp();
+}
+
+// Whether a two-phase expand culls while it gathers, by the edge frontier raw
+// its level started from: on large levels (more than 4 entries per thread of
+// the grid, the hybrid's saturation point) most gathered neighbours are
+// already visited -- the contract phase before the barrier has set every bit
+// of the level -- and dropping them early saves their queue traffic and
+// contraction; on small levels the extra probe only lengthens the level's
+// dependent chain.
+__device__ __forceinline__ bool gather_cull(unsigned raw) {
+    return (unsigned long long)raw > 4ull * blockDim.x * gridDim.x;
+}
+
+// The gather-time cull of the edge-frontier strategies: a gathered neighbour
+// whose visited bit is already set (seen in the CTA's history cache of mask
+// words, else by one L2 probe of the mask) can never be contracted, so it is
+// dropped instead of being written to the next edge frontier, read back and
+// culled there.  The bit is only read here; the next phase's contraction
+// still claims every remaining vertex with atomicOr.  Entries outside [0,
+// nodes) raise ERR_BAD_VERTEX here, as contraction would.
+template <int THREADS, bool MP>
+struct FilterSink {
+    const BfsParams &p;
+    Smem<THREADS, MP> &sm;
+    int *q_out;
+    int *pq_out;
+    unsigned *qlen_out;
+
+    __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&own)[4],
+                                               unsigned) const {
+        const bool history = p.cull_flags & CULL_HISTORY;
+        unsigned w[4], bit[4], m[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            bool ok = (valid >> j) & 1u;
+            if (ok && (unsigned)u[j] >= (unsigned)p.nodes) {
+                atomicOr(&p.ctr->error, ERR_BAD_VERTEX);
+                valid &= ~(1u << j);
+                ok = false;
+            }
+            w[j] = ok ? (unsigned)u[j] >> 5 : 0u;
+            bit[j] = 1u << ((unsigned)u[j] & 31u);
+            if (ok && history) {
+                const unsigned long long e = sm.vcache[vcache_slot(w[j])];
+                if (unsigned(e >> 32) == w[j] && (unsigned(e) & bit[j])) valid &= ~(1u << j);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) m[j] = ((valid >> j) & 1u) ? ld_cg(p.mask + w[j]) : 0u;
+        unsigned keep = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if ((valid >> j) & 1u) {
+                if (!(m[j] & bit[j])) keep |= 1u << j;
+                if (history) sm.vcache[vcache_slot(w[j])] = ((unsigned long long)w[j] << 32) | m[j];
+            }
+        }
+        stage_pairs4(sm.w[threadIdx.x >> 5], keep, u, own, q_out, pq_out, qlen_out, p.qcap, &p.ctr->error);
+    }
+    __device__ __forceinline__ void drain() const {
+        WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
+        const unsigned n = ws.nbuf;
+        if (n) pair_flush(ws, n, q_out, pq_out, qlen_out, p.qcap, &p.ctr->error);
+        if (lane_id() == 0) ws.nbuf = 0;
+        __syncwarp();
+    }
+};
 
 // Direction-optimizing counts: a warp sums its discoveries (n vertices with
 // deg edges per lane) in shared memory during a level and adds them to the
@@ -502,29 +749,13 @@ struct DiscoverSink {
     }
 };
 
-// Edge-frontier output (contract-expand / two-phase expand): neighbours are
-// written at reserved positions, duplicates kept.
-template <bool MP>
-struct PositionSink {
-    int *q_out;
-    int *pq_out;
-    __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
-                                               unsigned out0) const {
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if ((valid >> j) & 1u) {
-                q_out[out0 + j] = u[j];
-                if (MP) pq_out[out0 + j] = pred[j];
-            }
-        }
-    }
-};
-
 // Contract-expand: cull and label the edge-frontier elements (label it,
 // contract_expand_atomic/cta.cuh:264-304), then expand the survivors at once:
 // long lists become CTA or warp chunks of the next level (contracted from the
-// column array there), short ones are copied into the next edge frontier by a
-// scan-based gather.
+// column array there), the others are copied into the next edge frontier by
+// one window gather of all the warp's survivors.  (No gather-time cull here:
+// the neighbours gathered in a level are mostly vertices that other warps
+// contract in the same level, whose bits are not set yet.)
 template <int THREADS, bool MP>
 struct ContractExpandSink {
     const BfsParams &p;
@@ -536,37 +767,24 @@ struct ContractExpandSink {
     __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
                                                unsigned) const {
         const unsigned surv = cull4<THREADS, MP>(p, sm, valid, u);
+        if (!__any_sync(FULL, surv != 0u)) return;
+        // The survivors' row ranges (all loads in flight together), then their
+        // lists: long ones to the next phase's chunk tables, the rest gathered
+        // by the warp into the next edge frontier at once.
+        int st[4], ln[4];
+        const unsigned has = row_ranges4(p, surv, u, st, ln);
 #pragma unroll
         for (int j = 0; j < 4; j++)
             if ((surv >> j) & 1u) p.labels[u[j]] = MP ? pred[j] : it;
-        // Compact the warp's survivors into its window.
         WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
-        const unsigned lt = lanemask_lt();
-        unsigned total = 0, pre[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            unsigned b = __ballot_sync(FULL, (surv >> j) & 1u);
-            pre[j] = total + __popc(b & lt);
-            total += __popc(b);
-        }
-        if (total == 0u) return;
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-            if ((surv >> j) & 1u) ws.surv[pre[j]] = u[j];
-        __syncwarp();
+        count_raw(&ws.raw_n, has, ln);
+        const unsigned placed = place4<THREADS>(p, q + 1, has, st, ln, u);
         const int nq = (q + 1) & 1;
-        PositionSink<MP> out{p.queue[nq], p.pred_queue[nq]};
-        for (unsigned g = 0; g < total; g += 32) {
-            int v = -1, start = 0, len = 0;
-            if (g + lane_id() < total) {
-                v = ws.surv[g + lane_id()];
-                row_range(p, v, start, len);
-            }
-            if (place1<THREADS>(p, q + 1, len > 0, start, len, v)) len = 0;
-            warp_lists<MP, true>(p, ws, out, pol, start, len, v, &p.ctr->qlen[(q + 1) & 3]);
-        }
-        __syncwarp();
+        gather_positional4<MP>(p, ws, has & ~placed, st, ln, u, p.queue[nq], p.pred_queue[nq],
+                               &p.ctr->qlen[(q + 1) & 3], pol);
     }
+    // Adds the warp's raw count to the counters; every warp calls it at the phase's end.
+    __device__ __forceinline__ void drain() const { flush_raw(p, sm.w[threadIdx.x >> 5], q + 1); }
 };
 
 // Two-phase contract: cull and label (iteration it), then append the survivors
@@ -598,6 +816,9 @@ struct ContractSink {
 // ---------------------------------------------------------------------------------------
 
 // Expand-contract level it: vertex frontier -> discovered vertices labelled it+1.
+// Warp tiles of frontier vertices (vertices_per_lane): their row ranges are
+// loaded together and their lists streamed by one window gather into the
+// discovery sink.
 template <int THREADS, bool MP>
 __device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, unsigned nwch, Smem<THREADS, MP> &sm,
                          uint64_t pol) {
@@ -607,19 +828,17 @@ __device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, u
     gather_chunk_tables<THREADS>(p, p.chunks[it & 1], nch, p.wchunks[it & 1], nwch, sink, pol);
     WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
     const int *q_in = p.queue[it & 1];
-    const unsigned ntiles = (L + 31) / 32;
+    const unsigned per = vertices_per_lane(L);
+    const unsigned ntiles = (L + 32u * per - 1) / (32u * per);
     const unsigned grab = tile_grab(ntiles);
     const unsigned nruns = (ntiles + grab - 1) / grab;
     for (unsigned r = global_warp(); r < nruns; r = next_run(nruns, &c->steal[it & 3])) {
         const unsigned t0 = r * grab;
         for (unsigned t = t0; t < t0 + grab && t < ntiles; t++) {
-            const unsigned idx = t * 32 + lane_id();
-            int v = -1, start = 0, len = 0;
-            if (idx < L) {
-                v = ld_cg(q_in + idx);
-                row_range(p, v, start, len);
-            }
-            warp_lists<MP, false>(p, ws, sink, pol, start, len, v, nullptr);
+            int v[4], st[4], ln[4];
+            const unsigned sel = load_tile(q_in, L, t, per, v);
+            const unsigned has = row_ranges4(p, sel, v, st, ln);
+            gather_windows4<MP>(p, ws, has, st, ln, v, sink, pol);
         }
     }
     sink.drain();
@@ -644,15 +863,29 @@ __device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, u
 constexpr int BU_WORDS = 4;  // = the 4 lists per lane that place4 and stage4 take
 static_assert(BU_WORDS == 4, "bottom-up steps hand 4 vertices per lane to place4 / stage4");
 
+// A bottom-up step's inputs staged in shared memory: the row offsets of its
+// 128 vertices (129 used, whole 16-byte units copied), their heaviest-neighbour
+// keys and the step's 4 visited-mask words.  Each warp keeps two, so that the
+// bulk copies of its next step run while it works on the current one.
+struct alignas(16) BuStage {
+    int off[32 * BU_WORDS + 4];
+    unsigned long long key[32 * BU_WORDS];
+    unsigned mask[BU_WORDS];
+};
+struct alignas(16) WarpStage {
+    BuStage buf[2];
+    unsigned long long bar[2];  // mbarriers: bar[b] completes when buf[b] has landed
+};
+
 // One bottom-up step: visited-mask words w0 .. w0 + BU_WORDS - 1.
 template <int THREADS, bool MP>
 __device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0, unsigned nwords, WarpSmem<MP> &ws,
-                                        int *q_out, unsigned *qlen_out) {
+                                        int *q_out, unsigned *qlen_out, const BuStage *sg) {
     Counters *c = p.ctr;
     const int lane = lane_id();
     unsigned mw[BU_WORDS];
 #pragma unroll
-    for (int j = 0; j < BU_WORDS; j++) mw[j] = w0 + j < nwords ? ld_cg(p.mask + w0 + j) : FULL;
+    for (int j = 0; j < BU_WORDS; j++) mw[j] = w0 + j < nwords ? (sg ? sg->mask[j] : ld_cg(p.mask + w0 + j)) : FULL;
     bool any_open = false;
 #pragma unroll
     for (int j = 0; j < BU_WORDS; j++) any_open |= mw[j] != FULL;
@@ -671,10 +904,16 @@ __device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0,
     for (int j = 0; j < BU_WORDS; j++) {
         v[j] = int((w0 + j) * 32u) + lane;
         if (v[j] < p.nodes && !((mw[j] >> lane) & 1u)) open |= 1u << j;
-        const int vv = ((open >> j) & 1u) ? v[j] : 0;
-        r0[j] = __ldg(p.row_offsets + vv);
-        r1[j] = __ldg(p.row_offsets + vv + 1);
-        hk[j] = p.heavy ? __ldg(p.heavy + vv) : 0ull;
+        if (sg) {  // staged: the step's slice, read from shared memory
+            r0[j] = sg->off[j * 32 + lane];
+            r1[j] = sg->off[j * 32 + lane + 1];
+            hk[j] = p.heavy ? sg->key[j * 32 + lane] : 0ull;
+        } else {
+            const int vv = ((open >> j) & 1u) ? v[j] : 0;
+            r0[j] = __ldg(p.row_offsets + vv);
+            r1[j] = __ldg(p.row_offsets + vv + 1);
+            hk[j] = p.heavy ? __ldg(p.heavy + vv) : 0ull;
+        }
     }
 #pragma unroll
     for (int j = 0; j < BU_WORDS; j++) {
@@ -846,9 +1085,50 @@ __device__ __forceinline__ void snapshot_mask(const BfsParams &p) {
         p.mask_snap[w] = ld_cg(p.mask + w);
 }
 
-// open: an estimate of the vertices still unvisited.
+// Issues the bulk copies of bottom-up step `step` into stage buffer b (lane 0
+// of the warp).  Copy sizes are whole 16-byte units, clamped to the padded
+// ends of the arrays (ROW_PAD, HEAVY_PAD, MASK_PAD_BYTES).  The mask words
+// were written by generic stores in earlier levels; the proxy fence orders
+// those writes, which the level's grid barrier made visible to this thread,
+// before the bulk reads.  Within a bottom-up level no other step writes the
+// step's words.
+__device__ __forceinline__ void bu_prefetch(const BfsParams &p, unsigned step, WarpStage *stg, int b) {
+    if (lane_id() == 0) {
+        const long long v0 = (long long)step * (32 * BU_WORDS);
+        const long long n = p.nodes;
+        const unsigned offs = unsigned(min((long long)(32 * BU_WORDS + 4), n + 1 + ROW_PAD - v0)) & ~3u;
+        const unsigned keys = p.heavy ? unsigned(min((long long)(32 * BU_WORDS), n + HEAVY_PAD - v0)) & ~1u : 0u;
+        fence_proxy_async_global();
+        mbar_arrive_expect_tx(&stg->bar[b], offs * 4u + keys * 8u + 16u);
+        bulk_copy_g2s(stg->buf[b].off, p.row_offsets + v0, offs * 4u, &stg->bar[b]);
+        if (keys) bulk_copy_g2s(stg->buf[b].key, p.heavy + v0, keys * 8u, &stg->bar[b]);
+        bulk_copy_g2s(stg->buf[b].mask, p.mask + step * BU_WORDS, 16u, &stg->bar[b]);
+    }
+}
+
+// Waits, with the grid barrier's time limit, for stage buffer b's copies;
+// phase holds the parity each buffer completes next.  Returns false, with
+// ERR_BARRIER_TIMEOUT raised, when the limit passed (warp-uniform).
+__device__ __forceinline__ bool bu_stage_wait(const BfsParams &p, WarpStage *stg, int b, unsigned &phase) {
+    const unsigned parity = (phase >> b) & 1u;
+    bool ok = mbar_try_wait(&stg->bar[b], parity);
+    if (!ok) {
+        const unsigned long long t0 = globaltimer_ns();
+        while (!(ok = mbar_try_wait(&stg->bar[b], parity)))
+            if (globaltimer_ns() - t0 > p.wait_ns) break;
+    }
+    ok = __all_sync(FULL, ok);
+    if (ok) phase ^= 1u << b;
+    else if (lane_id() == 0) atomicOr(&p.ctr->error, ERR_BARRIER_TIMEOUT);
+    return ok;
+}
+
+// open: an estimate of the vertices still unvisited.  stg (a warp's stage
+// buffers, or NULL) stages each step's row offsets, keys and mask words one
+// step ahead with bulk copies; phase is their mbarriers' parity state.
 template <int THREADS, bool MP>
-__device__ void bu_level(const BfsParams &p, int it, Smem<THREADS, MP> &sm, unsigned open) {
+__device__ void bu_level(const BfsParams &p, int it, Smem<THREADS, MP> &sm, unsigned open, WarpStage *stg,
+                         unsigned &phase) {
     Counters *c = p.ctr;
     int *q_out = p.queue[(it + 1) & 1];
     unsigned *qlen_out = &c->qlen[(it + 1) & 3];
@@ -863,11 +1143,44 @@ __device__ void bu_level(const BfsParams &p, int it, Smem<THREADS, MP> &sm, unsi
     // atomic's latency.  Once fewer than a quarter are open, most steps are
     // cheap and alike, and a static interleave spares the counter its atomics.
     const bool dynamic = nsteps > W && (unsigned long long)open * 4ull > (unsigned long long)p.nodes;
-    for (unsigned step = global_warp(); step < nsteps;) {
-        unsigned nxt = 0;
-        if (dynamic && lane_id() == 0) nxt = atomicAdd(&c->steal[it & 3], 1u);
-        bu_step<THREADS, MP>(p, it, step * BU_WORDS, nwords, ws, q_out, qlen_out);
-        step = dynamic ? W + __shfl_sync(FULL, nxt, 0) : step + W;
+    if (!stg) {
+        for (unsigned step = global_warp(); step < nsteps;) {
+            unsigned nxt = 0;
+            if (dynamic && lane_id() == 0) nxt = atomicAdd(&c->steal[it & 3], 1u);
+            bu_step<THREADS, MP>(p, it, step * BU_WORDS, nwords, ws, q_out, qlen_out, nullptr);
+            step = dynamic ? W + __shfl_sync(FULL, nxt, 0) : step + W;
+        }
+    } else {
+        // Two steps in hand: cur (being worked on, in buf b) and nxt (its
+        // copies in flight into buf b ^ 1).  The step after nxt is asked for
+        // while cur runs and staged into buf b once cur is done.
+        unsigned cur = global_warp(), nxt = nsteps;
+        int b = 0;
+        if (cur < nsteps) {
+            bu_prefetch(p, cur, stg, 0);
+            unsigned t = 0;
+            if (dynamic && lane_id() == 0) t = atomicAdd(&c->steal[it & 3], 1u);
+            nxt = dynamic ? W + __shfl_sync(FULL, t, 0) : cur + W;
+            if (nxt < nsteps) bu_prefetch(p, nxt, stg, 1);
+        }
+        while (cur < nsteps) {
+            unsigned t = 0;
+            const bool more = nxt < nsteps;
+            if (more && dynamic && lane_id() == 0) t = atomicAdd(&c->steal[it & 3], 1u);
+            if (!bu_stage_wait(p, stg, b, phase)) {
+                // Abandon the level: wait (bounded again) for the copies still
+                // in flight into the other buffer, then leave.
+                if (more) bu_stage_wait(p, stg, b ^ 1, phase);
+                break;
+            }
+            bu_step<THREADS, MP>(p, it, cur * BU_WORDS, nwords, ws, q_out, qlen_out, &stg->buf[b]);
+            unsigned nxt2 = nsteps;
+            if (more) nxt2 = dynamic ? W + __shfl_sync(FULL, t, 0) : nxt + W;
+            if (nxt2 < nsteps) bu_prefetch(p, nxt2, stg, b);
+            cur = nxt;
+            nxt = nxt2;
+            b ^= 1;
+        }
     }
     stage_drain(ws, q_out, qlen_out, p.qcap, &c->error);
     flush_discovered(p, ws, it + 1);
@@ -905,6 +1218,7 @@ __device__ void ce_level(const BfsParams &p, int it, int q, unsigned L, unsigned
     ContractExpandSink<THREADS, MP> sink{p, sm, it, q, pol};
     gather_chunk_tables<THREADS>(p, p.chunks[q & 1], nch, p.wchunks[q & 1], nwch, sink, pol);
     edge_tiles<MP>(p.queue[q & 1], p.pred_queue[q & 1], L, sink);
+    sink.drain();
 }
 
 // Two-phase contract, phase qi = 2 * it.
@@ -917,30 +1231,38 @@ __device__ void tp_contract(const BfsParams &p, int it, int qi, unsigned L, unsi
     sink.drain();
 }
 
-// Two-phase expand, phase qi = 2 * it + 1 (two_phase/expand_atomic/cta.cuh:606-719).
+// Two-phase expand, phase qi = 2 * it + 1 (two_phase/expand_atomic/cta.cuh:606-719):
+// warp tiles of frontier vertices (vertices_per_lane); long lists become
+// chunks of the next phase, the others are streamed by one window gather per
+// tile through the gather-time cull into the next edge frontier.
 template <int THREADS, bool MP>
-__device__ void tp_expand(const BfsParams &p, int qi, unsigned L, Smem<THREADS, MP> &sm, uint64_t pol) {
+__device__ void tp_expand(const BfsParams &p, int qi, unsigned L, bool cull, Smem<THREADS, MP> &sm, uint64_t pol) {
     Counters *c = p.ctr;
     const int nq = (qi + 1) & 1;
-    PositionSink<MP> out{p.queue[nq], p.pred_queue[nq]};
     WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
+    const FilterSink<THREADS, MP> out{p, sm, p.queue[nq], p.pred_queue[nq], &c->qlen[(qi + 1) & 3]};
     const int *q_in = p.queue[qi & 1];
-    const unsigned ntiles = (L + 31) / 32;
+    const unsigned per = vertices_per_lane(L);
+    const unsigned ntiles = (L + 32u * per - 1) / (32u * per);
     const unsigned grab = tile_grab(ntiles);
     const unsigned nruns = (ntiles + grab - 1) / grab;
     for (unsigned r = global_warp(); r < nruns; r = next_run(nruns, &c->steal[qi & 3])) {
         const unsigned t0 = r * grab;
         for (unsigned t = t0; t < t0 + grab && t < ntiles; t++) {
-            const unsigned idx = t * 32 + lane_id();
-            int v = -1, start = 0, len = 0;
-            if (idx < L) {
-                v = ld_cg(q_in + idx);
-                row_range(p, v, start, len);
-            }
-            if (place1<THREADS>(p, qi + 1, len > 0, start, len, v)) len = 0;
-            warp_lists<MP, true>(p, ws, out, pol, start, len, v, &c->qlen[(qi + 1) & 3]);
+            int v[4], st[4], ln[4];
+            const unsigned sel = load_tile(q_in, L, t, per, v);
+            const unsigned has = row_ranges4(p, sel, v, st, ln);
+            count_raw(&ws.raw_n, has, ln);
+            const unsigned placed = place4<THREADS>(p, qi + 1, has, st, ln, v);
+            if (cull)
+                gather_windows4<MP>(p, ws, has & ~placed, st, ln, v, out, pol);
+            else
+                gather_positional4<MP>(p, ws, has & ~placed, st, ln, v, p.queue[nq], p.pred_queue[nq],
+                                       &c->qlen[(qi + 1) & 3], pol);
         }
     }
+    out.drain();
+    flush_raw(p, ws, qi + 1);
 }
 
 // Ring housekeeping for phase q: the entries phase q+1 writes start at zero.
@@ -949,6 +1271,7 @@ __device__ __forceinline__ void ring_prepare(Counters *c, int q) {
     c->qlen[(q + 2) & 3] = 0u;
     c->big[(q + 2) & 3] = 0u;
     c->wch[(q + 2) & 3] = 0u;
+    c->raw[(q + 2) & 3] = 0u;
     c->nf[(q + 2) & 3] = 0u;
     c->mf[(q + 2) & 3] = 0ull;
     c->steal[(q + 1) & 3] = 0u;
@@ -967,10 +1290,20 @@ __device__ __forceinline__ void log_phase(const BfsParams &p, int idx, unsigned 
     }
 }
 
+// Level log: the time the last CTA finished phase idx's work, taken when every
+// warp of the CTA is done (before the phase's grid barrier).
+__device__ __forceinline__ void log_work_end(const BfsParams &p, int idx) {
+    if (p.levels && idx < p.level_cap) {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicMax(&p.levels[idx].t_work_end, globaltimer_ns());
+    }
+}
+
 template <int THREADS, bool MP>
 __device__ __forceinline__ void init_hist(Smem<THREADS, MP> &sm, unsigned flags) {
     if (lane_id() == 0) {
         sm.w[threadIdx.x >> 5].nbuf = 0;
+        sm.w[threadIdx.x >> 5].raw_n = 0;
         sm.w[threadIdx.x >> 5].disc_n = 0;
         sm.w[threadIdx.x >> 5].disc_m = 0;
     }
@@ -1025,6 +1358,7 @@ __global__ void search_init_kernel(BfsParams p, int strategy, int mark_pred, int
     for (int i = threadIdx.x; i < WORDS; i += blockDim.x) w[i] = 0u;
     __syncthreads();
     if (threadIdx.x != 0) return;
+    c->raw[0] = 1u;  // the first edge frontier is the source
     if (strategy == STRATEGY_EXPAND_CONTRACT) {
         p.labels[p.src] = mark_pred ? -2 : 0;
         p.mask[unsigned(p.src) >> 5] |= 1u << (unsigned(p.src) & 31u);
@@ -1109,11 +1443,41 @@ __device__ __forceinline__ LevelCounts read_counts(Counters *c, int q, bool dir,
     return sm.lc;
 }
 
+// Dynamic shared memory of the expand-contract kernel: Smem, then one
+// WarpStage per warp when they fit without lowering the kernel's occupancy
+// (MIN_BLOCKS CTAs per SM in the SM's 228 KB, 1 KB reserved per CTA).
+template <int THREADS, bool MP>
+__host__ __device__ constexpr size_t ec_stage_offset() { return (sizeof(Smem<THREADS, MP>) + 15) & ~size_t(15); }
+template <int THREADS, bool MP>
+__host__ __device__ constexpr bool stage_fits() {
+    return (ec_stage_offset<THREADS, MP>() + sizeof(WarpStage) * (THREADS / 32) + 1024) * MIN_BLOCKS(THREADS) <=
+           228u * 1024u;
+}
+template <int THREADS, bool MP>
+__host__ __device__ constexpr size_t ec_smem_bytes() {
+    return stage_fits<THREADS, MP>() ? ec_stage_offset<THREADS, MP>() + sizeof(WarpStage) * (THREADS / 32)
+                                     : sizeof(Smem<THREADS, MP>);
+}
+
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(BfsParams p) {
     Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
-    const uint64_t pol = policy_evict_first();
+    WarpStage *stg = nullptr;  // this warp's bottom-up stage buffers
+    unsigned phase = 0;        // parity their mbarriers complete next
+    if constexpr (stage_fits<THREADS, MP>()) {
+        if (p.stage_bu) {
+            extern __shared__ __align__(128) unsigned char dyn_smem[];
+            stg = reinterpret_cast<WarpStage *>(dyn_smem + ec_stage_offset<THREADS, MP>()) + (threadIdx.x >> 5);
+            if (lane_id() == 0) {
+                mbar_init(&stg->bar[0], 1u);
+                mbar_init(&stg->bar[1], 1u);
+                mbar_init_fence();
+            }
+            __syncwarp();
+        }
+    }
+    const uint64_t pol = column_policy(p);
     Counters *c = p.ctr;
     DirectionChoice dir;
     BusyClock clk;
@@ -1137,11 +1501,12 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
                 if (!grid_barrier(c, p.wait_ns, &sm.flag)) break;
             }
             const unsigned done = dir.visited + lc.zmarked;
-            bu_level<THREADS, MP>(p, it, sm, done < unsigned(p.nodes) ? unsigned(p.nodes) - done : 0u);
+            bu_level<THREADS, MP>(p, it, sm, done < unsigned(p.nodes) ? unsigned(p.nodes) - done : 0u, stg, phase);
         } else {
             ec_level<THREADS, MP>(p, it, L, nch, nw, sm, pol);
         }
         clk.stop(p);
+        log_work_end(p, it);
         if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, it + 1, dcounts))) break;
         lc = sm.lc;
         it++;
@@ -1154,7 +1519,7 @@ template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(BfsParams p) {
     Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
-    const uint64_t pol = policy_evict_first();
+    const uint64_t pol = column_policy(p);
     Counters *c = p.ctr;
     BusyClock clk;
     int it = 0;
@@ -1162,14 +1527,17 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
     for (;;) {
         clk.start(p);
         const unsigned L = lc.L, nch = lc.nch, nw = lc.nw;
-        if (stop_level_loop(p, it, L + nch + nw)) break;
+        // raw: the edge frontier before the gather-time cull, so the loop runs
+        // (and counts) the levels the reference runs, the last one empty here
+        if (stop_level_loop(p, it, L + nch + nw + lc.raw)) break;
         if (leader()) {
             ring_prepare(c, it);
-            c->total_queued += L;
-            log_phase(p, it, L, nch, nw);
+            c->total_queued += lc.raw;
+            log_phase(p, it, lc.raw, nch, nw);
         }
         ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, pol);
         clk.stop(p);
+        log_work_end(p, it);
         if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, it + 1, false))) break;
         lc = sm.lc;
         it++;
@@ -1186,7 +1554,7 @@ template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(BfsParams p) {
     Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
-    const uint64_t pol = policy_evict_first();
+    const uint64_t pol = column_policy(p);
     Counters *c = p.ctr;
     BusyClock clk;
     int it = 0, qi = 0;
@@ -1195,14 +1563,16 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
         clk.start(p);
         unsigned L = lc.L;
         const unsigned nch = lc.nch, nw = lc.nw;
-        if (stop_level_loop(p, it, L + nch + nw)) break;
+        if (stop_level_loop(p, it, L + nch + nw + lc.raw)) break;
+        const bool cull = gather_cull(lc.raw);
         if (leader()) {
             ring_prepare(c, qi);
-            c->total_queued += L;
-            log_phase(p, qi, L, nch, nw);
+            c->total_queued += lc.raw;
+            log_phase(p, qi, lc.raw, nch, nw);
         }
         tp_contract<THREADS, MP>(p, it, qi, L, nch, nw, sm, pol);
         clk.stop(p);
+        log_work_end(p, qi);
         if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, qi + 1, false))) break;
         clk.start(p);
         qi++;
@@ -1212,8 +1582,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
             ring_prepare(c, qi);
             log_phase(p, qi, L, 0u, 0u);
         }
-        tp_expand<THREADS, MP>(p, qi, L, sm, pol);
+        tp_expand<THREADS, MP>(p, qi, L, cull, sm, pol);
         clk.stop(p);
+        log_work_end(p, qi);
         if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, qi + 1, false))) break;
         lc = sm.lc;
         qi++;
@@ -1236,7 +1607,7 @@ template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(BfsParams p) {
     Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
-    const uint64_t pol = policy_evict_first();
+    const uint64_t pol = column_policy(p);
     Counters *c = p.ctr;
     const unsigned long long saturation = 4ull * THREADS * gridDim.x;
     BusyClock clk;
@@ -1246,25 +1617,27 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
         clk.start(p);
         unsigned L = lc.L;
         const unsigned nch = lc.nch, nw = lc.nw;
-        if (stop_level_loop(p, it, L + nch + nw)) break;
+        if (stop_level_loop(p, it, L + nch + nw + lc.raw)) break;
         if (leader()) {
             ring_prepare(c, q);
-            c->total_queued += L;
-            log_phase(p, q, L, nch, nw);
+            c->total_queued += lc.raw;
+            log_phase(p, q, lc.raw, nch, nw);
         }
-        const unsigned long long edges =
-            L + (unsigned long long)nch * chunk_edges<THREADS>() + (unsigned long long)nw * WARP_CHUNK;
-        if (edges <= saturation) {
+        // the level's edge frontier as the reference counts it (before the gather-time cull)
+        if (lc.raw <= saturation) {
             ce_level<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
             clk.stop(p);
+            log_work_end(p, q);
             if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, q + 1, false))) break;
             lc = sm.lc;
             q++;
             it++;
             continue;
         }
+        const bool cull = gather_cull(lc.raw);
         tp_contract<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
         clk.stop(p);
+        log_work_end(p, q);
         if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, q + 1, false))) break;
         clk.start(p);
         q++;
@@ -1274,8 +1647,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
             ring_prepare(c, q);
             log_phase(p, q, L, 0u, 0u);
         }
-        tp_expand<THREADS, MP>(p, q, L, sm, pol);
+        tp_expand<THREADS, MP>(p, q, L, cull, sm, pol);
         clk.stop(p);
+        log_work_end(p, q);
         if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, q + 1, false))) break;
         lc = sm.lc;
         q++;
@@ -1295,7 +1669,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_level_kernel(
     const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3], nw = p.ctr->wch[it & 3];
     if (L + nch + nw == 0u || p.ctr->error) return;
     if (leader()) log_phase(p, it, L, nch, nw);
-    ec_level<THREADS, MP>(p, it, L, nch, nw, sm, policy_evict_first());
+    ec_level<THREADS, MP>(p, it, L, nch, nw, sm, column_policy(p));
 }
 
 template <int THREADS, bool MP>
@@ -1304,9 +1678,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_level_kernel(
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it;
     const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3], nw = p.ctr->wch[it & 3];
-    if (L + nch + nw == 0u || p.ctr->error) return;
-    if (leader()) log_phase(p, it, L, nch, nw);
-    ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, policy_evict_first());
+    const unsigned raw = p.ctr->raw[it & 3];
+    if (L + nch + nw + raw == 0u || p.ctr->error) return;
+    if (leader()) log_phase(p, it, raw, nch, nw);
+    ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, column_policy(p));
 }
 
 // Two-phase per-level: qi = 2 * it (contract) and 2 * it + 1 (expand).
@@ -1316,9 +1691,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_contract_kern
     init_hist(sm, p.cull_flags);
     const int it = p.ctr->cur_it, qi = 2 * it;
     const unsigned L = p.ctr->qlen[qi & 3], nch = p.ctr->big[qi & 3], nw = p.ctr->wch[qi & 3];
-    if (L + nch + nw == 0u || p.ctr->error) return;
-    if (leader()) log_phase(p, qi, L, nch, nw);
-    tp_contract<THREADS, MP>(p, it, qi, L, nch, nw, sm, policy_evict_first());
+    const unsigned raw = p.ctr->raw[qi & 3];
+    if (L + nch + nw + raw == 0u || p.ctr->error) return;
+    if (leader()) log_phase(p, qi, raw, nch, nw);
+    tp_contract<THREADS, MP>(p, it, qi, L, nch, nw, sm, column_policy(p));
 }
 
 template <int THREADS, bool MP>
@@ -1329,7 +1705,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_expand_kernel
     const unsigned L = p.ctr->qlen[qi & 3];
     if (L == 0u || p.ctr->error) return;
     if (leader()) log_phase(p, qi, L, 0u, 0u);
-    tp_expand<THREADS, MP>(p, qi, L, sm, policy_evict_first());
+    tp_expand<THREADS, MP>(p, qi, L, gather_cull(p.ctr->raw[(qi - 1) & 3]), sm, column_policy(p));
 }
 
 // Runs alone between levels of a per-level graph: records the level, prepares
@@ -1341,9 +1717,10 @@ __global__ void level_control_kernel(BfsParams p, int strategy) {
     bool more;
     if (strategy == STRATEGY_TWO_PHASE) {
         const int qi = 2 * it;
-        const unsigned vq = c->qlen[(qi + 1) & 3];                        // contract output
-        const unsigned eq = c->qlen[(qi + 2) & 3] + c->big[(qi + 2) & 3] + c->wch[(qi + 2) & 3];  // expand output
-        c->total_queued += c->qlen[qi & 3];
+        const unsigned vq = c->qlen[(qi + 1) & 3];  // contract output
+        const unsigned eq =                          // expand output, before and after the gather-time cull
+            c->raw[(qi + 2) & 3] + c->qlen[(qi + 2) & 3] + c->big[(qi + 2) & 3] + c->wch[(qi + 2) & 3];
+        c->total_queued += c->raw[qi & 3];
         if (vq == 0u) {
             c->iteration = it;  // the reference leaves after contract without ++
             more = false;
@@ -1360,16 +1737,21 @@ __global__ void level_control_kernel(BfsParams p, int strategy) {
         c->big[(qi + 4) & 3] = 0u;
         c->wch[(qi + 3) & 3] = 0u;
         c->wch[(qi + 4) & 3] = 0u;
+        c->raw[(qi + 3) & 3] = 0u;
+        c->raw[(qi + 4) & 3] = 0u;
         if (!more) log_phase(p, vq == 0u ? qi + 1 : qi + 2, 0u, 0u, 0u);
     } else {
-        const unsigned next = c->qlen[(it + 1) & 3] + c->big[(it + 1) & 3] + c->wch[(it + 1) & 3];
-        c->total_queued += c->qlen[it & 3];
+        const bool edge = strategy != STRATEGY_EXPAND_CONTRACT;
+        const unsigned next = c->qlen[(it + 1) & 3] + c->big[(it + 1) & 3] + c->wch[(it + 1) & 3] +
+                              (edge ? c->raw[(it + 1) & 3] : 0u);
+        c->total_queued += edge ? c->raw[it & 3] : c->qlen[it & 3];
         c->iteration = it + 1;
         more = next != 0u;
         c->steal[(it + 1) & 3] = 0u;
         c->qlen[(it + 2) & 3] = 0u;
         c->big[(it + 2) & 3] = 0u;
         c->wch[(it + 2) & 3] = 0u;
+        c->raw[(it + 2) & 3] = 0u;
         if (!more) log_phase(p, it + 1, 0u, 0u, 0u);
     }
     if (more && level_limit_hit(it + 1, p.nodes)) {
@@ -1567,6 +1949,23 @@ static size_t smem_bytes(const KernelConfig &kc) {
     return kc.mark_pred ? smem_bytes_t<true>(kc.threads) : smem_bytes_t<false>(kc.threads);
 }
 
+// The fused kernels' dynamic shared memory: the expand-contract kernel adds
+// its bottom-up stage buffers where they fit.
+template <bool MP>
+static size_t fused_smem_bytes_t(int threads, int strategy) {
+    if (strategy != STRATEGY_EXPAND_CONTRACT) return smem_bytes_t<MP>(threads);
+    switch (threads) {
+    case 128: return ec_smem_bytes<128, MP>();
+    case 512: return ec_smem_bytes<512, MP>();
+    default: return ec_smem_bytes<256, MP>();
+    }
+}
+static size_t fused_smem_bytes(const KernelConfig &kc) {
+    if (!kc.stage_bu) return smem_bytes(kc);  // the stage buffers take L1 capacity: only when used
+    return kc.mark_pred ? fused_smem_bytes_t<true>(kc.threads, kc.strategy)
+                        : fused_smem_bytes_t<false>(kc.threads, kc.strategy);
+}
+
 // Opts a kernel in to its dynamic shared memory size (beyond 48 KB needs it).
 static cudaError_t allow_smem(const void *fn, size_t bytes) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
@@ -1630,7 +2029,7 @@ cudaError_t launch_search_init(const BfsParams &p, const KernelConfig &kc, cudaS
 }
 
 cudaError_t fused_grid_limit(const KernelConfig &kc, int *grid) {
-    return grid_for((const void *)pick_fused(kc), kc.threads, smem_bytes(kc), grid);
+    return grid_for((const void *)pick_fused(kc), kc.threads, fused_smem_bytes(kc), grid);
 }
 
 cudaError_t level_grid_limit(const KernelConfig &kc, int *grid) {
@@ -1684,7 +2083,7 @@ cudaError_t launch_csr_check(const int *row_offsets, const int *col, int nodes, 
 
 cudaError_t launch_fused(const BfsParams &p, const KernelConfig &kc, int grid, cudaStream_t stream) {
     KernelFn fn = pick_fused(kc);
-    const size_t smem = smem_bytes(kc);
+    const size_t smem = fused_smem_bytes(kc);
     cudaError_t e = allow_smem((const void *)fn, smem);
     if (e) return e;
     BfsParams arg = p;

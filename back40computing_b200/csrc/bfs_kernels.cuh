@@ -29,6 +29,7 @@ struct LevelRecord {
     unsigned chunks;
     unsigned wchunks;
     unsigned bottom_up;  // 1 when the level ran bottom-up (direction-optimizing)
+    unsigned long long t_work_end = 0;  // when the last CTA finished the level's work (before its barrier)
 };
 
 // Everything a BFS kernel needs, passed by value.
@@ -70,7 +71,20 @@ struct BfsParams {
     // INSTRUMENT: per CTA of a fused kernel, the %globaltimer ns it spent in
     // level work (barrier waits excluded), written at the kernel's end; NULL: off.
     unsigned long long *cta_busy;
+    // 1: stream the column array through L2 with evict_first (it is large
+    // next to L2); 0: ordinary caching (the graph fits in L2).
+    int stream_col;
+    // 1: bottom-up steps stage their row offsets, heaviest-neighbour keys and
+    // mask words in shared memory with bulk copies, one step ahead; the
+    // arrays then carry ROW_PAD / HEAVY_PAD / MASK_PAD_BYTES of padding.
+    int stage_bu;
 };
+
+// Padding of the device arrays a staged bottom-up step copies in whole
+// 16-byte units past their ends.
+constexpr int ROW_PAD = 4;          // int entries after row_offsets[nodes]
+constexpr int HEAVY_PAD = 2;        // keys after heavy[nodes - 1]
+constexpr int MASK_PAD_BYTES = 16;  // bytes after the last visited-mask word
 
 // Edges per CTA chunk: four passes of one 16-byte load per thread of a CTA.
 template <int THREADS>
@@ -82,6 +96,7 @@ struct KernelConfig {
     int strategy;
     int threads;  // 128, 256 or 512
     bool mark_pred;
+    bool stage_bu = false;  // the launch carries the bottom-up stage buffers (BfsParams::stage_bu)
 };
 
 // Enqueues the per-search initialisation (counters, source) on stream.

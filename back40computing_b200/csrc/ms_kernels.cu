@@ -55,7 +55,11 @@ __device__ __forceinline__ MsSmem<THREADS, MP> &ms_smem() {
 }
 
 __device__ __forceinline__ bool leader() { return blockIdx.x == 0 && threadIdx.x == 0; }
-__device__ __forceinline__ int global_warp() { return int(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)); }
+// Warp w of the grid is warp w / gridDim.x of CTA w % gridDim.x: consecutive
+// work items (tiles, steps, runs) go to different CTAs, and so to different
+// SMs, so a level with few items still spreads over the whole GPU instead of
+// crowding the issue slots and memory pipes of the first few SMs.
+__device__ __forceinline__ int global_warp() { return int((threadIdx.x >> 5) * gridDim.x + blockIdx.x); }
 __device__ __forceinline__ int grid_warps() { return int(gridDim.x * (blockDim.x >> 5)); }
 
 __device__ __forceinline__ MsSlot load_slot(const MsParams &p, int s) {

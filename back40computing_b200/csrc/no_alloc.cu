@@ -207,6 +207,7 @@ extern "C" int b40c_enact_search_no_alloc(int nodes, int edges, const int *d_row
     bp.warp_th = NOALLOC_WARP_TH;
     bp.cta_th = NOALLOC_CTA_TH;
     bp.cull_flags = CULL_HISTORY;
+    bp.stream_col = 1;  // column loads keep their evict_first L2 policy
     const KernelConfig kc{STRATEGY_EXPAND_CONTRACT, NOALLOC_THREADS, false};
 
     // What must start at zero (counters, sticky error word included, and the

@@ -172,6 +172,13 @@ int b40c_enactor_set_level_log(b40c_enactor_t *enactor, int enable);
  * Levels of the two-phase strategy are its phases. */
 int b40c_enactor_level_log(b40c_enactor_t *enactor, int max_records, int64_t *t_start_ns,
                            int *frontier, int *chunks, int *wchunks, int *bottom_up, int *count);
+/* The level log's times (same records as b40c_enactor_level_log): each
+ * phase's start and the moment the last CTA finished its work, before the
+ * grid barrier that ends it (0 for per-level launches and the end marker);
+ * the gap to the next start is the barrier's cost.  No counterpart in the
+ * reference. */
+int b40c_enactor_level_times(b40c_enactor_t *enactor, int max_records, int64_t *t_start_ns,
+                             int64_t *t_work_end_ns, int *count);
 /* Direction-optimizing expand-contract (an addition; the reference's
  * expand-contract is top-down only): a level runs bottom-up -- each unvisited
  * vertex scans its list for a parent in the frontier -- once the frontier's
@@ -187,6 +194,25 @@ int b40c_enactor_level_log(b40c_enactor_t *enactor, int max_records, int64_t *t_
 int b40c_enactor_set_direction_optimizing(b40c_enactor_t *enactor, int alpha, int beta);
 /* Spin limit of every device-side wait (grid barrier), in microseconds. */
 int b40c_enactor_set_wait_limit_us(b40c_enactor_t *enactor, long long us);
+/* L2 residency of the search state (no counterpart in the reference, which
+ * reads the visited mask through the texture cache, contract_expand_atomic/
+ * cta.cuh:213-258): what = 0 off (the default), 1 the visited mask, 2 the
+ * visited mask and the labels.  The enactor sets a persisting access-policy
+ * window on its stream for its own launches and clears it after them; the
+ * first use sets the context's persisting-L2 limit
+ * (cudaLimitPersistingL2CacheSize, which ends with the process) to the
+ * window's size, within the device maximum. */
+int b40c_enactor_set_l2_persistence(b40c_enactor_t *enactor, int what);
+/* Bottom-up levels of direction-optimizing searches stage each step's row
+ * offsets, heaviest-neighbour keys and visited-mask words in shared memory
+ * with bulk copies issued one step ahead (enable = 1, where the kernel's
+ * shared memory allows it: 512-thread CTAs, depth labels), or load them when
+ * the step starts (0, the default: on R-MAT scale 22 the stage buffers' share
+ * of each SM's shared memory and L1 costs more than the copies save).
+ * Results are the same either way.  No
+ * counterpart in the reference, which reads row offsets per tile through the
+ * texture path (contract_expand_atomic/cta.cuh:187-207). */
+int b40c_enactor_set_bottom_up_staging(b40c_enactor_t *enactor, int enable);
 
 /* ---- host CSR graph builders (b40c/graph/builder/*.cuh, csr_graph.cuh) ---- */
 typedef struct b40c_csr {

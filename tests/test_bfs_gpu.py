@@ -520,3 +520,93 @@ def test_eight_byte_vertex_ids(cuda_device, oracle, rmat16):
                                               g.row_offsets.ctypes.data_as(P), 1) == 1
     assert lib().b40c_problem_from_host_ids64(prob._h, 1, g.nodes, g.edges, col64.ctypes.data_as(P),
                                               g.row_offsets.ctypes.data_as(P), 1) == 801
+
+
+@pytest.mark.parametrize("strategy", [1, 2, 3])
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_edge_frontier_total_queued_is_the_references(cuda_device, oracle, rmat16, strategy, variant):
+    """Edge-frontier strategies count total_queued as the reference does: the
+    sum of the levels' edge frontiers, every neighbour of every contracted
+    vertex -- 1 (the source) + edges_visited -- whether a neighbour was queued,
+    cut into a chunk, or dropped by the gather-time cull; labels and search
+    depth unchanged."""
+    b = bfs_mod()
+    for g, s in ((rmat16, int(rmat16.sample_sources(1, 13)[0])), (b.grid2d(96), 48 * 96 + 48)):
+        if strategy == 3 and variant == 2:
+            continue  # the hybrid has one way to run
+        ref, _ = oracle.bfs(g, s)
+        _, edges = oracle.visit_stats(g, ref)
+        prob = b.CsrProblem(False).from_graph(g)
+        en = b.make_enactor(strategy, INSTRUMENT=True)
+        b.check(prob.Reset(en.GetFrontierType(), 1.3))
+        b.check(en.EnactFusedSearch(prob, s) if variant == 1 else en.EnactIterativeSearch(prob, s))
+        assert oracle.first_mismatch(prob.labels(), ref) == -1
+        queued, depth, _ = en.GetStatistics()
+        assert queued == 1 + edges, (g.name, strategy, variant)
+        assert depth in expected_search_depths(strategy, g, ref)
+
+
+@pytest.mark.parametrize("what", [0, 1, 2])
+def test_l2_persistence_keeps_labels(cuda_device, oracle, rmat16, what):
+    """The persisting L2 window (visited mask, or mask and labels) changes no
+    result; an out-of-range setting is rejected."""
+    b = bfs_mod()
+    g = rmat16
+    prob = b.CsrProblem(False).from_graph(g)
+    for strategy in (0, 1):
+        en = b.make_enactor(strategy)
+        en.set_l2_persistence(what)
+        for s in g.sample_sources(2, 17 + what):
+            ref, _ = oracle.bfs(g, int(s))
+            b.check(prob.Reset(en.GetFrontierType(), 1.3))
+            b.check(en.EnactSearch(prob, int(s)))
+            assert oracle.first_mismatch(prob.labels(), ref) == -1
+    with pytest.raises(b.BfsError):
+        b.make_enactor(0).set_l2_persistence(3)
+
+
+@pytest.mark.parametrize("strategy", STRATEGIES)
+def test_level_times_are_ordered(cuda_device, rmat16, strategy):
+    """The level log's work-end time of a fused search's phase lies between the
+    phase's start and the next phase's start (the grid barrier between)."""
+    b = bfs_mod()
+    g = rmat16
+    prob = b.CsrProblem(False).from_graph(g)
+    en = b.make_enactor(strategy)
+    en.set_level_log(True)
+    b.check(prob.Reset(en.GetFrontierType(), 1.3))
+    b.check(en.EnactFusedSearch(prob, int(g.sample_sources(1, 23)[0])))
+    log = en.level_log()
+    assert len(log) >= 3
+    for cur, nxt in zip(log[:-1], log[1:]):
+        assert cur["work_end_ns"] is not None
+        assert cur["start_ns"] <= cur["work_end_ns"] <= nxt["start_ns"]
+
+
+@pytest.mark.parametrize("alpha", [14, 1])
+def test_bottom_up_staging_matches_loads(cuda_device, oracle, rmat16, alpha):
+    """Bottom-up steps with their inputs staged in shared memory by bulk copies
+    and with plain loads give the oracle's labels, search depth and
+    total_queued, including a graph whose vertex count is not a multiple of a
+    step's 128 vertices (the last step's copies are clamped to the arrays'
+    padded ends)."""
+    b = bfs_mod()
+    graphs = [rmat16, b.erdos_renyi(5003, 12.0 / 5002, seed=9), b.grid2d(61)]
+    for g in graphs:
+        prob = b.CsrProblem(False).from_graph(g)
+        for s in g.sample_sources(3, 31):
+            ref, _ = oracle.bfs(g, int(s))
+            stats = []
+            for staged in (True, False):
+                en = b.EnactorExpandContract(INSTRUMENT=True)
+                en.set_direction_optimizing(alpha, 24)
+                en.set_bottom_up_staging(staged)
+                en.set_level_log(True)
+                b.check(prob.Reset(en.GetFrontierType(), 1.3))
+                b.check(en.EnactSearch(prob, int(s)))
+                assert oracle.first_mismatch(prob.labels(), ref) == -1, (g.name, int(s), staged)
+                queued, depth, _ = en.GetStatistics()
+                stats.append((queued, depth))
+                if alpha == 1:
+                    assert any(r["bottom_up"] for r in en.level_log()), g.name
+            assert stats[0] == stats[1]
