@@ -128,3 +128,26 @@ def test_bench_batched_set_every_search_matches_oracle(cuda_device, oracle):
             assert oracle.first_mismatch(batch.labels(int(i)), refs[k]) == -1, (gi, int(i), int(srcs[i]))
             assert batch.search_depth(int(i)) == int(refs[k].max())
     batch.close()
+
+
+def test_replica_share_through_a_batch(cuda_device, oracle, mixed_graphs):
+    """One replica's share (here, every query: one process) run by
+    replicas.batch_share on a BfsBatch holding every graph, gathered in query
+    order; each label array against the oracle."""
+    from back40computing_b200.batch import BfsBatch
+    from back40computing_b200.replicas import batch_share, run_partitioned
+    batch = BfsBatch()
+    for g in mixed_graphs:
+        batch.add_graph(g)
+    gids, srcs = [], []
+    for gi, g in enumerate(mixed_graphs):
+        for s in g.sample_sources(3, 71 + gi):
+            gids.append(gi)
+            srcs.append(int(s))
+    costs = [mixed_graphs[g].edges for g in gids]
+    labels, secs = run_partitioned(gids, srcs, batch_share(batch), costs=costs)
+    assert len(secs) == 1 and secs[0] > 0
+    for i, (g, s) in enumerate(zip(gids, srcs)):
+        ref, _ = oracle.bfs(mixed_graphs[g], s)
+        assert oracle.first_mismatch(labels[i], ref) == -1, i
+    batch.close()
