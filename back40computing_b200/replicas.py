@@ -18,8 +18,8 @@ independent replicas (bench.py under torchrun).
 
 ``run_share(indices, graph_ids, sources) -> (labels, seconds)`` is the per-rank
 search: :func:`batch_share` runs a :class:`~back40computing_b200.batch.BfsBatch`
-on the rank's GPU; any callable with that signature works (the tests use the
-CPU oracle to exercise the placement on gloo ranks).
+on the rank's GPU; any callable with that signature works (the tests run a
+CPU search on gloo ranks to exercise the placement).
 """
 from __future__ import annotations
 
