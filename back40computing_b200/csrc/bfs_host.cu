@@ -979,16 +979,19 @@ extern "C" int b40c_enactor_create(int strategy, int instrument, int debug, b40c
     b40c_enactor *e = new (std::nothrow) b40c_enactor();
     if (!e) return set_error(B40C_ERR_MEMORY_ALLOCATION, "enactor allocation");
     e->strategy = strategy;
-    // Measured defaults: expand-contract runs 512-thread CTAs and gathers
-    // lists of 128+ edges with warps; the edge-frontier strategies run
-    // 256-thread CTAs and gather lists of 64+.
-    // Expand-contract switches direction with the published alpha = 14,
-    // beta = 24 (Beamer, Asanovic and Patterson, SC 2012).
+    // Measured defaults: expand-contract and contract-expand run 512-thread
+    // CTAs (best for both on R-MAT scale 22 and on the lattices); two-phase
+    // and the hybrid run 256-thread CTAs (best on R-MAT scale 22).
+    // Expand-contract gathers lists of 128+ edges with warps, the others lists
+    // of 64+, and expand-contract switches direction with the published
+    // alpha = 14, beta = 24 (Beamer, Asanovic and Patterson, SC 2012).
     if (strategy == B40C_EXPAND_CONTRACT) {
-        e->threads = 512;  // measured best for expand-contract on R-MAT and lattices alike
+        e->threads = 512;
         e->warp_th = 128;
         e->do_alpha = 14;
         e->do_beta = 24;
+    } else if (strategy == B40C_CONTRACT_EXPAND) {
+        e->threads = 512;
     }
     e->instrument = instrument != 0;
     e->debug = debug != 0;

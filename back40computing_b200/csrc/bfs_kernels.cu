@@ -99,9 +99,16 @@ __device__ __forceinline__ uint64_t column_policy(const BfsParams &p) {
 // probe, whose result refreshes the entry.  Hub vertices' words stay cached,
 // which keeps their mask lines from becoming L2 hot spots.  The optional warp
 // cull (__match_any_sync) drops repeats inside a warp first.
-template <int THREADS, bool MP>
+//
+// probe: test the mask with an L2 load before claiming (large levels, where
+// most elements are already visited and the load spares their atomics); on
+// small levels every element the cache does not cull goes straight to
+// atomicOr, one round trip less.  With ROWS, the row ranges of the elements
+// sent to atomicOr are loaded together with the atomics, and st / ln hold
+// those of the claimed elements (0 / 0 otherwise).
+template <int THREADS, bool MP, bool ROWS = false>
 __device__ __forceinline__ unsigned cull4(const BfsParams &p, Smem<THREADS, MP> &sm, unsigned valid,
-                                          const int (&u)[4]) {
+                                          const int (&u)[4], bool probe, int (&st)[4], int (&ln)[4]) {
     const bool history = p.cull_flags & CULL_HISTORY;
     if (p.cull_flags & CULL_WARP) {
 #pragma unroll
@@ -129,15 +136,30 @@ __device__ __forceinline__ unsigned cull4(const BfsParams &p, Smem<THREADS, MP> 
             if (unsigned(e >> 32) == w[j] && (unsigned(e) & bit[j])) valid &= ~(1u << j);
         }
     }
+    unsigned need = valid;
+    if (probe) {
 #pragma unroll
-    for (int j = 0; j < 4; j++) m[j] = ((valid >> j) & 1u) ? ld_cg(p.mask + w[j]) : 0u;  // probes in flight
-    unsigned need = 0;
+        for (int j = 0; j < 4; j++) m[j] = ((valid >> j) & 1u) ? ld_cg(p.mask + w[j]) : 0u;  // probes in flight
+        need = 0;
 #pragma unroll
-    for (int j = 0; j < 4; j++)
-        if (((valid >> j) & 1u) && !(m[j] & bit[j])) need |= 1u << j;
+        for (int j = 0; j < 4; j++)
+            if (((valid >> j) & 1u) && !(m[j] & bit[j])) need |= 1u << j;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) m[j] = 0u;
+    }
     unsigned old[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) old[j] = ((need >> j) & 1u) ? atomicOr(p.mask + w[j], bit[j]) : m[j];
+    int r0[4], r1[4];
+    if (ROWS) {  // issued behind the atomics, before their results are used
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int vv = ((need >> j) & 1u) ? u[j] : 0;
+            r0[j] = __ldg(p.row_offsets + vv);
+            r1[j] = __ldg(p.row_offsets + vv + 1);
+        }
+    }
     unsigned claimed = 0;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -147,7 +169,29 @@ __device__ __forceinline__ unsigned cull4(const BfsParams &p, Smem<THREADS, MP> 
                 sm.vcache[vcache_slot(w[j])] = ((unsigned long long)w[j] << 32) | (old[j] | bit[j]);
         }
     }
+    if (ROWS) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const bool c = (claimed >> j) & 1u;
+            st[j] = c ? r0[j] : 0;
+            ln[j] = c ? r1[j] - r0[j] : 0;
+        }
+    }
     return claimed;
+}
+
+// The elements a phase's sinks receive: its queue entries (each list of a
+// vertex queue counted as avg_list entries) and its chunk tables' edges.
+template <int THREADS>
+__device__ __forceinline__ unsigned long long phase_work(unsigned L, unsigned avg_list, unsigned nch, unsigned nw) {
+    return (unsigned long long)L * avg_list + (unsigned long long)nch * chunk_edges<THREADS>() +
+           (unsigned long long)nw * WARP_CHUNK;
+}
+
+// Whether a level whose sinks receive about `work` elements probes the mask
+// before claiming (cull4): more than 4 elements per thread of the grid.
+__device__ __forceinline__ bool probe_level(unsigned long long work) {
+    return work > 4ull * blockDim.x * gridDim.x;
 }
 
 // Writes the warp's staged appends to queue q with one atomicAdd (coalesced
@@ -430,20 +474,22 @@ __device__ __forceinline__ void gather_positional4(const BfsParams &p, WarpSmem<
     const unsigned total = list_layout(has, ln, o);
     if (total == 0u) return;  // warp-uniform
     unsigned base = 0;
-    if (lane_id() == 0) {
-        base = atomicAdd(qlen_out, total);
-        if ((unsigned long long)base + total > (unsigned long long)p.qcap) {
-            atomicOr(&p.ctr->error, ERR_OVERFLOW);
-            base = 0xffffffffu;
-        }
-    }
-    base = __shfl_sync(FULL, base, 0);
-    if (base == 0xffffffffu) return;  // warp-uniform: output dropped on overflow
     for (unsigned w0 = 0; w0 < total; w0 += WINDOW) {
         int e[4], own[4], x[4];
         window_entries<MP>(ws, has, st, ln, pr, o, w0, total, e, own);
 #pragma unroll
         for (int m = 0; m < 4; m++) x[m] = e[m] >= 0 ? ldg_stream(p.col + e[m], pol) : 0;
+        if (w0 == 0) {  // the reservation's round trip overlaps the first window's loads
+            if (lane_id() == 0) {
+                base = atomicAdd(qlen_out, total);
+                if ((unsigned long long)base + total > (unsigned long long)p.qcap) {
+                    atomicOr(&p.ctr->error, ERR_OVERFLOW);
+                    base = 0xffffffffu;
+                }
+            }
+            base = __shfl_sync(FULL, base, 0);
+            if (base == 0xffffffffu) return;  // warp-uniform: output dropped on overflow
+        }
 #pragma unroll
         for (int m = 0; m < 4; m++) {
             if (e[m] >= 0) {
@@ -724,20 +770,15 @@ struct DiscoverSink {
     int *q_out;
     unsigned *qlen_out;
     int label;  // it + 1; also the phase whose inputs the discovered lists become
+    bool probe;  // cull4's mask probe before claiming (probe_level)
 
     __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
                                                unsigned) const {
-        const unsigned disc = cull4<THREADS, MP>(p, sm, valid, u);
         int st[4], ln[4];
+        const unsigned disc = cull4<THREADS, MP, true>(p, sm, valid, u, probe, st, ln);
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            st[j] = 0;
-            ln[j] = 0;
-            if ((disc >> j) & 1u) {
-                p.labels[u[j]] = MP ? pred[j] : label;
-                row_range(p, u[j], st[j], ln[j]);
-            }
-        }
+        for (int j = 0; j < 4; j++)
+            if ((disc >> j) & 1u) p.labels[u[j]] = MP ? pred[j] : label;
         if (p.do_alpha)
             count_discovered(sm.w[threadIdx.x >> 5], __popc(disc), (long long)ln[0] + ln[1] + ln[2] + ln[3]);
         const unsigned enq = disc & ~place4<THREADS>(p, label, disc, st, ln, u);
@@ -763,16 +804,20 @@ struct ContractExpandSink {
     int it;  // depth label of the contracted vertices
     int q;   // ring phase: reads queue[q&1], writes queue[(q+1)&1] and ring slot q+1
     uint64_t pol;
+    bool probe;  // cull4's mask probe before claiming (probe_level)
 
     __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
                                                unsigned) const {
-        const unsigned surv = cull4<THREADS, MP>(p, sm, valid, u);
-        if (!__any_sync(FULL, surv != 0u)) return;
-        // The survivors' row ranges (all loads in flight together), then their
-        // lists: long ones to the next phase's chunk tables, the rest gathered
-        // by the warp into the next edge frontier at once.
+        // The survivors' row ranges come with the claims (loaded together with
+        // the atomics), then their lists: long ones to the next phase's chunk
+        // tables, the rest gathered by the warp into the next edge frontier.
         int st[4], ln[4];
-        const unsigned has = row_ranges4(p, surv, u, st, ln);
+        const unsigned surv = cull4<THREADS, MP, true>(p, sm, valid, u, probe, st, ln);
+        if (!__any_sync(FULL, surv != 0u)) return;
+        unsigned has = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (ln[j] > 0) has |= 1u << j;
 #pragma unroll
         for (int j = 0; j < 4; j++)
             if ((surv >> j) & 1u) p.labels[u[j]] = MP ? pred[j] : it;
@@ -796,10 +841,12 @@ struct ContractSink {
     int *q_out;
     unsigned *qlen_out;
     int it;
+    bool probe;  // cull4's mask probe before claiming (probe_level)
 
     __device__ __forceinline__ void operator()(unsigned valid, const int (&u)[4], const int (&pred)[4],
                                                unsigned) const {
-        const unsigned surv = cull4<THREADS, MP>(p, sm, valid, u);
+        int st[4], ln[4];
+        const unsigned surv = cull4<THREADS, MP>(p, sm, valid, u, probe, st, ln);
 #pragma unroll
         for (int j = 0; j < 4; j++)
             if ((surv >> j) & 1u) p.labels[u[j]] = MP ? pred[j] : it;
@@ -824,7 +871,9 @@ __device__ void ec_level(const BfsParams &p, int it, unsigned L, unsigned nch, u
                          uint64_t pol) {
     Counters *c = p.ctr;
     const int nq = (it + 1) & 1;
-    DiscoverSink<THREADS, MP> sink{p, sm, p.queue[nq], &c->qlen[(it + 1) & 3], it + 1};
+    // a vertex queue's lists are shorter than warp_th; count 16 entries each
+    DiscoverSink<THREADS, MP> sink{p, sm, p.queue[nq], &c->qlen[(it + 1) & 3], it + 1,
+                                   probe_level(phase_work<THREADS>(L, 16u, nch, nwch))};
     gather_chunk_tables<THREADS>(p, p.chunks[it & 1], nch, p.wchunks[it & 1], nwch, sink, pol);
     WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
     const int *q_in = p.queue[it & 1];
@@ -1215,7 +1264,7 @@ __device__ __forceinline__ void edge_tiles(const int *q_in, const int *pq_in, un
 template <int THREADS, bool MP>
 __device__ void ce_level(const BfsParams &p, int it, int q, unsigned L, unsigned nch, unsigned nwch,
                          Smem<THREADS, MP> &sm, uint64_t pol) {
-    ContractExpandSink<THREADS, MP> sink{p, sm, it, q, pol};
+    ContractExpandSink<THREADS, MP> sink{p, sm, it, q, pol, probe_level(phase_work<THREADS>(L, 1u, nch, nwch))};
     gather_chunk_tables<THREADS>(p, p.chunks[q & 1], nch, p.wchunks[q & 1], nwch, sink, pol);
     edge_tiles<MP>(p.queue[q & 1], p.pred_queue[q & 1], L, sink);
     sink.drain();
@@ -1225,7 +1274,8 @@ __device__ void ce_level(const BfsParams &p, int it, int q, unsigned L, unsigned
 template <int THREADS, bool MP>
 __device__ void tp_contract(const BfsParams &p, int it, int qi, unsigned L, unsigned nch, unsigned nwch,
                             Smem<THREADS, MP> &sm, uint64_t pol) {
-    ContractSink<THREADS, MP> sink{p, sm, p.queue[(qi + 1) & 1], &p.ctr->qlen[(qi + 1) & 3], it};
+    ContractSink<THREADS, MP> sink{p, sm, p.queue[(qi + 1) & 1], &p.ctr->qlen[(qi + 1) & 3], it,
+                                   probe_level(phase_work<THREADS>(L, 1u, nch, nwch))};
     gather_chunk_tables<THREADS>(p, p.chunks[qi & 1], nch, p.wchunks[qi & 1], nwch, sink, pol);
     edge_tiles<MP>(p.queue[qi & 1], p.pred_queue[qi & 1], L, sink);
     sink.drain();
@@ -1315,7 +1365,12 @@ __device__ __forceinline__ void init_hist(Smem<THREADS, MP> &sm, unsigned flags)
     }
 }
 
-__device__ __forceinline__ bool leader() { return blockIdx.x == 0 && threadIdx.x == 0; }
+// The thread that does a fused kernel's per-level bookkeeping (ring entries,
+// statistics, level log): lane 0 of CTA 0's last warp, which takes tiles only
+// when a level has more than (warps per CTA - 1) * grid of them, so that the
+// bookkeeping's round trips stay off the warp that takes a small level's
+// first tile.
+__device__ __forceinline__ bool leader() { return blockIdx.x == 0 && threadIdx.x == blockDim.x - 32; }
 
 // INSTRUMENT duty (the reference's KernelRuntimeStats MarkStart / MarkStop,
 // b40c/util/kernel_runtime_stats.cuh): thread 0 of each CTA sums the time from
