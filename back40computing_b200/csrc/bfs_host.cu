@@ -395,6 +395,7 @@ int fill_params(b40c_enactor *e, b40c_problem *p, int src, BfsParams &bp) {
     bp.cull_flags = e->cull_flags;
     bp.edges = p->edges;
     bp.stream_col = stream_column(p->device, p->edges) ? 1 : 0;
+    bp.count_raw = e->instrument ? 1 : 0;
     bp.do_alpha = 0;  // enabled by enqueue_search for searches that can run bottom-up
     bp.do_beta = 0;
     if (qcap < 1) return set_error(B40C_ERR_ILLEGAL_STATE, "frontier queues not allocated: call Reset first");

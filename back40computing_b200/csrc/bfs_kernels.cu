@@ -665,6 +665,16 @@ __device__ __forceinline__ void flush_raw(const BfsParams &p, WarpSmem<MP> &ws, 
     __syncwarp();
 }
 
+// The edge frontier a phase starts from: its raw count when the phase before
+// counted it (INSTRUMENT, or a culling expand), else its queue entries plus
+// the edges of its chunk tables.
+template <int THREADS>
+__device__ __forceinline__ unsigned long long level_edges(const LevelCounts &lc) {
+    const unsigned long long est = (unsigned long long)lc.L + (unsigned long long)lc.nch * chunk_edges<THREADS>() +
+                                   (unsigned long long)lc.nw * WARP_CHUNK;
+    return est > lc.raw ? est : (unsigned long long)lc.raw;
+}
+
 // Whether a two-phase expand culls while it gathers, by the edge frontier raw
 // its level started from: on large levels (more than 4 entries per thread of
 // the grid, the hybrid's saturation point) most gathered neighbours are
@@ -672,8 +682,8 @@ __device__ __forceinline__ void flush_raw(const BfsParams &p, WarpSmem<MP> &ws, 
 // of the level -- and dropping them early saves their queue traffic and
 // contraction; on small levels the extra probe only lengthens the level's
 // dependent chain.
-__device__ __forceinline__ bool gather_cull(unsigned raw) {
-    return (unsigned long long)raw > 4ull * blockDim.x * gridDim.x;
+__device__ __forceinline__ bool gather_cull(unsigned long long raw) {
+    return raw > 4ull * blockDim.x * gridDim.x;
 }
 
 // The gather-time cull of the edge-frontier strategies: a gathered neighbour
@@ -822,7 +832,7 @@ struct ContractExpandSink {
         for (int j = 0; j < 4; j++)
             if ((surv >> j) & 1u) p.labels[u[j]] = MP ? pred[j] : it;
         WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
-        count_raw(&ws.raw_n, has, ln);
+        if (p.count_raw) count_raw(&ws.raw_n, has, ln);
         const unsigned placed = place4<THREADS>(p, q + 1, has, st, ln, u);
         const int nq = (q + 1) & 1;
         gather_positional4<MP>(p, ws, has & ~placed, st, ln, u, p.queue[nq], p.pred_queue[nq],
@@ -1302,7 +1312,7 @@ __device__ void tp_expand(const BfsParams &p, int qi, unsigned L, bool cull, Sme
             int v[4], st[4], ln[4];
             const unsigned sel = load_tile(q_in, L, t, per, v);
             const unsigned has = row_ranges4(p, sel, v, st, ln);
-            count_raw(&ws.raw_n, has, ln);
+            if (cull || p.count_raw) count_raw(&ws.raw_n, has, ln);
             const unsigned placed = place4<THREADS>(p, qi + 1, has, st, ln, v);
             if (cull)
                 gather_windows4<MP>(p, ws, has & ~placed, st, ln, v, out, pol);
@@ -1588,7 +1598,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
         if (leader()) {
             ring_prepare(c, it);
             c->total_queued += lc.raw;
-            log_phase(p, it, lc.raw, nch, nw);
+            log_phase(p, it, lc.raw ? lc.raw : L, nch, nw);
         }
         ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, pol);
         clk.stop(p);
@@ -1619,11 +1629,11 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
         unsigned L = lc.L;
         const unsigned nch = lc.nch, nw = lc.nw;
         if (stop_level_loop(p, it, L + nch + nw + lc.raw)) break;
-        const bool cull = gather_cull(lc.raw);
+        const bool cull = gather_cull(level_edges<THREADS>(lc));
         if (leader()) {
             ring_prepare(c, qi);
             c->total_queued += lc.raw;
-            log_phase(p, qi, lc.raw, nch, nw);
+            log_phase(p, qi, lc.raw ? lc.raw : L, nch, nw);
         }
         tp_contract<THREADS, MP>(p, it, qi, L, nch, nw, sm, pol);
         clk.stop(p);
@@ -1676,10 +1686,11 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
         if (leader()) {
             ring_prepare(c, q);
             c->total_queued += lc.raw;
-            log_phase(p, q, lc.raw, nch, nw);
+            log_phase(p, q, lc.raw ? lc.raw : L, nch, nw);
         }
         // the level's edge frontier as the reference counts it (before the gather-time cull)
-        if (lc.raw <= saturation) {
+        const unsigned long long edges = level_edges<THREADS>(lc);
+        if (edges <= saturation) {
             ce_level<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
             clk.stop(p);
             log_work_end(p, q);
@@ -1689,7 +1700,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
             it++;
             continue;
         }
-        const bool cull = gather_cull(lc.raw);
+        const bool cull = gather_cull(edges);
         tp_contract<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
         clk.stop(p);
         log_work_end(p, q);
@@ -1735,7 +1746,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_level_kernel(
     const unsigned L = p.ctr->qlen[it & 3], nch = p.ctr->big[it & 3], nw = p.ctr->wch[it & 3];
     const unsigned raw = p.ctr->raw[it & 3];
     if (L + nch + nw + raw == 0u || p.ctr->error) return;
-    if (leader()) log_phase(p, it, raw, nch, nw);
+    if (leader()) log_phase(p, it, raw ? raw : L, nch, nw);
     ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, column_policy(p));
 }
 
@@ -1748,7 +1759,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_contract_kern
     const unsigned L = p.ctr->qlen[qi & 3], nch = p.ctr->big[qi & 3], nw = p.ctr->wch[qi & 3];
     const unsigned raw = p.ctr->raw[qi & 3];
     if (L + nch + nw + raw == 0u || p.ctr->error) return;
-    if (leader()) log_phase(p, qi, raw, nch, nw);
+    if (leader()) log_phase(p, qi, raw ? raw : L, nch, nw);
     tp_contract<THREADS, MP>(p, it, qi, L, nch, nw, sm, column_policy(p));
 }
 
@@ -1760,7 +1771,13 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_expand_kernel
     const unsigned L = p.ctr->qlen[qi & 3];
     if (L == 0u || p.ctr->error) return;
     if (leader()) log_phase(p, qi, L, 0u, 0u);
-    tp_expand<THREADS, MP>(p, qi, L, gather_cull(p.ctr->raw[(qi - 1) & 3]), sm, column_policy(p));
+    const int qc = qi - 1;  // the level's contract phase
+    LevelCounts in{};
+    in.L = p.ctr->qlen[qc & 3];
+    in.nch = p.ctr->big[qc & 3];
+    in.nw = p.ctr->wch[qc & 3];
+    in.raw = p.ctr->raw[qc & 3];
+    tp_expand<THREADS, MP>(p, qi, L, gather_cull(level_edges<THREADS>(in)), sm, column_policy(p));
 }
 
 // Runs alone between levels of a per-level graph: records the level, prepares

@@ -78,6 +78,10 @@ struct BfsParams {
     // mask words in shared memory with bulk copies, one step ahead; the
     // arrays then carry ROW_PAD / HEAVY_PAD / MASK_PAD_BYTES of padding.
     int stage_bu;
+    // 1: count every phase's raw edge frontier (INSTRUMENT's total_queued);
+    // 0: only phases that cull while they gather count it (their queue
+    // alone would stop the level loop early).
+    int count_raw;
 };
 
 // Padding of the device arrays a staged bottom-up step copies in whole
