@@ -377,6 +377,12 @@ class SequentialSearches:
         b.check(self.problems[gid].ResetAsync(self.ft, 1.3))
         b.check(self.en.EnactSearchAsync(self.problems[gid], int(src), 0, 1))
 
+    def run(self, gid, src):
+        """One synchronous query: Reset + EnactSearch, waiting for the search."""
+        b = self.b
+        b.check(self.problems[gid].Reset(self.ft, 1.3))
+        b.check(self.en.EnactSearch(self.problems[gid], int(src)))
+
     def labels(self, gid):
         b = self.b
         b.check(self.en.Sync())
@@ -532,21 +538,13 @@ def served_leg(b, torch, stream, args, main_graph):
     gs, desc = served_set(main_graph)
     G = len(gs)
     pool = [g.sample_sources(16, 400 + i) for i, g in enumerate(gs)]
+    # Every (graph, source) pair searched alone: the labels each served query must reproduce.
     seq = SequentialSearches(b, gs, stream)
-    # Service time of every (graph, source) pair, alone, after a warm-up search.
-    service = np.zeros((G, 16))
     crc = np.zeros((G, 16), np.int64)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     for gi in range(G):
-        seq.enqueue(gi, pool[gi][0])
-        b.check(seq.en.Sync())
         for k, s in enumerate(pool[gi]):
-            ev[0].record(stream)
             seq.enqueue(gi, s)
-            ev[1].record(stream)
             crc[gi, k] = _crc(seq.labels(gi))
-            service[gi, k] = ev[0].elapsed_time(ev[1]) * 1e3
-    seq.close()
     budget = min(48 << 30, int(torch.cuda.mem_get_info()[0] * 0.6))
     srv = BfsServer(max_slots=1024, hbm_budget_bytes=budget)
     for g in gs:
@@ -571,31 +569,60 @@ def served_leg(b, torch, stream, args, main_graph):
                        "queries (graph, source) uniform over graphs, 16 seeded sources per graph",
            "labels": "identical alone and in the mix (crc32, 256-query trace at 50K req/s)"}
     rates = []
+    traces = []
     for rate, nq in ((1000.0, 1000), (10000.0, 2000), (50000.0, 4000), (None, 4000)):
         gids, ks, srcs, arr = trace(nq, rate, 21 + nq)
+        traces.append((rate, nq, gids, srcs, arr))
         lat, span = srv.run_trace(gids, srcs, arr)
-        svc = service[gids, ks]
-        fin, t = np.zeros(nq), 0.0
-        for i in range(nq):
-            t = max(t, arr[i]) + svc[i]
-            fin[i] = t
-        slat = fin - arr
         rates.append({
             "rate_per_s": rate if rate is not None else "all at t=0", "queries": nq,
             "queries_per_s": nq / (span / 1e6), "p50_us": float(np.percentile(lat, 50)),
-            "p99_us": float(np.percentile(lat, 99)),
-            "sequential_queries_per_s": nq / (fin[-1] / 1e6), "sequential_p50_us": float(np.percentile(slat, 50)),
-            "sequential_p99_us": float(np.percentile(slat, 99)),
-        })
+            "p99_us": float(np.percentile(lat, 99))})
     st = srv.stats()
     srv.close()
+    # The same traces served sequentially, for real: one query at a time in
+    # arrival order through the plain synchronous Reset + EnactSearch,
+    # latency = completion - arrival on the host clock.
+    for r, (rate, nq, gids, srcs, arr) in zip(rates, traces):
+        fin = np.zeros(nq)
+        t0 = time.perf_counter()
+        for i in range(nq):
+            now = (time.perf_counter() - t0) * 1e6
+            if arr[i] > now:
+                time.sleep((arr[i] - now) / 1e6)
+            seq.run(gids[i], srcs[i])
+            fin[i] = (time.perf_counter() - t0) * 1e6
+        slat = fin - arr
+        r.update({"sequential_queries_per_s": nq / (fin[-1] / 1e6),
+                  "sequential_p50_us": float(np.percentile(slat, 50)),
+                  "sequential_p99_us": float(np.percentile(slat, 99))})
+    seq.close()
     sat = rates[-1]
     out.update({"rates": rates, "saturated_queries_per_s": sat["queries_per_s"],
                 "sequential_saturated_queries_per_s": sat["sequential_queries_per_s"],
                 "speedup_vs_sequential": sat["queries_per_s"] / sat["sequential_queries_per_s"],
                 "server": st,
-                "timing": "server: host clock in the request loop, real-time replay; sequential: FIFO of each "
-                          "query's device service time (Reset+EnactSearch alone), no host overhead"})
+                "timing": "server: host clock in the request loop, real-time replay; sequential: the same "
+                          "traces replayed in real time through synchronous Reset + EnactSearch, one query at a "
+                          "time in arrival order, host clock"})
+    return out
+
+
+def summary_block(e2e, batched, served, lattices, results):
+    """The line's figures in a few keys placed near its front (the full
+    objects follow later in the line)."""
+    out = {"strategies_ms": {STRATEGY_NAMES[s]: round(r["kernel_ms_mean"], 4) for s, r in results.items()}}
+    if e2e:
+        out["e2e_gteps"] = round(e2e["value"], 1)
+    if batched:
+        out["batched_queries_per_s"] = round(batched["queries_per_s"])
+        out["batched_speedup_vs_sequential"] = round(batched["speedup_vs_sequential"], 2)
+    if served:
+        out["served_queries_per_s"] = round(served["saturated_queries_per_s"])
+        out["served_speedup_vs_sequential"] = round(served["speedup_vs_sequential"], 2)
+    if lattices:
+        out["lattices_ms"] = {name: {STRATEGY_NAMES[s]: round(row[STRATEGY_NAMES[s]]["ms"], 2) for s in range(4)}
+                              for name, row in lattices.items()}
     return out
 
 
@@ -831,6 +858,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded R-MAT, 64 sources)",
         "config": bench_config(args, g.nodes, g.edges, nsrc, world),
+        "summary": summary_block(e2e, batched, served, lattices, results),
         "headline": f"strategy {STRATEGY_NAMES[HEADLINE]} "
                     f"{'fused, direction-optimizing (alpha 14, beta 24)' if args.variant == 1 else 'iterative'}",
         "roofline": {"bound": "hbm", "achieved": head["alg_gbs"], "peak": peak, "unit": "GB/s",
