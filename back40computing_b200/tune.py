@@ -37,7 +37,8 @@ DEFAULT_POLICY = {"cta_threads": 512, "warp_gather_threshold": 128, "cta_gather_
 
 DEFAULT_CACHE = Path(os.environ.get("B40C_TUNE_CACHE", Path.home() / ".cache" / "b40c_bfs_tune.json"))
 # Tunings this package ships, made on a B200 by tune_enactor / tune_batch
-# (the bench workloads: R-MAT s22 single searches; the 1024-search batch).
+# (the bench workloads: R-MAT s22 single searches; the 1024-search batch; every
+# strategy's single searches on the lattices grid2d 1024^2 and grid3d 256^3).
 SHIPPED = Path(__file__).resolve().parent / "tuned_policies.json"
 
 

@@ -482,9 +482,10 @@ def lattice_leg(b, torch, stream, args):
     """The lattice workloads: grid2d 1024 x 1024 from its centre (1,048,576
     vertices, 4,190,208 entries) and grid3d 256^3 from vertex 0 (16,777,216
     vertices, 100,270,080 entries; 766 levels): single searches with each
-    strategy in the persistent kernel and as per-level launches, device
+    strategy in the persistent kernel (with the autotuner's policy for the
+    graph, and with the library defaults) and as per-level launches, device
     time, labels checked against the oracle once."""
-    from back40computing_b200 import graphs
+    from back40computing_b200 import graphs, tune
     sys.path.insert(0, str(ROOT / "oracle"))
     from oracle import Oracle
     orc = Oracle()
@@ -496,9 +497,7 @@ def lattice_leg(b, torch, stream, args):
         prob.set_stream(stream.cuda_stream)
         row = {"nodes": g.nodes, "edges": g.edges, "source": src, "depth": int(ref.max())}
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        for strat in (0, 1, 2, 3):
-            en = b.make_enactor(strat)
-            en.set_stream(stream.cuda_stream)
+        def fused_ms(en):
             ft = en.GetFrontierType()
             b.check(prob.Reset(ft, 1.3))
             b.check(en.EnactSearch(prob, src))
@@ -512,8 +511,23 @@ def lattice_leg(b, torch, stream, args):
                 ev[1].record(stream)
                 b.check(en.Sync())
                 ms.append(ev[0].elapsed_time(ev[1]))
-            t = float(np.median(ms))
-            row[STRATEGY_NAMES[strat]] = {"ms": t, "gteps": E / (t / 1e3) / 1e9, "us_per_level": t * 1e3 / (row["depth"] + 1)}
+            return float(np.median(ms))
+
+        for strat in (0, 1, 2, 3):
+            en = b.make_enactor(strat)
+            en.set_stream(stream.cuda_stream)
+            ft = en.GetFrontierType()
+            t_default = fused_ms(en)
+            # The autotuner's policy for this graph (its B200 result ships with
+            # the package; a graph it has not seen is tuned here).
+            policy = tune.tune_enactor(g, strat, cache=tune.TuneCache(None, seed=tune.SHIPPED))
+            tuned = b.make_enactor(strat)
+            tuned.set_stream(stream.cuda_stream)
+            tune.apply_enactor_policy(tuned, policy)
+            t = fused_ms(tuned)
+            del tuned
+            row[STRATEGY_NAMES[strat]] = {"ms": t, "gteps": E / (t / 1e3) / 1e9, "us_per_level": t * 1e3 / (row["depth"] + 1),
+                                          "policy": policy, "default_policy_ms": t_default}
             if strat != 3:  # the same search as per-level launches (a CUDA graph with a conditional loop)
                 it_ms = []
                 for _ in range(3):
