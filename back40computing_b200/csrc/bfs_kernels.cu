@@ -61,6 +61,7 @@ struct WarpSmem {
     int opred[MP ? OBUF : 1];    // owners staged with obuf (edge-frontier appends with predecessors)
     unsigned nbuf;
     unsigned raw_n;              // edge-frontier entries this warp's expansions produced in the phase
+    unsigned zmark_n;            // bottom-up: vertices without edges this warp marked in the level
     unsigned disc_n;             // direction-optimizing counts of this warp's discoveries
     unsigned long long disc_m;   // in the current level, added to the counters at its end
     unsigned bfound[4];          // bottom-up window scans: vertex 32j + lane found a parent
@@ -763,8 +764,12 @@ __device__ __forceinline__ void flush_discovered(const BfsParams &p, WarpSmem<MP
             atomicAdd(&p.ctr->nf[q & 3], ws.disc_n);
             atomicAdd(&p.ctr->mf[q & 3], ws.disc_m);
         }
+        // Bottom-up levels count the vertices without edges they mark per warp
+        // (one atomic per step on one address made that address a hot spot).
+        if (ws.zmark_n) atomicAdd(&p.ctr->zmarked, ws.zmark_n);
         ws.disc_n = 0u;
         ws.disc_m = 0ull;
+        ws.zmark_n = 0u;
     }
     __syncwarp();
 }
@@ -1124,7 +1129,7 @@ __device__ __forceinline__ void bu_step(const BfsParams &p, int it, unsigned w0,
         const unsigned fb = __ballot_sync(FULL, f);
         const unsigned zb = __ballot_sync(FULL, ((open >> j) & 1u) && ln[j] == 0);
         if (lane == 0 && (fb | zb)) __stcg(p.mask + w0 + j, mw[j] | fb | zb);
-        if (lane == 0 && zb) atomicAdd(&c->zmarked, unsigned(__popc(zb)));
+        if (lane == 0 && zb) ws.zmark_n += unsigned(__popc(zb));  // added to the counters once, at the level's end
         if (f) {
             p.labels[v[j]] = MP ? par[j] : it + 1;
             nfound++;
@@ -1364,6 +1369,7 @@ __device__ __forceinline__ void init_hist(Smem<THREADS, MP> &sm, unsigned flags)
     if (lane_id() == 0) {
         sm.w[threadIdx.x >> 5].nbuf = 0;
         sm.w[threadIdx.x >> 5].raw_n = 0;
+        sm.w[threadIdx.x >> 5].zmark_n = 0;
         sm.w[threadIdx.x >> 5].disc_n = 0;
         sm.w[threadIdx.x >> 5].disc_m = 0;
     }
