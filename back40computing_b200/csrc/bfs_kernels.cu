@@ -805,6 +805,40 @@ struct DiscoverSink {
     }
 };
 
+// Contract-expand survivors' short lists staged per warp before their gather:
+// the warp's append buffer obuf (idle in contract-expand) holds up to LSTAGE
+// lists as three arrays (starts, lengths, owners), and one positional gather
+// -- one queue reservation -- serves them all.  A reservation per contracted
+// tile (most tiles of a large level contract one or two vertices) made the
+// queue's length counter the level's hot spot.
+constexpr int LSTAGE = 64;
+static_assert(3 * LSTAGE <= OBUF, "the list stage lives in obuf");
+
+// Gathers the staged lists (two per lane) into queue q_out and empties the
+// stage.  Called by all lanes together.
+template <bool MP>
+__device__ __forceinline__ void flush_lists(const BfsParams &p, WarpSmem<MP> &ws, int *q_out, int *pq_out,
+                                         unsigned *qlen_out, uint64_t pol) {
+    const unsigned n = ws.nbuf;
+    if (n == 0u) return;  // warp-uniform
+    int st[4] = {0, 0, 0, 0}, ln[4] = {0, 0, 0, 0}, pr[4] = {0, 0, 0, 0};
+    unsigned has = 0;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const unsigned k = unsigned(j) * 32u + lane_id();
+        if (k < n) {
+            st[j] = ws.obuf[k];
+            ln[j] = ws.obuf[LSTAGE + k];
+            pr[j] = ws.obuf[2 * LSTAGE + k];
+            has |= 1u << j;
+        }
+    }
+    __syncwarp();
+    if (lane_id() == 0) ws.nbuf = 0u;
+    __syncwarp();
+    gather_positional4<MP>(p, ws, has, st, ln, pr, q_out, pq_out, qlen_out, pol);
+}
+
 // Contract-expand: cull and label the edge-frontier elements (label it,
 // contract_expand_atomic/cta.cuh:264-304), then expand the survivors at once:
 // long lists become CTA or warp chunks of the next level (contracted from the
@@ -839,12 +873,48 @@ struct ContractExpandSink {
         WarpSmem<MP> &ws = sm.w[threadIdx.x >> 5];
         if (p.count_raw) count_raw(&ws.raw_n, has, ln);
         const unsigned placed = place4<THREADS>(p, q + 1, has, st, ln, u);
+        const unsigned rest = has & ~placed;
         const int nq = (q + 1) & 1;
-        gather_positional4<MP>(p, ws, has & ~placed, st, ln, u, p.queue[nq], p.pred_queue[nq],
-                               &p.ctr->qlen[(q + 1) & 3], pol);
+        // Stage the short lists; gather when the stage would overflow.
+        const unsigned lt = lanemask_lt();
+        unsigned total = 0, pre[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const unsigned b = __ballot_sync(FULL, (rest >> j) & 1u);
+            pre[j] = total + __popc(b & lt);
+            total += __popc(b);
+        }
+        if (total == 0u) return;  // warp-uniform
+        unsigned n = ws.nbuf;
+        if (n + total > unsigned(LSTAGE)) {
+            flush_lists(p, ws, p.queue[nq], p.pred_queue[nq], &p.ctr->qlen[(q + 1) & 3], pol);
+            n = 0u;
+        }
+        if (total > unsigned(LSTAGE)) {  // more than a stage's worth in one tile: gather them now
+            gather_positional4<MP>(p, ws, rest, st, ln, u, p.queue[nq], p.pred_queue[nq], &p.ctr->qlen[(q + 1) & 3],
+                                   pol);
+            return;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if ((rest >> j) & 1u) {
+                const unsigned k = n + pre[j];
+                ws.obuf[k] = st[j];
+                ws.obuf[LSTAGE + k] = ln[j];
+                ws.obuf[2 * LSTAGE + k] = u[j];
+            }
+        }
+        __syncwarp();
+        if (lane_id() == 0) ws.nbuf = n + total;
+        __syncwarp();
     }
-    // Adds the warp's raw count to the counters; every warp calls it at the phase's end.
-    __device__ __forceinline__ void drain() const { flush_raw(p, sm.w[threadIdx.x >> 5], q + 1); }
+    // Gathers the warp's staged lists and adds its raw count to the counters;
+    // every warp calls it at the phase's end.
+    __device__ __forceinline__ void drain() const {
+        const int nq = (q + 1) & 1;
+        flush_lists(p, sm.w[threadIdx.x >> 5], p.queue[nq], p.pred_queue[nq], &p.ctr->qlen[(q + 1) & 3], pol);
+        flush_raw(p, sm.w[threadIdx.x >> 5], q + 1);
+    }
 };
 
 // Two-phase contract: cull and label (iteration it), then append the survivors
