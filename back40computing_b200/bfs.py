@@ -266,6 +266,17 @@ class _Enactor:
         """Bottom-up steps stage their inputs in shared memory one step ahead (default off)."""
         check(lib().b40c_enactor_set_bottom_up_staging(self._h, int(bool(enable))))
 
+    def set_narrow_levels(self, team_ctas: int, max_frontier: int) -> None:
+        """Contract-expand: levels of at most max_frontier queued edges run on
+        one cluster of team_ctas CTAs (0 turns it off, the default)."""
+        check(lib().b40c_enactor_set_narrow_levels(self._h, int(team_ctas), int(max_frontier)))
+
+    def narrow_team(self) -> int:
+        """CTAs of the cluster narrow levels run on (0: off or none fits)."""
+        t = ctypes.c_int(0)
+        check(lib().b40c_enactor_narrow_team(self._h, ctypes.byref(t)))
+        return t.value
+
     def set_l2_persistence(self, what: int) -> None:
         """0 off, 1 keep the visited mask L2-resident, 2 the mask and the labels."""
         check(lib().b40c_enactor_set_l2_persistence(self._h, int(what)))

@@ -58,7 +58,8 @@ struct alignas(256) Counters {
     unsigned done;       // 1 once the search has finished (per-level variants)
     unsigned long long total_queued;  // sum of frontier lengths (instrumented)
     unsigned retired[4];  // multi-search: searches retired at the start of level q, at [q&3]
-    unsigned pad_e[54];
+    int resume;           // level a full-grid fused launch starts at (set by a narrow launch before it)
+    unsigned pad_e[53];
     // Direction-optimizing expand-contract: the vertices discovered as input of
     // phase q (mf: the sum of their degrees, nf: their number), at [q&3].
     unsigned long long mf[4];
@@ -270,6 +271,10 @@ __device__ __forceinline__ bool grid_barrier(Counters *c, unsigned long long wai
     return grid_barrier(c, wait_ns, smem_flag, gridDim.x, &next);
 }
 
+// ---- cluster barrier -------------------------------------------------------------
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
 // The same barrier with a serial section: the CTA whose arrival completes the
 // count runs serial() with all its threads (it may use __syncthreads) before
 // it publishes the new generation, so serial() sees everything every CTA did

@@ -102,6 +102,10 @@ struct b40c_enactor {
     unsigned long long wait_ns = 5000000000ull;
     int l2_persist = 0;  // b40c_enactor_set_l2_persistence
     bool stage_bu = false;  // b40c_enactor_set_bottom_up_staging
+    int narrow_team = 0;       // b40c_enactor_set_narrow_levels: cluster CTAs asked for (0: off)
+    unsigned narrow_max = 0;   // and its frontier bound
+    int narrow_key = -1;       // launch configuration narrow_got was found for
+    int narrow_got = 0;        // the cluster size used (0: none fits)
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     Counters *d_ctr = nullptr;
@@ -528,6 +532,17 @@ int launch_search(b40c_enactor *e, BfsParams &bp, const KernelConfig &kc, cudaSt
             }
             bp.cta_busy = e->d_busy;
             e->busy_grid = grid;
+        }
+        if (e->narrow_team > 0) {
+            const int key = (kc.threads << 8) | (kc.mark_pred ? 128 : 0) | e->narrow_team;
+            if (e->narrow_key != key) {
+                CUDA_TRY(narrow_team_limit(kc, e->narrow_team, &e->narrow_got), "cluster occupancy query");
+                e->narrow_key = key;
+            }
+            if (e->narrow_got > 0) {
+                bp.narrow_max = e->narrow_max;
+                CUDA_TRY(launch_narrow(bp, kc, e->narrow_got, s), "cluster launch of the narrow BFS kernel");
+            }
         }
         CUDA_TRY(launch_fused(bp, kc, grid, s), "cooperative launch of the fused BFS kernel");
     } else if (variant == B40C_VARIANT_ITERATIVE) {
@@ -1215,6 +1230,27 @@ extern "C" int b40c_enactor_set_bottom_up_staging(b40c_enactor_t *e, int enable)
     clear_error();
     if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
     e->stage_bu = enable != 0;
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_set_narrow_levels(b40c_enactor_t *e, int team_ctas, int max_frontier) {
+    clear_error();
+    if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
+    if (team_ctas < 0 || team_ctas > 16 || max_frontier < 0)
+        return set_error(B40C_ERR_INVALID_VALUE, "narrow levels: team_ctas in [0, 16], max_frontier >= 0");
+    e->narrow_team = team_ctas;
+    e->narrow_max = unsigned(max_frontier);
+    return B40C_SUCCESS;
+}
+
+extern "C" int b40c_enactor_narrow_team(b40c_enactor_t *e, int *team) {
+    clear_error();
+    if (!e || !team) return set_error(B40C_ERR_INVALID_VALUE, "NULL argument");
+    *team = 0;
+    if (e->narrow_team == 0) return B40C_SUCCESS;
+    CUDA_TRY(cudaSetDevice(e->device), "cudaSetDevice");
+    const KernelConfig kc{e->strategy, e->threads, false};
+    CUDA_TRY(narrow_team_limit(kc, e->narrow_team, team), "cluster occupancy query");
     return B40C_SUCCESS;
 }
 

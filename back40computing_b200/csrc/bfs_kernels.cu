@@ -33,8 +33,10 @@
 // (__match_any_sync) and per-CTA history-hash culls drop repeats first
 // (two_phase/contract_atomic/cta.cuh:276-327).
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstddef>
 
 #include "bfs_kernels.cuh"
@@ -296,9 +298,10 @@ __device__ __forceinline__ unsigned place_tier(int4 *table, unsigned *count, int
 // cut into CTA chunks, lists >= warp_th into warp chunks; shorter lists stay
 // with their lanes.  Returns the bits of the lists placed in a chunk table.
 // Called by all lanes together.
+// c: the counters the chunk counts go to (p.ctr, or a narrow launch's copy).
 template <int THREADS>
 __device__ __forceinline__ unsigned place4(const BfsParams &p, int q_next, unsigned has, const int (&st)[4],
-                                           const int (&ln)[4], const int (&pr)[4]) {
+                                           const int (&ln)[4], const int (&pr)[4], Counters *c) {
     constexpr int CH = chunk_edges<THREADS>();
     unsigned cta = 0, wrp = 0;
     int ncta = 0, nw = 0, nc[4];
@@ -320,9 +323,14 @@ __device__ __forceinline__ unsigned place4(const BfsParams &p, int q_next, unsig
     }
     if (!__any_sync(FULL, (cta | wrp) != 0u)) return 0u;
     const int nq = q_next & 1;
-    unsigned placed = place_tier<CH>(p.chunks[nq], &p.ctr->big[q_next & 3], p.chunk_cap, cta, ncta, nc, st, ln, pr);
-    placed |= place_tier<WARP_CHUNK>(p.wchunks[nq], &p.ctr->wch[q_next & 3], p.wchunk_cap, wrp, nw, nc, st, ln, pr);
+    unsigned placed = place_tier<CH>(p.chunks[nq], &c->big[q_next & 3], p.chunk_cap, cta, ncta, nc, st, ln, pr);
+    placed |= place_tier<WARP_CHUNK>(p.wchunks[nq], &c->wch[q_next & 3], p.wchunk_cap, wrp, nw, nc, st, ln, pr);
     return placed;
+}
+template <int THREADS>
+__device__ __forceinline__ unsigned place4(const BfsParams &p, int q_next, unsigned has, const int (&st)[4],
+                                           const int (&ln)[4], const int (&pr)[4]) {
+    return place4<THREADS>(p, q_next, has, st, ln, pr, p.ctr);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1633,7 +1641,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
         if (p.do_alpha) bottom_up = dir.next(p, lc.nf, lc.mf);
         if (leader()) {
             ring_prepare(c, it);
-            c->total_queued += L;
+            atomicAdd(&c->total_queued, (unsigned long long)L);
             log_phase(p, it, L, nch, nw, bottom_up ? 1u : 0u);
         }
         if (bottom_up) {
@@ -1656,16 +1664,91 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
     finish_search(p, it, it);
 }
 
+// Contract-expand level of a narrow launch (at most a few thousand queued
+// edges on one cluster), written for latency: element i of the edge
+// frontier goes to lane i % 32 of warp i / 32 (warps numbered across the
+// cluster's CTAs); the lane claims its vertex with one atomicOr, the row
+// range loaded behind the atomic; lists of warp_th edges and more go to the
+// chunk tables (place4: the next level then belongs to the full grid); the
+// warp reserves queue room for its other lists with one atomicAdd, and each
+// lane copies its own list, the first entries loaded while the reservation
+// is in flight.  No history cache, no probe, no staging: a narrow level is a
+// chain of round trips, and every step the throughput path adds lengthens it.
+// Labels, queue contents (in another order) and counts are ce_level's.
+// c: the level counters (the narrow launch's copy in shared memory).
 template <int THREADS, bool MP>
-__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(BfsParams p) {
+__device__ void ce_narrow_level(const BfsParams &p, Counters *c, int it, unsigned L) {
+    const int *q_in = p.queue[it & 1];
+    const int *pq_in = p.pred_queue[it & 1];
+    const int nq = (it + 1) & 1;
+    int *q_out = p.queue[nq];
+    int *pq_out = p.pred_queue[nq];
+    unsigned *qlen_out = &c->qlen[(it + 1) & 3];
+    const unsigned W = unsigned(grid_warps());
+    const unsigned lane = lane_id();
+    unsigned raw = 0;
+    for (unsigned w = unsigned(global_warp()); w * 32u < L; w += W) {
+        const unsigned i = w * 32u + lane;
+        bool ok = i < L;
+        const int u = ok ? ld_cg(q_in + i) : 0;
+        const int pr = (MP && ok) ? ld_cg(pq_in + i) : 0;
+        if (ok && (unsigned)u >= (unsigned)p.nodes) {
+            atomicOr(&c->error, ERR_BAD_VERTEX);
+            ok = false;
+        }
+        const unsigned bit = 1u << ((unsigned)u & 31u);
+        const unsigned old = ok ? atomicOr(p.mask + ((unsigned)u >> 5), bit) : bit;
+        const int r0 = ok ? __ldg(p.row_offsets + u) : 0;  // issued behind the atomic
+        const int r1 = ok ? __ldg(p.row_offsets + u + 1) : 0;
+        const bool claimed = !(old & bit);
+        if (claimed) p.labels[u] = MP ? pr : it;
+        const int len = claimed ? r1 - r0 : 0;
+        if (p.count_raw) raw += unsigned(len);
+        const int st4[4] = {r0, 0, 0, 0}, ln4[4] = {len, 0, 0, 0}, own4[4] = {u, 0, 0, 0};
+        const unsigned placed = place4<THREADS>(p, it + 1, len > 0 ? 1u : 0u, st4, ln4, own4, c);
+        const int n = placed ? 0 : len;
+        const int incl = warp_inclusive_scan(n);
+        const unsigned total = (unsigned)__shfl_sync(FULL, incl, 31);
+        if (total == 0u) continue;  // warp-uniform
+        int first[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) first[k] = k < n ? __ldg(p.col + r0 + k) : 0;
+        unsigned base = 0;
+        if (lane == 31) base = atomicAdd(qlen_out, total);
+        base = __shfl_sync(FULL, base, 31);
+        const unsigned long long pos = (unsigned long long)base + unsigned(incl - n);
+        for (int k = 0; k < n; k++) {
+            const int v = k < 4 ? first[k] : __ldg(p.col + r0 + k);
+            if (pos + k < (unsigned long long)p.qcap) {
+                q_out[pos + k] = v;
+                if (MP) pq_out[pos + k] = u;
+            } else {
+                atomicOr(&c->error, ERR_OVERFLOW);
+            }
+        }
+    }
+    if (p.count_raw) {
+        raw = __reduce_add_sync(FULL, raw);
+        if (lane == 0 && raw) atomicAdd(&c->raw[(it + 1) & 3], raw);
+    }
+}
+
+// The contract-expand level loop of the full grid.  It starts at
+// Counters::resume: 0, or the first level a narrow launch before it left.
+template <int THREADS, bool MP>
+__device__ __forceinline__ void ce_search(const BfsParams &p) {
     Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
     init_hist(sm, p.cull_flags);
     const uint64_t pol = column_policy(p);
     Counters *c = p.ctr;
     BusyClock clk;
-    int it = 0;
-    LevelCounts lc = read_counts(c, 0, false, sm);
-    for (;;) {
+    int it = __ldcg(&c->resume);
+    LevelCounts lc = read_counts(c, it, false, sm);
+    // A narrow launch before this one raised an error: no level runs.  (A CTA
+    // may also see an error another CTA raised in its first level and leave
+    // at once; the others' grid barrier ends on the error.)
+    const bool failed = ld_relaxed_gpu(&c->error) != 0u;
+    for (; !failed;) {
         clk.start(p);
         const unsigned L = lc.L, nch = lc.nch, nw = lc.nw;
         // raw: the edge frontier before the gather-time cull, so the loop runs
@@ -1673,7 +1756,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
         if (stop_level_loop(p, it, L + nch + nw + lc.raw)) break;
         if (leader()) {
             ring_prepare(c, it);
-            c->total_queued += lc.raw;
+            atomicAdd(&c->total_queued, (unsigned long long)lc.raw);
             log_phase(p, it, lc.raw ? lc.raw : L, nch, nw);
         }
         ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, pol);
@@ -1685,6 +1768,102 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(
     }
     clk.flush(p);
     finish_search(p, it, it);
+}
+
+// A level's counts from counters in shared memory (a narrow launch's).
+__device__ __forceinline__ LevelCounts shared_counts(const Counters *c, int q) {
+    const volatile Counters *v = c;
+    LevelCounts r{};
+    r.L = v->qlen[q & 3];
+    r.nch = v->big[q & 3];
+    r.nw = v->wch[q & 3];
+    r.raw = v->raw[q & 3];
+    return r;
+}
+
+// The contract-expand level loop of a narrow launch: ONE thread-block
+// cluster (gridDim.x CTAs: the helpers spread work over gridDim, so it is
+// the grid) runs the search's first levels with ce_narrow_level while their
+// input is at most p.narrow_max queued edges without chunked lists, and
+// leaves the first larger level to the full-grid launch after it
+// (Counters::resume).  A level of a high-diameter graph is a few thousand
+// edges; on the full grid its time is mostly latency: the grid barrier, the
+// counts read back from L2 after it, the queue reservation's L2 atomic.
+// Here the levels end at the cluster's hardware barrier, and the per-level
+// counters live in CTA 0's shared memory, which every CTA of the cluster
+// reaches as distributed shared memory: reservations and count reads are
+// shared-memory round trips.  CTA 0 copies the counters in from global memory
+// at the start and the ring entries and error bits back at the end (the
+// total_queued sum stays in global memory).  Every CTA leaves the loop on the
+// same counts, read after the same barrier, never on the error word: the
+// hardware barrier has no timeout, and a CTA missing from it would stall the
+// others.
+template <int THREADS, bool MP>
+__device__ __forceinline__ void ce_narrow_search(const BfsParams &p) {
+    __shared__ Counters shared_ctr;  // CTA 0's copy serves the cluster
+    Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
+    Counters *g = p.ctr;
+    constexpr int WORDS = int(offsetof(Counters, sticky) / 4);
+    if (blockIdx.x == 0) {
+        const unsigned *from = reinterpret_cast<const unsigned *>(g);
+        unsigned *to = reinterpret_cast<unsigned *>(&shared_ctr);
+        for (int i = threadIdx.x; i < WORDS; i += THREADS) to[i] = __ldcg(from + i);
+    }
+    cluster_sync_all();
+    Counters *c = cooperative_groups::this_cluster().map_shared_rank(&shared_ctr, 0);
+    int it = __ldcg(&g->resume);
+    if (threadIdx.x == 0) sm.lc = shared_counts(c, it);
+    __syncthreads();
+    LevelCounts lc = sm.lc;
+    for (;;) {
+        const unsigned L = lc.L, nch = lc.nch, nw = lc.nw;
+        if (L + nch + nw + lc.raw == 0u) break;
+        if (level_limit_hit(it, p.nodes)) {
+            if (leader()) atomicOr(&c->error, ERR_LEVEL_LIMIT);
+            break;
+        }
+        // hand over levels with chunked lists, levels above the bound, and a
+        // queue that overflowed (its entries beyond qcap were never written;
+        // the full-grid launch sees the error and stops)
+        if (nch + nw != 0u || L > p.narrow_max || (long long)L > p.qcap) break;
+        if (leader()) {
+            ring_prepare(c, it);
+            atomicAdd(&g->total_queued, (unsigned long long)lc.raw);
+            log_phase(p, it, lc.raw ? lc.raw : L, nch, nw);
+        }
+        ce_narrow_level<THREADS, MP>(p, c, it, L);
+        log_work_end(p, it);
+        cluster_sync_all();
+        if (threadIdx.x == 0) sm.lc = shared_counts(c, it + 1);
+        __syncthreads();
+        lc = sm.lc;
+        it++;
+    }
+    cluster_sync_all();  // no CTA touches CTA 0's counters after this
+    if (blockIdx.x == 0 && threadIdx.x < 4) {
+        const int k = threadIdx.x;
+        g->qlen[k] = shared_ctr.qlen[k];
+        g->steal[k] = shared_ctr.steal[k];
+        g->big[k] = shared_ctr.big[k];
+        g->wch[k] = shared_ctr.wch[k];
+        g->raw[k] = shared_ctr.raw[k];
+        if (k == 0) {
+            if (shared_ctr.error) atomicOr(&g->error, shared_ctr.error);
+            g->resume = it;  // the full-grid launch ends the search (or finds it ended)
+        }
+    }
+}
+
+template <int THREADS, bool MP>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(BfsParams p) {
+    ce_search<THREADS, MP>(p);
+}
+
+// Contract-expand levels of small frontiers on one thread-block cluster,
+// launched before ce_fused_kernel.
+template <int THREADS, bool MP>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_narrow_kernel(BfsParams p) {
+    ce_narrow_search<THREADS, MP>(p);
 }
 
 // Fused two-phase: contract and expand phases alternate across grid barriers
@@ -1708,7 +1887,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
         const bool cull = gather_cull(level_edges<THREADS>(lc));
         if (leader()) {
             ring_prepare(c, qi);
-            c->total_queued += lc.raw;
+            atomicAdd(&c->total_queued, (unsigned long long)lc.raw);
             log_phase(p, qi, lc.raw ? lc.raw : L, nch, nw);
         }
         tp_contract<THREADS, MP>(p, it, qi, L, nch, nw, sm, pol);
@@ -1761,7 +1940,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
         if (stop_level_loop(p, it, L + nch + nw + lc.raw)) break;
         if (leader()) {
             ring_prepare(c, q);
-            c->total_queued += lc.raw;
+            atomicAdd(&c->total_queued, (unsigned long long)lc.raw);
             log_phase(p, q, lc.raw ? lc.raw : L, nch, nw);
         }
         // the level's edge frontier as the reference counts it (before the gather-time cull)
@@ -2121,6 +2300,67 @@ static cudaError_t allow_smem(const void *fn, size_t bytes) {
 
 static KernelFn pick_fused(const KernelConfig &kc) {
     return kc.mark_pred ? fused_fn_t<true>(kc.threads, kc.strategy) : fused_fn_t<false>(kc.threads, kc.strategy);
+}
+
+template <bool MP>
+static KernelFn narrow_fn_t(int threads, int strategy) {
+    if (strategy != STRATEGY_CONTRACT_EXPAND) return nullptr;
+    switch (threads) {
+    case 128: return ce_narrow_kernel<128, MP>;
+    case 512: return ce_narrow_kernel<512, MP>;
+    default: return ce_narrow_kernel<256, MP>;
+    }
+}
+static KernelFn pick_narrow(const KernelConfig &kc) {
+    return kc.mark_pred ? narrow_fn_t<true>(kc.threads, kc.strategy) : narrow_fn_t<false>(kc.threads, kc.strategy);
+}
+
+static cudaLaunchConfig_t narrow_config(const KernelConfig &kc, int team, cudaStream_t stream,
+                                        cudaLaunchAttribute *attr) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(team));
+    cfg.blockDim = dim3(unsigned(kc.threads));
+    cfg.dynamicSmemBytes = fused_smem_bytes(kc);
+    cfg.stream = stream;
+    attr->id = cudaLaunchAttributeClusterDimension;
+    attr->val.clusterDim.x = unsigned(team);
+    attr->val.clusterDim.y = 1;
+    attr->val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+cudaError_t narrow_team_limit(const KernelConfig &kc, int want, int *team) {
+    *team = 0;
+    KernelFn fn = pick_narrow(kc);
+    if (!fn || want < 1) return cudaSuccess;
+    cudaError_t e = allow_smem((const void *)fn, fused_smem_bytes(kc));
+    if (e) return e;
+    if ((e = cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1))) return e;
+    for (int t = std::min(want, 16); t >= 1; t--) {
+        cudaLaunchAttribute attr;
+        cudaLaunchConfig_t cfg = narrow_config(kc, t, nullptr, &attr);
+        int clusters = 0;
+        if ((e = cudaOccupancyMaxActiveClusters(&clusters, (const void *)fn, &cfg))) {
+            cudaGetLastError();  // a size the device refuses: try a smaller one
+            continue;
+        }
+        if (clusters >= 1) {
+            *team = t;
+            return cudaSuccess;
+        }
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_narrow(const BfsParams &p, const KernelConfig &kc, int team, cudaStream_t stream) {
+    KernelFn fn = pick_narrow(kc);
+    if (!fn || team < 1 || team > 16) return cudaErrorInvalidValue;
+    cudaLaunchAttribute attr;
+    const cudaLaunchConfig_t cfg = narrow_config(kc, team, stream, &attr);
+    BfsParams arg = p;
+    return cudaLaunchKernelEx(&cfg, fn, arg);
 }
 
 struct LevelFns {

@@ -82,6 +82,10 @@ struct BfsParams {
     // 0: only phases that cull while they gather count it (their queue
     // alone would stop the level loop early).
     int count_raw;
+    // Narrow launch (one thread-block cluster): it runs levels while their
+    // input is an edge-frontier queue of at most narrow_max entries with no
+    // chunked lists, and leaves the rest to the full-grid launch after it.
+    unsigned narrow_max;
 };
 
 // Padding of the device arrays a staged bottom-up step copies in whole
@@ -130,6 +134,14 @@ cudaError_t launch_csr_check(const int *row_offsets, const int *col, int nodes, 
                              unsigned long long *out, cudaStream_t stream);
 // Cooperative launch of the persistent kernel that runs every BFS level.
 cudaError_t launch_fused(const BfsParams &p, const KernelConfig &kc, int grid, cudaStream_t stream);
+// Whether strategy kc.strategy has a narrow kernel (the levels of small
+// frontiers on one thread-block cluster), and the largest cluster of at most
+// `want` CTAs it can launch (*team, 0 when none fits or there is no kernel).
+cudaError_t narrow_team_limit(const KernelConfig &kc, int want, int *team);
+// The narrow launch: one cluster of `team` CTAs runs the search's levels from
+// Counters::resume while their frontiers stay within p.narrow_max, then
+// writes the next level to Counters::resume for launch_fused's kernel.
+cudaError_t launch_narrow(const BfsParams &p, const KernelConfig &kc, int team, cudaStream_t stream);
 // Builds a graph whose conditional-while node runs one BFS level per pass:
 // level kernel(s), then a control kernel that advances the iteration and
 // sets the loop condition on the device.  p.cond_handle is filled in.

@@ -1,0 +1,125 @@
+"""Narrow levels: contract-expand searches whose small levels run on one
+thread-block cluster (b40c_enactor_set_narrow_levels) give the oracle's labels
+and valid predecessors, and the same search depth and total_queued as the
+full-grid search, whether the handover to the full grid comes at the source,
+in the middle of the search, or never; other strategies ignore the option."""
+from __future__ import annotations
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CE = 1
+
+
+def bfs_mod():
+    import back40computing_b200 as b
+    return b
+
+
+def _graphs(b):
+    return [
+        (b.grid2d(200), [100 * 200 + 100, 0]),
+        (b.grid3d(24), [0, 12 * 24 * 24 + 12 * 24 + 12]),
+        (b.rmat(15, 8, seed=4), None),
+        (b.erdos_renyi(3001, 5.0 / 3000, seed=2), None),
+    ]
+
+
+def _search(b, prob, src, team, max_frontier, threads=0):
+    en = b.make_enactor(CE, INSTRUMENT=True)
+    if threads:
+        en.set_policy(cta_threads=threads)
+    en.set_narrow_levels(team, max_frontier)
+    b.check(prob.Reset(en.GetFrontierType(), 1.3))
+    b.check(en.EnactSearch(prob, int(src)))
+    return prob.labels(), en.GetStatistics(), en
+
+
+@pytest.mark.parametrize("team", [16, 8, 3, 1])
+def test_narrow_levels_match_oracle(cuda_device, oracle, team):
+    b = bfs_mod()
+    for g, sources in _graphs(b):
+        prob = b.CsrProblem(False).from_graph(g)
+        srcs = sources if sources is not None else [int(s) for s in g.sample_sources(2, 41)]
+        for s in srcs:
+            ref, _ = oracle.bfs(g, int(s))
+            _, full_stats, _ = _search(b, prob, s, 0, 0)
+            # handover at the source, after a few levels, never
+            for max_frontier in (0, 200, 1 << 24):
+                labels, stats, en = _search(b, prob, s, team, max_frontier)
+                assert oracle.first_mismatch(labels, ref) == -1, (g.name, int(s), team, max_frontier)
+                assert stats[:2] == full_stats[:2], (g.name, int(s), team, max_frontier)
+                assert 1 <= en.narrow_team() <= team
+
+
+@pytest.mark.parametrize("threads", [128, 256, 512])
+def test_narrow_levels_policies_and_predecessors(cuda_device, oracle, threads):
+    b = bfs_mod()
+    g = b.grid2d(128)
+    src = 64 * 128 + 64
+    ref, _ = oracle.bfs(g, src)
+    prob = b.CsrProblem(False).from_graph(g)
+    labels, _, _ = _search(b, prob, src, 16, 1 << 20, threads=threads)
+    assert oracle.first_mismatch(labels, ref) == -1
+    pprob = b.CsrProblem(True).from_graph(g)
+    preds, _, _ = _search(b, pprob, src, 16, 1 << 20, threads=threads)
+    assert preds[src] == -2
+    bad, reason = oracle.check_predecessors(g, preds, ref)
+    assert bad == -1, f"node {bad} fails check {reason}"
+
+
+def test_narrow_levels_are_logged(cuda_device, oracle):
+    """The level log holds every level, the narrow ones included, in order,
+    each with its work-end time between its start and the next level's."""
+    b = bfs_mod()
+    g = b.grid2d(96)
+    src = 48 * 96 + 48
+    ref, _ = oracle.bfs(g, src)
+    prob = b.CsrProblem(False).from_graph(g)
+    en = b.make_enactor(CE)
+    en.set_narrow_levels(8, 40)  # the first levels narrow, then the full grid
+    en.set_level_log(True)
+    b.check(prob.Reset(en.GetFrontierType(), 1.3))
+    b.check(en.EnactSearch(prob, src))
+    assert oracle.first_mismatch(prob.labels(), ref) == -1
+    log = en.level_log()
+    _, depth, _ = en.GetStatistics()
+    assert len(log) == depth + 2  # levels 0..depth and the end marker
+    for cur, nxt in zip(log[:-1], log[1:]):
+        assert cur["start_ns"] <= cur["work_end_ns"] <= nxt["start_ns"]
+
+
+def test_narrow_levels_overflow_and_recovery(cuda_device, oracle):
+    b = bfs_mod()
+    g = b.grid2d(256)
+    src = 128 * 256 + 128
+    prob = b.CsrProblem(False).from_graph(g)
+    en = b.make_enactor(CE)
+    en.set_narrow_levels(16, 1 << 20)
+    b.check(prob.Reset(en.GetFrontierType(), 0.0005))
+    assert en.EnactSearch(prob, src) == b.bfs.cudaErrorInvalidConfiguration
+    ref, _ = oracle.bfs(g, src)
+    b.check(prob.Reset(en.GetFrontierType(), 1.3))
+    b.check(en.EnactSearch(prob, src))
+    assert oracle.first_mismatch(prob.labels(), ref) == -1
+
+
+def test_narrow_levels_arguments_and_other_strategies(cuda_device, oracle):
+    b = bfs_mod()
+    en = b.make_enactor(CE)
+    for bad in ((17, 100), (-1, 100), (4, -1)):
+        with pytest.raises(b.BfsError):
+            en.set_narrow_levels(*bad)
+    assert en.narrow_team() == 0
+    g = b.grid2d(64)
+    src = 32 * 64 + 32
+    ref, _ = oracle.bfs(g, src)
+    prob = b.CsrProblem(False).from_graph(g)
+    for strategy in (0, 2, 3):
+        other = b.make_enactor(strategy)
+        other.set_narrow_levels(16, 1 << 20)
+        assert other.narrow_team() == 0
+        b.check(prob.Reset(other.GetFrontierType(), 1.3))
+        b.check(other.EnactSearch(prob, src))
+        assert oracle.first_mismatch(prob.labels(), ref) == -1
