@@ -56,7 +56,7 @@ SIGNATURES = {
     "b40c_enactor_set_wait_limit_us": (c_int, [c_void_p, c_longlong]),
     "b40c_enactor_set_l2_persistence": (c_int, [c_void_p, c_int]),
     "b40c_enactor_set_bottom_up_staging": (c_int, [c_void_p, c_int]),
-    "b40c_enactor_set_narrow_levels": (c_int, [c_void_p, c_int, c_int]),
+    "b40c_enactor_set_narrow_levels": (c_int, [c_void_p, c_int, c_int, c_int]),
     "b40c_enactor_narrow_team": (c_int, [c_void_p, POINTER(c_int)]),
     "b40c_graph_grid2d": (c_int, [c_int, c_int, POINTER(CsrT)]),
     "b40c_graph_grid3d": (c_int, [c_int, c_int, POINTER(CsrT)]),

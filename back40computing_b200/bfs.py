@@ -266,10 +266,12 @@ class _Enactor:
         """Bottom-up steps stage their inputs in shared memory one step ahead (default off)."""
         check(lib().b40c_enactor_set_bottom_up_staging(self._h, int(bool(enable))))
 
-    def set_narrow_levels(self, team_ctas: int, max_frontier: int) -> None:
-        """Contract-expand: levels of at most max_frontier queued edges run on
-        one cluster of team_ctas CTAs (0 turns it off, the default)."""
-        check(lib().b40c_enactor_set_narrow_levels(self._h, int(team_ctas), int(max_frontier)))
+    def set_narrow_levels(self, team_ctas: int, max_frontier: int, grid_frontier: int = 0) -> None:
+        """Contract-expand: the first levels of at most max_frontier queued
+        edges run on one cluster of team_ctas CTAs (0: none), and full-grid
+        levels of at most grid_frontier queued edges run the latency-first
+        level body (0: none).  Both off by default."""
+        check(lib().b40c_enactor_set_narrow_levels(self._h, int(team_ctas), int(max_frontier), int(grid_frontier)))
 
     def narrow_team(self) -> int:
         """CTAs of the cluster narrow levels run on (0: off or none fits)."""

@@ -104,6 +104,7 @@ struct b40c_enactor {
     bool stage_bu = false;  // b40c_enactor_set_bottom_up_staging
     int narrow_team = 0;       // b40c_enactor_set_narrow_levels: cluster CTAs asked for (0: off)
     unsigned narrow_max = 0;   // and its frontier bound
+    unsigned flat_max = 0;     // full-grid levels with the latency-first body (0: none)
     int narrow_key = -1;       // launch configuration narrow_got was found for
     int narrow_got = 0;        // the cluster size used (0: none fits)
     cudaStream_t stream = nullptr;
@@ -533,6 +534,7 @@ int launch_search(b40c_enactor *e, BfsParams &bp, const KernelConfig &kc, cudaSt
             bp.cta_busy = e->d_busy;
             e->busy_grid = grid;
         }
+        if (kc.strategy == B40C_CONTRACT_EXPAND) bp.flat_max = e->flat_max;
         if (e->narrow_team > 0) {
             const int key = (kc.threads << 8) | (kc.mark_pred ? 128 : 0) | e->narrow_team;
             if (e->narrow_key != key) {
@@ -1233,13 +1235,16 @@ extern "C" int b40c_enactor_set_bottom_up_staging(b40c_enactor_t *e, int enable)
     return B40C_SUCCESS;
 }
 
-extern "C" int b40c_enactor_set_narrow_levels(b40c_enactor_t *e, int team_ctas, int max_frontier) {
+extern "C" int b40c_enactor_set_narrow_levels(b40c_enactor_t *e, int team_ctas, int max_frontier,
+                                              int grid_frontier) {
     clear_error();
     if (!e) return set_error(B40C_ERR_INVALID_VALUE, "NULL enactor");
-    if (team_ctas < 0 || team_ctas > 16 || max_frontier < 0)
-        return set_error(B40C_ERR_INVALID_VALUE, "narrow levels: team_ctas in [0, 16], max_frontier >= 0");
+    if (team_ctas < 0 || team_ctas > 16 || max_frontier < 0 || grid_frontier < 0)
+        return set_error(B40C_ERR_INVALID_VALUE,
+                         "narrow levels: team_ctas in [0, 16], max_frontier >= 0, grid_frontier >= 0");
     e->narrow_team = team_ctas;
     e->narrow_max = unsigned(max_frontier);
+    e->flat_max = unsigned(grid_frontier);
     return B40C_SUCCESS;
 }
 

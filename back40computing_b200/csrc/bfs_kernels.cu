@@ -1718,7 +1718,88 @@ __device__ void ce_narrow_level(const BfsParams &p, Counters *c, int it, unsigne
         base = __shfl_sync(FULL, base, 31);
         const unsigned long long pos = (unsigned long long)base + unsigned(incl - n);
         for (int k = 0; k < n; k++) {
-            const int v = k < 4 ? first[k] : __ldg(p.col + r0 + k);
+            const int v = k == 0 ? first[0] : k == 1 ? first[1] : k == 2 ? first[2] : k == 3 ? first[3]
+                                                                                          : __ldg(p.col + r0 + k);
+            if (pos + k < (unsigned long long)p.qcap) {
+                q_out[pos + k] = v;
+                if (MP) pq_out[pos + k] = u;
+            } else {
+                atomicOr(&c->error, ERR_OVERFLOW);
+            }
+        }
+    }
+    if (p.count_raw) {
+        raw = __reduce_add_sync(FULL, raw);
+        if (lane == 0 && raw) atomicAdd(&c->raw[(it + 1) & 3], raw);
+    }
+}
+
+// Contract-expand level on the full grid for levels of about one queued edge
+// per thread (at most p.flat_max): ce_narrow_level's latency-first body, with
+// element i going to thread i / G of CTA i % G (G = gridDim.x: a small level
+// spreads over every SM), in rounds of G x THREADS elements.  One element per
+// thread and round: these levels are chains of round trips whose length is
+// set by the instructions between them, and a body with 4 elements in flight
+// measured slower on every lattice level, the small ones most.  Each CTA
+// reserves the queue room of its round with ONE atomicAdd, scanned over its
+// warps in shared memory: per-warp reservations would put thousands of
+// atomics on the queue length per level.  Labels, queue contents (in another
+// order) and counts are ce_level's.
+template <int THREADS, bool MP>
+__device__ void ce_flat_level(const BfsParams &p, int it, unsigned L, Smem<THREADS, MP> &sm) {
+    constexpr int NW = THREADS / 32;
+    Counters *c = p.ctr;
+    const int *q_in = p.queue[it & 1];
+    const int *pq_in = p.pred_queue[it & 1];
+    const int nq = (it + 1) & 1;
+    int *q_out = p.queue[nq];
+    int *pq_out = p.pred_queue[nq];
+    unsigned *qlen_out = &c->qlen[(it + 1) & 3];
+    const unsigned warp = threadIdx.x >> 5, lane = lane_id();
+    const unsigned long long G = gridDim.x, round = G * THREADS;
+    unsigned raw = 0;
+    for (unsigned long long r0 = 0; r0 < L; r0 += round) {  // CTA-uniform
+        const unsigned long long i = r0 + (unsigned long long)threadIdx.x * G + blockIdx.x;
+        bool ok = i < L;
+        const int u = ok ? ld_cg(q_in + i) : 0;
+        const int pr = (MP && ok) ? ld_cg(pq_in + i) : 0;
+        if (ok && (unsigned)u >= (unsigned)p.nodes) {
+            atomicOr(&c->error, ERR_BAD_VERTEX);
+            ok = false;
+        }
+        const unsigned bit = 1u << ((unsigned)u & 31u);
+        const unsigned old = ok ? atomicOr(p.mask + ((unsigned)u >> 5), bit) : bit;
+        const int r0v = ok ? __ldg(p.row_offsets + u) : 0;  // issued behind the atomic
+        const int r1v = ok ? __ldg(p.row_offsets + u + 1) : 0;
+        const bool claimed = !(old & bit);
+        if (claimed) p.labels[u] = MP ? pr : it;
+        const int len = claimed ? r1v - r0v : 0;
+        if (p.count_raw) raw += unsigned(len);
+        const int st4[4] = {r0v, 0, 0, 0}, ln4[4] = {len, 0, 0, 0}, own4[4] = {u, 0, 0, 0};
+        const unsigned placed = place4<THREADS>(p, it + 1, len > 0 ? 1u : 0u, st4, ln4, own4);
+        const int n = placed ? 0 : len;
+        int first[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) first[k] = k < n ? __ldg(p.col + r0v + k) : 0;
+        const int incl = warp_inclusive_scan(n);
+        if (lane == 31) sm.w[warp].gofs[0] = incl;  // the warp's total
+        __syncthreads();
+        if (warp == 0) {
+            const int t = lane < unsigned(NW) ? sm.w[lane].gofs[0] : 0;
+            const int winc = warp_inclusive_scan(t);
+            const unsigned total = (unsigned)__shfl_sync(FULL, winc, 31);
+            unsigned base = 0;
+            if (lane == 0 && total) base = atomicAdd(qlen_out, total);
+            base = __shfl_sync(FULL, base, 0);
+            if (lane < unsigned(NW)) sm.w[lane].gofs[1] = int(base + unsigned(winc - t));
+        }
+        __syncthreads();
+        // (the next round writes gofs[0] only after every warp has read gofs[1]:
+        // its first __syncthreads waits for them)
+        const unsigned long long pos = (unsigned long long)(unsigned)sm.w[warp].gofs[1] + unsigned(incl - n);
+        for (int k = 0; k < n; k++) {
+            const int v = k == 0 ? first[0] : k == 1 ? first[1] : k == 2 ? first[2] : k == 3 ? first[3]
+                                                                                          : __ldg(p.col + r0v + k);
             if (pos + k < (unsigned long long)p.qcap) {
                 q_out[pos + k] = v;
                 if (MP) pq_out[pos + k] = u;
@@ -1759,7 +1840,10 @@ __device__ __forceinline__ void ce_search(const BfsParams &p) {
             atomicAdd(&c->total_queued, (unsigned long long)lc.raw);
             log_phase(p, it, lc.raw ? lc.raw : L, nch, nw);
         }
-        ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, pol);
+        if (nch + nw == 0u && L <= p.flat_max)
+            ce_flat_level<THREADS, MP>(p, it, L, sm);
+        else
+            ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, pol);
         clk.stop(p);
         log_work_end(p, it);
         if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, it + 1, false))) break;

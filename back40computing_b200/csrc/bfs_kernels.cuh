@@ -86,6 +86,9 @@ struct BfsParams {
     // input is an edge-frontier queue of at most narrow_max entries with no
     // chunked lists, and leaves the rest to the full-grid launch after it.
     unsigned narrow_max;
+    // Full-grid levels of at most flat_max queued edges without chunked lists
+    // run contract-expand's latency-first body (ce_flat_level); 0: never.
+    unsigned flat_max;
 };
 
 // Padding of the device arrays a staged bottom-up step copies in whole

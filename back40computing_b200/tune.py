@@ -31,6 +31,10 @@ CTA_THREADS = (128, 256, 512)
 WARP_THRESHOLDS = (32, 64, 128, 256)
 CTA_THRESHOLDS = (512, 1024, 4096)
 DIRECTIONS = ((0, 0), (14, 24), (6, 24))  # (alpha, beta); (0, 0) = top-down only
+# Contract-expand narrow levels (team_ctas, max_frontier, grid_frontier):
+# off; the first levels on a 16-CTA cluster; full-grid levels of up to about
+# one edge per thread with the latency-first body; both.
+NARROW = ((0, 0, 0), (16, 32768, 0), (0, 0, 262144), (16, 8192, 262144), (16, 32768, 262144))
 # The library's defaults for expand-contract searches and batches.
 DEFAULT_POLICY = {"cta_threads": 512, "warp_gather_threshold": 128, "cta_gather_threshold": 1024,
                   "alpha": 14, "beta": 24}
@@ -80,15 +84,19 @@ def is_symmetric(g: CsrGraph, chunk: int = 1 << 24) -> bool:
 
 
 def candidates(strategy: int = 0, directions: bool = True) -> list[dict]:
-    """Policy grid; the direction switch exists for expand-contract only."""
+    """Policy grid; the direction switch exists for expand-contract only, the
+    narrow levels for contract-expand only."""
     dirs = DIRECTIONS if (directions and strategy == 0) else ((None, None),)
+    narrow = NARROW if strategy == 1 else (None,)
     out = []
-    for t, w, c, (a, bb) in itertools.product(CTA_THREADS, WARP_THRESHOLDS, CTA_THRESHOLDS, dirs):
+    for t, w, c, (a, bb), nl in itertools.product(CTA_THREADS, WARP_THRESHOLDS, CTA_THRESHOLDS, dirs, narrow):
         if c < w:
             continue
         p = {"cta_threads": t, "warp_gather_threshold": w, "cta_gather_threshold": c}
         if a is not None:
             p["alpha"], p["beta"] = a, bb
+        if nl is not None:
+            p["narrow"] = list(nl)
         out.append(p)
     return out
 
@@ -139,6 +147,8 @@ def apply_enactor_policy(enactor, policy: dict) -> None:
                        cta_gather_threshold=policy["cta_gather_threshold"])
     if "alpha" in policy:
         enactor.set_direction_optimizing(policy["alpha"], policy["beta"])
+    if "narrow" in policy:
+        enactor.set_narrow_levels(*policy["narrow"])
 
 
 def apply_batch_policy(batch, policy: dict) -> None:

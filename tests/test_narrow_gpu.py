@@ -1,8 +1,10 @@
-"""Narrow levels: contract-expand searches whose small levels run on one
-thread-block cluster (b40c_enactor_set_narrow_levels) give the oracle's labels
-and valid predecessors, and the same search depth and total_queued as the
-full-grid search, whether the handover to the full grid comes at the source,
-in the middle of the search, or never; other strategies ignore the option."""
+"""Narrow levels (b40c_enactor_set_narrow_levels): contract-expand searches
+whose small levels run on one thread-block cluster, and whose small full-grid
+levels run the latency-first level body, give the oracle's labels and valid
+predecessors, and the same search depth and total_queued as the plain search,
+whether the handover to the full grid comes at the source, in the middle of
+the search, or never, and whichever body each full-grid level runs; other
+strategies ignore the option."""
 from __future__ import annotations
 
 import pytest
@@ -26,31 +28,35 @@ def _graphs(b):
     ]
 
 
-def _search(b, prob, src, team, max_frontier, threads=0):
+def _search(b, prob, src, team, max_frontier, grid_frontier=0, threads=0):
     en = b.make_enactor(CE, INSTRUMENT=True)
     if threads:
         en.set_policy(cta_threads=threads)
-    en.set_narrow_levels(team, max_frontier)
+    en.set_narrow_levels(team, max_frontier, grid_frontier)
     b.check(prob.Reset(en.GetFrontierType(), 1.3))
     b.check(en.EnactSearch(prob, int(src)))
     return prob.labels(), en.GetStatistics(), en
 
 
-@pytest.mark.parametrize("team", [16, 8, 3, 1])
+@pytest.mark.parametrize("team", [16, 8, 3, 1, 0])
 def test_narrow_levels_match_oracle(cuda_device, oracle, team):
     b = bfs_mod()
+    # (cluster bound, full-grid latency-first bound): handover at the source,
+    # after a few levels, never; full-grid levels all tiled, all latency-first,
+    # or mixed
+    settings = [(0, 0), (200, 0), (1 << 24, 0), (0, 1 << 24), (200, 1 << 24), (200, 700)]
     for g, sources in _graphs(b):
         prob = b.CsrProblem(False).from_graph(g)
         srcs = sources if sources is not None else [int(s) for s in g.sample_sources(2, 41)]
         for s in srcs:
             ref, _ = oracle.bfs(g, int(s))
-            _, full_stats, _ = _search(b, prob, s, 0, 0)
-            # handover at the source, after a few levels, never
-            for max_frontier in (0, 200, 1 << 24):
-                labels, stats, en = _search(b, prob, s, team, max_frontier)
-                assert oracle.first_mismatch(labels, ref) == -1, (g.name, int(s), team, max_frontier)
-                assert stats[:2] == full_stats[:2], (g.name, int(s), team, max_frontier)
-                assert 1 <= en.narrow_team() <= team
+            _, plain_stats, _ = _search(b, prob, s, 0, 0)
+            for max_frontier, grid_frontier in settings:
+                labels, stats, en = _search(b, prob, s, team, max_frontier, grid_frontier)
+                case = (g.name, int(s), team, max_frontier, grid_frontier)
+                assert oracle.first_mismatch(labels, ref) == -1, case
+                assert stats[:2] == plain_stats[:2], case
+                assert (1 <= en.narrow_team() <= team) if team else en.narrow_team() == 0
 
 
 @pytest.mark.parametrize("threads", [128, 256, 512])
@@ -60,13 +66,14 @@ def test_narrow_levels_policies_and_predecessors(cuda_device, oracle, threads):
     src = 64 * 128 + 64
     ref, _ = oracle.bfs(g, src)
     prob = b.CsrProblem(False).from_graph(g)
-    labels, _, _ = _search(b, prob, src, 16, 1 << 20, threads=threads)
-    assert oracle.first_mismatch(labels, ref) == -1
     pprob = b.CsrProblem(True).from_graph(g)
-    preds, _, _ = _search(b, pprob, src, 16, 1 << 20, threads=threads)
-    assert preds[src] == -2
-    bad, reason = oracle.check_predecessors(g, preds, ref)
-    assert bad == -1, f"node {bad} fails check {reason}"
+    for team, max_frontier, grid_frontier in ((16, 1 << 20, 0), (0, 0, 1 << 20), (16, 100, 1 << 20)):
+        labels, _, _ = _search(b, prob, src, team, max_frontier, grid_frontier, threads=threads)
+        assert oracle.first_mismatch(labels, ref) == -1
+        preds, _, _ = _search(b, pprob, src, team, max_frontier, grid_frontier, threads=threads)
+        assert preds[src] == -2
+        bad, reason = oracle.check_predecessors(g, preds, ref)
+        assert bad == -1, f"node {bad} fails check {reason}"
 
 
 def test_narrow_levels_are_logged(cuda_device, oracle):
@@ -90,13 +97,14 @@ def test_narrow_levels_are_logged(cuda_device, oracle):
         assert cur["start_ns"] <= cur["work_end_ns"] <= nxt["start_ns"]
 
 
-def test_narrow_levels_overflow_and_recovery(cuda_device, oracle):
+@pytest.mark.parametrize("setting", [(16, 1 << 20, 0), (0, 0, 1 << 20)])
+def test_narrow_levels_overflow_and_recovery(cuda_device, oracle, setting):
     b = bfs_mod()
     g = b.grid2d(256)
     src = 128 * 256 + 128
     prob = b.CsrProblem(False).from_graph(g)
     en = b.make_enactor(CE)
-    en.set_narrow_levels(16, 1 << 20)
+    en.set_narrow_levels(*setting)
     b.check(prob.Reset(en.GetFrontierType(), 0.0005))
     assert en.EnactSearch(prob, src) == b.bfs.cudaErrorInvalidConfiguration
     ref, _ = oracle.bfs(g, src)
@@ -108,7 +116,7 @@ def test_narrow_levels_overflow_and_recovery(cuda_device, oracle):
 def test_narrow_levels_arguments_and_other_strategies(cuda_device, oracle):
     b = bfs_mod()
     en = b.make_enactor(CE)
-    for bad in ((17, 100), (-1, 100), (4, -1)):
+    for bad in ((17, 100, 0), (-1, 100, 0), (4, -1, 0), (4, 100, -1)):
         with pytest.raises(b.BfsError):
             en.set_narrow_levels(*bad)
     assert en.narrow_team() == 0
@@ -118,7 +126,7 @@ def test_narrow_levels_arguments_and_other_strategies(cuda_device, oracle):
     prob = b.CsrProblem(False).from_graph(g)
     for strategy in (0, 2, 3):
         other = b.make_enactor(strategy)
-        other.set_narrow_levels(16, 1 << 20)
+        other.set_narrow_levels(16, 1 << 20, 1 << 20)
         assert other.narrow_team() == 0
         b.check(prob.Reset(other.GetFrontierType(), 1.3))
         b.check(other.EnactSearch(prob, src))

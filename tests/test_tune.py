@@ -14,6 +14,28 @@ def test_candidates_cover_the_knobs():
     assert {(c["alpha"], c["beta"]) for c in ec} == set(tune.DIRECTIONS)
     assert all("alpha" not in c for c in tune.candidates(1))  # no direction switch off expand-contract
     assert all(c["cta_gather_threshold"] >= c["warp_gather_threshold"] for c in ec)
+    # narrow levels: contract-expand only, every setting with every other knob
+    ce = tune.candidates(1)
+    assert {tuple(c["narrow"]) for c in ce} == set(tune.NARROW)
+    assert len(ce) == len(tune.candidates(2)) * len(tune.NARROW)
+    assert all("narrow" not in c for s in (0, 2, 3) for c in tune.candidates(s))
+
+
+def test_apply_enactor_policy_sets_every_knob():
+    from back40computing_b200 import tune
+
+    class Rec:
+        def __init__(self):
+            self.calls = []
+
+        def __getattr__(self, name):
+            return lambda *a, **k: self.calls.append((name, a, k))
+
+    r = Rec()
+    tune.apply_enactor_policy(r, {"cta_threads": 512, "warp_gather_threshold": 128, "cta_gather_threshold": 4096,
+                                  "narrow": [16, 8192, 262144]})
+    assert ("set_narrow_levels", (16, 8192, 262144), {}) in r.calls
+    assert [c[0] for c in r.calls] == ["set_policy", "set_narrow_levels"]
 
 
 def test_successive_halving_finds_the_minimum():
