@@ -28,13 +28,13 @@ def _graphs(b):
     ]
 
 
-def _search(b, prob, src, team, max_frontier, grid_frontier=0, threads=0):
+def _search(b, prob, src, team, max_frontier, grid_frontier=0, threads=0, max_grid=0):
     en = b.make_enactor(CE, INSTRUMENT=True)
     if threads:
         en.set_policy(cta_threads=threads)
     en.set_narrow_levels(team, max_frontier, grid_frontier)
     b.check(prob.Reset(en.GetFrontierType(), 1.3))
-    b.check(en.EnactSearch(prob, int(src)))
+    b.check(en.EnactSearch(prob, int(src), max_grid))
     return prob.labels(), en.GetStatistics(), en
 
 
@@ -57,6 +57,29 @@ def test_narrow_levels_match_oracle(cuda_device, oracle, team):
                 assert oracle.first_mismatch(labels, ref) == -1, case
                 assert stats[:2] == plain_stats[:2], case
                 assert (1 <= en.narrow_team() <= team) if team else en.narrow_team() == 0
+
+
+@pytest.mark.parametrize("max_grid", [1, 2, 5])
+def test_latency_first_levels_on_small_grids(cuda_device, oracle, max_grid):
+    """A grid of a few CTAs makes most levels larger than one round of the
+    latency-first body (a thread per element): levels of many rounds, against
+    the oracle and the plain search's statistics."""
+    b = bfs_mod()
+    for g, sources in _graphs(b):
+        prob = b.CsrProblem(False).from_graph(g)
+        pprob = b.CsrProblem(True).from_graph(g)
+        srcs = sources if sources is not None else [int(s) for s in g.sample_sources(1, 43)]
+        for s in srcs:
+            ref, _ = oracle.bfs(g, int(s))
+            _, plain_stats, _ = _search(b, prob, s, 0, 0, max_grid=max_grid)
+            for threads in (128, 512):
+                labels, stats, _ = _search(b, prob, s, 0, 0, 1 << 24, threads=threads, max_grid=max_grid)
+                case = (g.name, int(s), max_grid, threads)
+                assert oracle.first_mismatch(labels, ref) == -1, case
+                assert stats[:2] == plain_stats[:2], case
+                preds, _, _ = _search(b, pprob, s, 0, 0, 1 << 24, threads=threads, max_grid=max_grid)
+                bad, reason = oracle.check_predecessors(g, preds, ref)
+                assert bad == -1, (case, bad, reason)
 
 
 @pytest.mark.parametrize("threads", [128, 256, 512])
