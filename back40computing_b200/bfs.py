@@ -267,7 +267,7 @@ class _Enactor:
         check(lib().b40c_enactor_set_bottom_up_staging(self._h, int(bool(enable))))
 
     def set_narrow_levels(self, team_ctas: int, max_frontier: int, grid_frontier: int = 0) -> None:
-        """Contract-expand: the first levels of at most max_frontier queued
+        """Contract-expand and hybrid: the first levels of at most max_frontier queued
         edges run on one cluster of team_ctas CTAs (0: none), and full-grid
         levels of at most grid_frontier queued edges run the latency-first
         level body (0: none).  Both off by default."""

@@ -534,7 +534,7 @@ int launch_search(b40c_enactor *e, BfsParams &bp, const KernelConfig &kc, cudaSt
             bp.cta_busy = e->d_busy;
             e->busy_grid = grid;
         }
-        if (kc.strategy == B40C_CONTRACT_EXPAND) bp.flat_max = e->flat_max;
+        if (kc.strategy == B40C_CONTRACT_EXPAND || kc.strategy == B40C_HYBRID) bp.flat_max = e->flat_max;
         if (e->narrow_team > 0) {
             const int key = (kc.threads << 8) | (kc.mark_pred ? 128 : 0) | e->narrow_team;
             if (e->narrow_key != key) {
@@ -543,6 +543,10 @@ int launch_search(b40c_enactor *e, BfsParams &bp, const KernelConfig &kc, cudaSt
             }
             if (e->narrow_got > 0) {
                 bp.narrow_max = e->narrow_max;
+                // The hybrid runs a level above 4 edges per grid thread as two
+                // phases: its narrow levels stay below that.
+                if (kc.strategy == B40C_HYBRID)
+                    bp.narrow_max = unsigned(std::min<long long>(bp.narrow_max, 4ll * kc.threads * grid));
                 CUDA_TRY(launch_narrow(bp, kc, e->narrow_got, s), "cluster launch of the narrow BFS kernel");
             }
         }

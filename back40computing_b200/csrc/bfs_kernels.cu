@@ -1745,16 +1745,18 @@ __device__ void ce_narrow_level(const BfsParams &p, Counters *c, int it, unsigne
 // warps in shared memory: per-warp reservations would put thousands of
 // atomics on the queue length per level.  Labels, queue contents (in another
 // order) and counts are ce_level's.
+// it: the level (the label of a claimed vertex); q: its ring phase (q == it
+// except in the hybrid kernel, whose two-phase levels take two phases).
 template <int THREADS, bool MP>
-__device__ void ce_flat_level(const BfsParams &p, int it, unsigned L, Smem<THREADS, MP> &sm) {
+__device__ void ce_flat_level(const BfsParams &p, int it, int q, unsigned L, Smem<THREADS, MP> &sm) {
     constexpr int NW = THREADS / 32;
     Counters *c = p.ctr;
-    const int *q_in = p.queue[it & 1];
-    const int *pq_in = p.pred_queue[it & 1];
-    const int nq = (it + 1) & 1;
+    const int *q_in = p.queue[q & 1];
+    const int *pq_in = p.pred_queue[q & 1];
+    const int nq = (q + 1) & 1;
     int *q_out = p.queue[nq];
     int *pq_out = p.pred_queue[nq];
-    unsigned *qlen_out = &c->qlen[(it + 1) & 3];
+    unsigned *qlen_out = &c->qlen[(q + 1) & 3];
     const unsigned warp = threadIdx.x >> 5, lane = lane_id();
     const unsigned long long G = gridDim.x, round = G * THREADS;
     unsigned raw = 0;
@@ -1776,7 +1778,7 @@ __device__ void ce_flat_level(const BfsParams &p, int it, unsigned L, Smem<THREA
         const int len = claimed ? r1v - r0v : 0;
         if (p.count_raw) raw += unsigned(len);
         const int st4[4] = {r0v, 0, 0, 0}, ln4[4] = {len, 0, 0, 0}, own4[4] = {u, 0, 0, 0};
-        const unsigned placed = place4<THREADS>(p, it + 1, len > 0 ? 1u : 0u, st4, ln4, own4);
+        const unsigned placed = place4<THREADS>(p, q + 1, len > 0 ? 1u : 0u, st4, ln4, own4);
         const int n = placed ? 0 : len;
         int first[4];
 #pragma unroll
@@ -1810,7 +1812,7 @@ __device__ void ce_flat_level(const BfsParams &p, int it, unsigned L, Smem<THREA
     }
     if (p.count_raw) {
         raw = __reduce_add_sync(FULL, raw);
-        if (lane == 0 && raw) atomicAdd(&c->raw[(it + 1) & 3], raw);
+        if (lane == 0 && raw) atomicAdd(&c->raw[(q + 1) & 3], raw);
     }
 }
 
@@ -1841,7 +1843,7 @@ __device__ __forceinline__ void ce_search(const BfsParams &p) {
             log_phase(p, it, lc.raw ? lc.raw : L, nch, nw);
         }
         if (nch + nw == 0u && L <= p.flat_max)
-            ce_flat_level<THREADS, MP>(p, it, L, sm);
+            ce_flat_level<THREADS, MP>(p, it, it, L, sm);
         else
             ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, pol);
         clk.stop(p);
@@ -2015,9 +2017,12 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
     Counters *c = p.ctr;
     const unsigned long long saturation = 4ull * THREADS * gridDim.x;
     BusyClock clk;
-    int it = 0, q = 0;
-    LevelCounts lc = read_counts(c, 0, false, sm);
-    for (;;) {
+    // A narrow launch (contract-expand levels on one cluster, where the ring
+    // phase is the level) may have run the first levels.
+    int it = __ldcg(&c->resume), q = it;
+    LevelCounts lc = read_counts(c, q, false, sm);
+    const bool failed = ld_relaxed_gpu(&c->error) != 0u;  // as ce_search
+    for (; !failed;) {
         clk.start(p);
         unsigned L = lc.L;
         const unsigned nch = lc.nch, nw = lc.nw;
@@ -2030,7 +2035,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
         // the level's edge frontier as the reference counts it (before the gather-time cull)
         const unsigned long long edges = level_edges<THREADS>(lc);
         if (edges <= saturation) {
-            ce_level<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
+            if (nch + nw == 0u && L <= p.flat_max)
+                ce_flat_level<THREADS, MP>(p, it, q, L, sm);
+            else
+                ce_level<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);
             clk.stop(p);
             log_work_end(p, q);
             if (!grid_barrier(c, p.wait_ns, &sm.flag, next_counts(&sm.lc, q + 1, false))) break;
@@ -2386,9 +2394,11 @@ static KernelFn pick_fused(const KernelConfig &kc) {
     return kc.mark_pred ? fused_fn_t<true>(kc.threads, kc.strategy) : fused_fn_t<false>(kc.threads, kc.strategy);
 }
 
+// The hybrid's first levels are contract-expand levels: the same narrow kernel
+// runs them, and hy_fused_kernel resumes after it.
 template <bool MP>
 static KernelFn narrow_fn_t(int threads, int strategy) {
-    if (strategy != STRATEGY_CONTRACT_EXPAND) return nullptr;
+    if (strategy != STRATEGY_CONTRACT_EXPAND && strategy != STRATEGY_HYBRID) return nullptr;
     switch (threads) {
     case 128: return ce_narrow_kernel<128, MP>;
     case 512: return ce_narrow_kernel<512, MP>;

@@ -1,10 +1,10 @@
-"""Narrow levels (b40c_enactor_set_narrow_levels): contract-expand searches
-whose small levels run on one thread-block cluster, and whose small full-grid
-levels run the latency-first level body, give the oracle's labels and valid
-predecessors, and the same search depth and total_queued as the plain search,
-whether the handover to the full grid comes at the source, in the middle of
-the search, or never, and whichever body each full-grid level runs; other
-strategies ignore the option."""
+"""Narrow levels (b40c_enactor_set_narrow_levels): contract-expand and hybrid
+searches whose small levels run on one thread-block cluster, and whose small
+full-grid levels run the latency-first level body, give the oracle's labels
+and valid predecessors, and the same search depth and total_queued as the
+plain search, whether the handover to the full grid comes at the source, in
+the middle of the search, or never, and whichever body each full-grid level
+runs; the other strategies ignore the option."""
 from __future__ import annotations
 
 import pytest
@@ -12,6 +12,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 CE = 1
+NARROW_STRATEGIES = [1, 3]  # contract-expand, hybrid
 
 
 def bfs_mod():
@@ -28,8 +29,8 @@ def _graphs(b):
     ]
 
 
-def _search(b, prob, src, team, max_frontier, grid_frontier=0, threads=0, max_grid=0):
-    en = b.make_enactor(CE, INSTRUMENT=True)
+def _search(b, prob, src, team, max_frontier, grid_frontier=0, threads=0, max_grid=0, strategy=CE):
+    en = b.make_enactor(strategy, INSTRUMENT=True)
     if threads:
         en.set_policy(cta_threads=threads)
     en.set_narrow_levels(team, max_frontier, grid_frontier)
@@ -38,8 +39,9 @@ def _search(b, prob, src, team, max_frontier, grid_frontier=0, threads=0, max_gr
     return prob.labels(), en.GetStatistics(), en
 
 
+@pytest.mark.parametrize("strategy", NARROW_STRATEGIES)
 @pytest.mark.parametrize("team", [16, 8, 3, 1, 0])
-def test_narrow_levels_match_oracle(cuda_device, oracle, team):
+def test_narrow_levels_match_oracle(cuda_device, oracle, team, strategy):
     b = bfs_mod()
     # (cluster bound, full-grid latency-first bound): handover at the source,
     # after a few levels, never; full-grid levels all tiled, all latency-first,
@@ -50,17 +52,18 @@ def test_narrow_levels_match_oracle(cuda_device, oracle, team):
         srcs = sources if sources is not None else [int(s) for s in g.sample_sources(2, 41)]
         for s in srcs:
             ref, _ = oracle.bfs(g, int(s))
-            _, plain_stats, _ = _search(b, prob, s, 0, 0)
+            _, plain_stats, _ = _search(b, prob, s, 0, 0, strategy=strategy)
             for max_frontier, grid_frontier in settings:
-                labels, stats, en = _search(b, prob, s, team, max_frontier, grid_frontier)
-                case = (g.name, int(s), team, max_frontier, grid_frontier)
+                labels, stats, en = _search(b, prob, s, team, max_frontier, grid_frontier, strategy=strategy)
+                case = (strategy, g.name, int(s), team, max_frontier, grid_frontier)
                 assert oracle.first_mismatch(labels, ref) == -1, case
                 assert stats[:2] == plain_stats[:2], case
                 assert (1 <= en.narrow_team() <= team) if team else en.narrow_team() == 0
 
 
+@pytest.mark.parametrize("strategy", NARROW_STRATEGIES)
 @pytest.mark.parametrize("max_grid", [1, 2, 5])
-def test_latency_first_levels_on_small_grids(cuda_device, oracle, max_grid):
+def test_latency_first_levels_on_small_grids(cuda_device, oracle, max_grid, strategy):
     """A grid of a few CTAs makes most levels larger than one round of the
     latency-first body (a thread per element): levels of many rounds, against
     the oracle and the plain search's statistics."""
@@ -71,19 +74,22 @@ def test_latency_first_levels_on_small_grids(cuda_device, oracle, max_grid):
         srcs = sources if sources is not None else [int(s) for s in g.sample_sources(1, 43)]
         for s in srcs:
             ref, _ = oracle.bfs(g, int(s))
-            _, plain_stats, _ = _search(b, prob, s, 0, 0, max_grid=max_grid)
             for threads in (128, 512):
-                labels, stats, _ = _search(b, prob, s, 0, 0, 1 << 24, threads=threads, max_grid=max_grid)
-                case = (g.name, int(s), max_grid, threads)
+                _, plain_stats, _ = _search(b, prob, s, 0, 0, threads=threads, max_grid=max_grid, strategy=strategy)
+                labels, stats, _ = _search(b, prob, s, 0, 0, 1 << 24, threads=threads, max_grid=max_grid,
+                                           strategy=strategy)
+                case = (strategy, g.name, int(s), max_grid, threads)
                 assert oracle.first_mismatch(labels, ref) == -1, case
                 assert stats[:2] == plain_stats[:2], case
-                preds, _, _ = _search(b, pprob, s, 0, 0, 1 << 24, threads=threads, max_grid=max_grid)
+                preds, _, _ = _search(b, pprob, s, 0, 0, 1 << 24, threads=threads, max_grid=max_grid,
+                                      strategy=strategy)
                 bad, reason = oracle.check_predecessors(g, preds, ref)
                 assert bad == -1, (case, bad, reason)
 
 
+@pytest.mark.parametrize("strategy", NARROW_STRATEGIES)
 @pytest.mark.parametrize("threads", [128, 256, 512])
-def test_narrow_levels_policies_and_predecessors(cuda_device, oracle, threads):
+def test_narrow_levels_policies_and_predecessors(cuda_device, oracle, threads, strategy):
     b = bfs_mod()
     g = b.grid2d(128)
     src = 64 * 128 + 64
@@ -91,15 +97,16 @@ def test_narrow_levels_policies_and_predecessors(cuda_device, oracle, threads):
     prob = b.CsrProblem(False).from_graph(g)
     pprob = b.CsrProblem(True).from_graph(g)
     for team, max_frontier, grid_frontier in ((16, 1 << 20, 0), (0, 0, 1 << 20), (16, 100, 1 << 20)):
-        labels, _, _ = _search(b, prob, src, team, max_frontier, grid_frontier, threads=threads)
+        labels, _, _ = _search(b, prob, src, team, max_frontier, grid_frontier, threads=threads, strategy=strategy)
         assert oracle.first_mismatch(labels, ref) == -1
-        preds, _, _ = _search(b, pprob, src, team, max_frontier, grid_frontier, threads=threads)
+        preds, _, _ = _search(b, pprob, src, team, max_frontier, grid_frontier, threads=threads, strategy=strategy)
         assert preds[src] == -2
         bad, reason = oracle.check_predecessors(g, preds, ref)
         assert bad == -1, f"node {bad} fails check {reason}"
 
 
-def test_narrow_levels_are_logged(cuda_device, oracle):
+@pytest.mark.parametrize("strategy", NARROW_STRATEGIES)
+def test_narrow_levels_are_logged(cuda_device, oracle, strategy):
     """The level log holds every level, the narrow ones included, in order,
     each with its work-end time between its start and the next level's."""
     b = bfs_mod()
@@ -107,7 +114,7 @@ def test_narrow_levels_are_logged(cuda_device, oracle):
     src = 48 * 96 + 48
     ref, _ = oracle.bfs(g, src)
     prob = b.CsrProblem(False).from_graph(g)
-    en = b.make_enactor(CE)
+    en = b.make_enactor(strategy)
     en.set_narrow_levels(8, 40)  # the first levels narrow, then the full grid
     en.set_level_log(True)
     b.check(prob.Reset(en.GetFrontierType(), 1.3))
@@ -120,13 +127,14 @@ def test_narrow_levels_are_logged(cuda_device, oracle):
         assert cur["start_ns"] <= cur["work_end_ns"] <= nxt["start_ns"]
 
 
+@pytest.mark.parametrize("strategy", NARROW_STRATEGIES)
 @pytest.mark.parametrize("setting", [(16, 1 << 20, 0), (0, 0, 1 << 20)])
-def test_narrow_levels_overflow_and_recovery(cuda_device, oracle, setting):
+def test_narrow_levels_overflow_and_recovery(cuda_device, oracle, setting, strategy):
     b = bfs_mod()
     g = b.grid2d(256)
     src = 128 * 256 + 128
     prob = b.CsrProblem(False).from_graph(g)
-    en = b.make_enactor(CE)
+    en = b.make_enactor(strategy)
     en.set_narrow_levels(*setting)
     b.check(prob.Reset(en.GetFrontierType(), 0.0005))
     assert en.EnactSearch(prob, src) == b.bfs.cudaErrorInvalidConfiguration
@@ -147,7 +155,8 @@ def test_narrow_levels_arguments_and_other_strategies(cuda_device, oracle):
     src = 32 * 64 + 32
     ref, _ = oracle.bfs(g, src)
     prob = b.CsrProblem(False).from_graph(g)
-    for strategy in (0, 2, 3):
+    assert b.make_enactor(3).narrow_team() == 0  # off until set
+    for strategy in (0, 2):
         other = b.make_enactor(strategy)
         other.set_narrow_levels(16, 1 << 20, 1 << 20)
         assert other.narrow_team() == 0

@@ -14,11 +14,12 @@ def test_candidates_cover_the_knobs():
     assert {(c["alpha"], c["beta"]) for c in ec} == set(tune.DIRECTIONS)
     assert all("alpha" not in c for c in tune.candidates(1))  # no direction switch off expand-contract
     assert all(c["cta_gather_threshold"] >= c["warp_gather_threshold"] for c in ec)
-    # narrow levels: contract-expand only, every setting with every other knob
-    ce = tune.candidates(1)
-    assert {tuple(c["narrow"]) for c in ce} == set(tune.NARROW)
-    assert len(ce) == len(tune.candidates(2)) * len(tune.NARROW)
-    assert all("narrow" not in c for s in (0, 2, 3) for c in tune.candidates(s))
+    # narrow levels: contract-expand and hybrid only, every setting with every other knob
+    for strategy in (1, 3):
+        ce = tune.candidates(strategy)
+        assert {tuple(c["narrow"]) for c in ce} == set(tune.NARROW)
+        assert len(ce) == len(tune.candidates(2)) * len(tune.NARROW)
+    assert all("narrow" not in c for s in (0, 2) for c in tune.candidates(s))
 
 
 def test_apply_enactor_policy_sets_every_knob():
