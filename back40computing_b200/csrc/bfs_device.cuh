@@ -59,7 +59,11 @@ struct alignas(256) Counters {
     unsigned long long total_queued;  // sum of frontier lengths (instrumented)
     unsigned retired[4];  // multi-search: searches retired at the start of level q, at [q&3]
     int resume;           // level a full-grid fused launch starts at (set by a narrow launch before it)
-    unsigned pad_e[53];
+    // Expand-contract direction-switch state before level `resume` (set by a
+    // narrow launch with the handover; see DirectionChoice).
+    unsigned dir_visited, dir_prev_nf, dir_bottom_up;
+    unsigned long long dir_explored;
+    unsigned pad_e[48];
     // Direction-optimizing expand-contract: the vertices discovered as input of
     // phase q (mf: the sum of their degrees, nf: their number), at [q&3].
     unsigned long long mf[4];

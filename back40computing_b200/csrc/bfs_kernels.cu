@@ -1579,6 +1579,19 @@ struct DirectionChoice {
         prev_nf = nf;
         return bottom_up;
     }
+    // The state handed from a narrow launch to the full-grid one.
+    __device__ __forceinline__ void store(Counters *c) const {
+        c->dir_explored = explored;
+        c->dir_visited = visited;
+        c->dir_prev_nf = prev_nf;
+        c->dir_bottom_up = bottom_up ? 1u : 0u;
+    }
+    __device__ __forceinline__ void load(const Counters *c) {
+        explored = __ldcg(&c->dir_explored);
+        visited = __ldcg(&c->dir_visited);
+        prev_nf = __ldcg(&c->dir_prev_nf);
+        bottom_up = __ldcg(&c->dir_bottom_up) != 0u;
+    }
 };
 
 // The counts a fused kernel's first phase starts from, read once per CTA and
@@ -1608,6 +1621,105 @@ __host__ __device__ constexpr size_t ec_smem_bytes() {
                                      : sizeof(Smem<THREADS, MP>);
 }
 
+// Adds a warp's discovered-vertex degree sum to mf[q] of counters in shared
+// memory (a narrow launch's copy) as a 32-bit add on the low word: degrees
+// of distinct vertices of one graph sum to less than its int32 edge count, so
+// no carry reaches the high word.
+__device__ __forceinline__ void add_mf_low(Counters *c, int q, unsigned m) {
+    atomicAdd(reinterpret_cast<unsigned *>(&c->mf[q & 3]), m);  // little-endian: the low word
+}
+
+// Expand-contract top-down level of a narrow launch, written for latency (as
+// ce_narrow_level): frontier vertex i goes to lane i % 32 of warp i / 32
+// (warps numbered across the cluster's CTAs).  The lane reads its vertex's
+// row range and takes its list (shorter than warp_th: longer ones are in the
+// chunk tables, which hand the level to the full grid) 4 entries at a time:
+// the 4 claims go out together, each claimed neighbour's row range loaded
+// behind its atomic; a discovered vertex is labelled it + 1, its list placed
+// by length (place4: a long one makes the next level the full grid's), and
+// the warp reserves queue room for the rest with one atomicAdd.  c: the
+// level counters (the narrow launch's copy in shared memory).  Labels, queue
+// contents (in another order) and counts are ec_level's.
+template <int THREADS, bool MP>
+__device__ void ec_narrow_level(const BfsParams &p, Counters *c, int it, unsigned L) {
+    const int *q_in = p.queue[it & 1];
+    int *q_out = p.queue[(it + 1) & 1];
+    unsigned *qlen_out = &c->qlen[(it + 1) & 3];
+    const int label = it + 1;
+    const unsigned W = unsigned(grid_warps());
+    const unsigned lane = lane_id(), lt = lanemask_lt();
+    unsigned dn = 0, dm = 0;  // this lane's discovered vertices and their degree sum
+    for (unsigned w = unsigned(global_warp()); w * 32u < L; w += W) {
+        const unsigned i = w * 32u + lane;
+        const bool ok = i < L;
+        const int u = ok ? ld_cg(q_in + i) : 0;
+        const int r0 = ok ? __ldg(p.row_offsets + u) : 0;
+        const int len = ok ? __ldg(p.row_offsets + u + 1) - r0 : 0;
+        for (int k0 = 0; __any_sync(FULL, k0 < len); k0 += 4) {
+            int v[4];
+            unsigned valid = 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                v[j] = k0 + j < len ? __ldg(p.col + r0 + k0 + j) : 0;
+                if (k0 + j < len) {
+                    if ((unsigned)v[j] < (unsigned)p.nodes) valid |= 1u << j;
+                    else atomicOr(&c->error, ERR_BAD_VERTEX);
+                }
+            }
+            unsigned old[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const unsigned bit = 1u << ((unsigned)v[j] & 31u);
+                old[j] = ((valid >> j) & 1u) ? atomicOr(p.mask + ((unsigned)v[j] >> 5), bit) : bit;
+            }
+            int st[4], ln[4];
+            unsigned disc = 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {  // row ranges issued behind the atomics
+                const bool vj = (valid >> j) & 1u;
+                st[j] = vj ? __ldg(p.row_offsets + v[j]) : 0;
+                const int r1 = vj ? __ldg(p.row_offsets + v[j] + 1) : 0;
+                const bool claimed = vj && !(old[j] & (1u << ((unsigned)v[j] & 31u)));
+                if (claimed) {
+                    disc |= 1u << j;
+                    p.labels[v[j]] = MP ? u : label;
+                }
+                ln[j] = claimed ? r1 - st[j] : 0;
+                dm += unsigned(ln[j]);
+            }
+            dn += unsigned(__popc(disc));
+            const unsigned enq = disc & ~place4<THREADS>(p, label, disc, st, ln, v, c);
+            unsigned total = 0, pre[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const unsigned b = __ballot_sync(FULL, (enq >> j) & 1u);
+                pre[j] = total + __popc(b & lt);
+                total += __popc(b);
+            }
+            if (total == 0u) continue;  // warp-uniform
+            unsigned base = 0;
+            if (lane == 0) base = atomicAdd(qlen_out, total);
+            base = __shfl_sync(FULL, base, 0);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if ((enq >> j) & 1u) {
+                    const unsigned long long pos = (unsigned long long)base + pre[j];
+                    if (pos < (unsigned long long)p.qcap) q_out[pos] = v[j];
+                    else atomicOr(&c->error, ERR_OVERFLOW);
+                }
+            }
+        }
+    }
+    if (p.do_alpha) {
+        dn = __reduce_add_sync(FULL, dn);
+        dm = __reduce_add_sync(FULL, dm);
+        if (lane == 0 && dn) {
+            atomicAdd(&c->nf[(it + 1) & 3], dn);
+            add_mf_low(c, it + 1, dm);
+        }
+    }
+}
+
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(BfsParams p) {
     Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
@@ -1630,10 +1742,14 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_fused_kernel(
     Counters *c = p.ctr;
     DirectionChoice dir;
     BusyClock clk;
-    int it = 0;
+    // A narrow launch may have run the first levels: resume after them, with
+    // the direction state they handed over.
+    int it = __ldcg(&c->resume);
+    if (it > 0) dir.load(c);
     const bool dcounts = p.do_alpha != 0u;
-    LevelCounts lc = read_counts(c, 0, dcounts, sm);
-    for (;;) {
+    LevelCounts lc = read_counts(c, it, dcounts, sm);
+    const bool failed = ld_relaxed_gpu(&c->error) != 0u;  // as ce_search
+    for (; !failed;) {
         clk.start(p);
         const unsigned L = lc.L, nch = lc.nch, nw = lc.nw;
         if (stop_level_loop(p, it, L + nch + nw)) break;
@@ -1856,14 +1972,19 @@ __device__ __forceinline__ void ce_search(const BfsParams &p) {
     finish_search(p, it, it);
 }
 
-// A level's counts from counters in shared memory (a narrow launch's).
-__device__ __forceinline__ LevelCounts shared_counts(const Counters *c, int q) {
+// A level's counts from counters in shared memory (a narrow launch's); dir:
+// also the direction switch's counts.
+__device__ __forceinline__ LevelCounts shared_counts(const Counters *c, int q, bool dir = false) {
     const volatile Counters *v = c;
     LevelCounts r{};
     r.L = v->qlen[q & 3];
     r.nch = v->big[q & 3];
     r.nw = v->wch[q & 3];
     r.raw = v->raw[q & 3];
+    if (dir) {
+        r.nf = v->nf[q & 3];
+        r.mf = v->mf[q & 3];
+    }
     return r;
 }
 
@@ -1938,6 +2059,83 @@ __device__ __forceinline__ void ce_narrow_search(const BfsParams &p) {
             g->resume = it;  // the full-grid launch ends the search (or finds it ended)
         }
     }
+}
+
+// The expand-contract level loop of a narrow launch: ce_narrow_search's
+// structure (one cluster, counters in CTA 0's shared memory, levels ending at
+// the cluster's hardware barrier) around ec_narrow_level.  With the
+// direction switch on, each level's direction is decided as the full-grid
+// kernel decides it, on a copy of the state: the first level that would run
+// bottom-up goes to the full grid, with the state as it was before that
+// level (Counters::dir_*), so the full-grid kernel takes the same decisions.
+template <int THREADS, bool MP>
+__device__ __forceinline__ void ec_narrow_search(const BfsParams &p) {
+    __shared__ Counters shared_ctr;  // CTA 0's copy serves the cluster
+    Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
+    Counters *g = p.ctr;
+    constexpr int WORDS = int(offsetof(Counters, sticky) / 4);
+    if (blockIdx.x == 0) {
+        const unsigned *from = reinterpret_cast<const unsigned *>(g);
+        unsigned *to = reinterpret_cast<unsigned *>(&shared_ctr);
+        for (int i = threadIdx.x; i < WORDS; i += THREADS) to[i] = __ldcg(from + i);
+    }
+    cluster_sync_all();
+    Counters *c = cooperative_groups::this_cluster().map_shared_rank(&shared_ctr, 0);
+    const bool dcounts = p.do_alpha != 0u;
+    DirectionChoice dir;  // a search's state before its level 0
+    int it = __ldcg(&g->resume);
+    if (threadIdx.x == 0) sm.lc = shared_counts(c, it, dcounts);
+    __syncthreads();
+    LevelCounts lc = sm.lc;
+    for (;;) {
+        const unsigned L = lc.L, nch = lc.nch, nw = lc.nw;
+        if (L + nch + nw == 0u) break;
+        if (level_limit_hit(it, p.nodes)) {
+            if (leader()) atomicOr(&c->error, ERR_LEVEL_LIMIT);
+            break;
+        }
+        if (nch + nw != 0u || L > p.narrow_max || (long long)L > p.qcap) break;
+        if (dcounts) {
+            DirectionChoice next = dir;
+            if (next.next(p, lc.nf, lc.mf)) break;  // bottom-up: the full grid's level
+            dir = next;
+        }
+        if (leader()) {
+            ring_prepare(c, it);
+            atomicAdd(&g->total_queued, (unsigned long long)L);
+            log_phase(p, it, L, nch, nw, 0u);
+        }
+        ec_narrow_level<THREADS, MP>(p, c, it, L);
+        log_work_end(p, it);
+        cluster_sync_all();
+        if (threadIdx.x == 0) sm.lc = shared_counts(c, it + 1, dcounts);
+        __syncthreads();
+        lc = sm.lc;
+        it++;
+    }
+    cluster_sync_all();  // no CTA touches CTA 0's counters after this
+    if (blockIdx.x == 0 && threadIdx.x < 4) {
+        const int k = threadIdx.x;
+        g->qlen[k] = shared_ctr.qlen[k];
+        g->steal[k] = shared_ctr.steal[k];
+        g->big[k] = shared_ctr.big[k];
+        g->wch[k] = shared_ctr.wch[k];
+        g->raw[k] = shared_ctr.raw[k];
+        g->nf[k] = shared_ctr.nf[k];
+        g->mf[k] = shared_ctr.mf[k];
+        if (k == 0) {
+            if (shared_ctr.error) atomicOr(&g->error, shared_ctr.error);
+            dir.store(g);
+            g->resume = it;
+        }
+    }
+}
+
+// Expand-contract levels of small frontiers on one thread-block cluster,
+// launched before ec_fused_kernel.
+template <int THREADS, bool MP>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_narrow_kernel(BfsParams p) {
+    ec_narrow_search<THREADS, MP>(p);
 }
 
 template <int THREADS, bool MP>
@@ -2395,9 +2593,16 @@ static KernelFn pick_fused(const KernelConfig &kc) {
 }
 
 // The hybrid's first levels are contract-expand levels: the same narrow kernel
-// runs them, and hy_fused_kernel resumes after it.
+// runs them, and hy_fused_kernel resumes after it.  Expand-contract has its own.
 template <bool MP>
 static KernelFn narrow_fn_t(int threads, int strategy) {
+    if (strategy == STRATEGY_EXPAND_CONTRACT) {
+        switch (threads) {
+        case 128: return ec_narrow_kernel<128, MP>;
+        case 512: return ec_narrow_kernel<512, MP>;
+        default: return ec_narrow_kernel<256, MP>;
+        }
+    }
     if (strategy != STRATEGY_CONTRACT_EXPAND && strategy != STRATEGY_HYBRID) return nullptr;
     switch (threads) {
     case 128: return ce_narrow_kernel<128, MP>;

@@ -213,22 +213,26 @@ int b40c_enactor_set_l2_persistence(b40c_enactor_t *enactor, int what);
  * counterpart in the reference, which reads row offsets per tile through the
  * texture path (contract_expand_atomic/cta.cuh:187-207). */
 int b40c_enactor_set_bottom_up_staging(b40c_enactor_t *enactor, int enable);
-/* Narrow levels (contract-expand and hybrid fused searches -- the hybrid's
- * small levels are contract-expand levels; other strategies ignore it), for
- * high-diameter graphs (lattices, road networks), whose levels are a few
- * thousand edges and whose search time is mostly the latency of each level:
- *  - the levels whose input is an edge frontier of at most max_frontier
- *    queued entries, without lists long enough to be cut into chunks, run
+/* Narrow levels (fused searches of expand-contract, contract-expand and the
+ * hybrid, whose small levels are contract-expand levels; two-phase ignores
+ * it), for high-diameter graphs (lattices, road networks), whose levels are a
+ * few thousand edges and whose search time is mostly the latency of each
+ * level:
+ *  - the levels whose input is a frontier (edges, or vertices for
+ *    expand-contract) of at most max_frontier queued entries, without lists
+ *    long enough to be cut into chunks, and, for expand-contract, that the
+ *    direction switch keeps top-down, run
  *    from the source on ONE thread-block cluster of team_ctas CTAs (at most
  *    16, fewer when the device cannot co-schedule that many), whose levels
  *    end at the cluster's hardware barrier; the first larger level and all
  *    after it run on the full persistent grid (team_ctas = 0: all do; the
  *    hybrid's bound is at most its contract-expand bound, 4 edges per grid
  *    thread);
- *  - full-grid levels of at most grid_frontier queued entries without
- *    chunked lists run a latency-first level body (one element per thread,
- *    short lists copied by their own thread, one queue reservation per CTA)
- *    instead of the tiled one (grid_frontier = 0: never).
+ *  - contract-expand and hybrid: full-grid contract-expand levels of at
+ *    most grid_frontier queued entries without chunked lists run a
+ *    latency-first level body (one element per thread, short lists copied by
+ *    their own thread, one queue reservation per CTA) instead of the tiled
+ *    one (grid_frontier = 0: never; expand-contract ignores it).
  * Both are off by default.  Results are the same either way.  No counterpart
  * in the reference. */
 int b40c_enactor_set_narrow_levels(b40c_enactor_t *enactor, int team_ctas, int max_frontier,

@@ -1,10 +1,11 @@
-"""Narrow levels (b40c_enactor_set_narrow_levels): contract-expand and hybrid
-searches whose small levels run on one thread-block cluster, and whose small
-full-grid levels run the latency-first level body, give the oracle's labels
-and valid predecessors, and the same search depth and total_queued as the
-plain search, whether the handover to the full grid comes at the source, in
-the middle of the search, or never, and whichever body each full-grid level
-runs; the other strategies ignore the option."""
+"""Narrow levels (b40c_enactor_set_narrow_levels): expand-contract,
+contract-expand and hybrid searches whose small levels run on one
+thread-block cluster, and whose small full-grid levels run the latency-first
+level body, give the oracle's labels and valid predecessors, and the same
+search depth and total_queued as the plain search, whether the handover to
+the full grid comes at the source, in the middle of the search, or never, and
+whichever body each full-grid level runs (expand-contract with its direction
+switch on, as by default); two-phase ignores the option."""
 from __future__ import annotations
 
 import pytest
@@ -12,7 +13,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 CE = 1
-NARROW_STRATEGIES = [1, 3]  # contract-expand, hybrid
+NARROW_STRATEGIES = [0, 1, 3]  # expand-contract, contract-expand, hybrid
 
 
 def bfs_mod():
@@ -156,10 +157,35 @@ def test_narrow_levels_arguments_and_other_strategies(cuda_device, oracle):
     ref, _ = oracle.bfs(g, src)
     prob = b.CsrProblem(False).from_graph(g)
     assert b.make_enactor(3).narrow_team() == 0  # off until set
-    for strategy in (0, 2):
+    for strategy in (2,):
         other = b.make_enactor(strategy)
         other.set_narrow_levels(16, 1 << 20, 1 << 20)
         assert other.narrow_team() == 0
         b.check(prob.Reset(other.GetFrontierType(), 1.3))
         b.check(other.EnactSearch(prob, src))
         assert oracle.first_mismatch(prob.labels(), ref) == -1
+
+
+@pytest.mark.parametrize("alpha", [1, 14])
+def test_narrow_levels_keep_the_direction_switch(cuda_device, oracle, alpha):
+    """Expand-contract hands its direction-switch state to the full grid: with
+    narrow levels the same levels run bottom-up as without, and labels, depth
+    and total_queued are the same."""
+    b = bfs_mod()
+    for g in (b.rmat(15, 8, seed=4), b.grid2d(120)):
+        prob = b.CsrProblem(False).from_graph(g)
+        for s in g.sample_sources(3, 47):
+            ref, _ = oracle.bfs(g, int(s))
+            runs = []
+            for setting in ((0, 0, 0), (16, 1 << 20, 0), (16, 1 << 20, 1 << 20), (4, 50, 1 << 20)):
+                en = b.make_enactor(0, INSTRUMENT=True)
+                en.set_direction_optimizing(alpha, 24)
+                en.set_narrow_levels(*setting)
+                en.set_level_log(True)
+                b.check(prob.Reset(en.GetFrontierType(), 1.3))
+                b.check(en.EnactSearch(prob, int(s)))
+                assert oracle.first_mismatch(prob.labels(), ref) == -1, (g.name, int(s), setting)
+                runs.append((en.GetStatistics()[:2], [r["bottom_up"] for r in en.level_log()]))
+            assert all(r == runs[0] for r in runs), (g.name, int(s), runs)
+            if alpha == 1 and g.name.startswith("rmat"):
+                assert any(runs[0][1])  # the switch did fire

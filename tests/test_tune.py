@@ -14,12 +14,13 @@ def test_candidates_cover_the_knobs():
     assert {(c["alpha"], c["beta"]) for c in ec} == set(tune.DIRECTIONS)
     assert all("alpha" not in c for c in tune.candidates(1))  # no direction switch off expand-contract
     assert all(c["cta_gather_threshold"] >= c["warp_gather_threshold"] for c in ec)
-    # narrow levels: contract-expand and hybrid only, every setting with every other knob
-    for strategy in (1, 3):
-        ce = tune.candidates(strategy)
-        assert {tuple(c["narrow"]) for c in ce} == set(tune.NARROW)
-        assert len(ce) == len(tune.candidates(2)) * len(tune.NARROW)
-    assert all("narrow" not in c for s in (0, 2) for c in tune.candidates(s))
+    # narrow levels: every strategy but two-phase, every setting with every other knob
+    for strategy in (0, 1, 3):
+        cs = tune.candidates(strategy)
+        assert {tuple(c["narrow"]) for c in cs} == set(tune.NARROW)
+        dirs = len(tune.DIRECTIONS) if strategy == 0 else 1
+        assert len(cs) == len(tune.candidates(2)) * len(tune.NARROW) * dirs
+    assert all("narrow" not in c for c in tune.candidates(2))
 
 
 def test_apply_enactor_policy_sets_every_knob():
