@@ -73,6 +73,15 @@ class EnactorCommon {
         return (cudaError_t)b40c_enactor_set_policy(handle, cta_threads, warp_gather_threshold,
                                                     cta_gather_threshold, cull_flags);
     }
+    /* Options with no counterpart in the reference (b40c_bfs.h): the
+     * expand-contract direction switch (alpha = 0: top-down only), and the
+     * narrow levels of high-diameter searches (team_ctas = 0: off). */
+    cudaError_t SetDirectionOptimizing(int alpha, int beta) {
+        return (cudaError_t)b40c_enactor_set_direction_optimizing(handle, alpha, beta);
+    }
+    cudaError_t SetNarrowLevels(int team_ctas, int max_frontier, int grid_frontier) {
+        return (cudaError_t)b40c_enactor_set_narrow_levels(handle, team_ctas, max_frontier, grid_frontier);
+    }
 
   private:
     EnactorCommon(const EnactorCommon &);

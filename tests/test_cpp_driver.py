@@ -28,6 +28,7 @@ int run(int n, int m, int *col, int *row, int *labels) {
     bfs::CsrProblem<int, int, false> csr_problem;
     if (csr_problem.FromHostProblem(false, n, m, col, row, 1)) return 1;
     bfs::EnactorContractExpand<false> contract_expand(false);
+    if (contract_expand.SetNarrowLevels(16, 8192, 262144)) return 1;  // a lattice setting
     if (csr_problem.Reset(contract_expand.GetFrontierType(), 1.3)) return 1;
     if (contract_expand.EnactFusedSearch(csr_problem, 0)) return 1;
     long long total_queued = 0; int search_depth = 0; double avg_duty = 0;
@@ -39,6 +40,7 @@ int run_g500(int n, int m, long long *col, int *row, long long *labels) {
     bfs::CsrProblem<long long, int, false> csr_problem;
     if (csr_problem.FromHostProblem(false, n, m, col, row, 1)) return 1;
     bfs::EnactorHybrid<false> hybrid(false);
+    if (hybrid.SetDirectionOptimizing(0, 0)) return 1;  // accepted, used by expand-contract only
     if (csr_problem.Reset(hybrid.GetFrontierType(), 1.3)) return 1;
     if (hybrid.EnactSearch(csr_problem, (long long)0)) return 1;
     long long total_queued = 0; long long search_depth = 0; double avg_duty = 0;
