@@ -1850,8 +1850,8 @@ __device__ void ce_narrow_level(const BfsParams &p, Counters *c, int it, unsigne
     }
 }
 
-// Contract-expand level on the full grid for levels of about one queued edge
-// per thread (at most p.flat_max): ce_narrow_level's latency-first body, with
+// Contract-expand level on the full grid for levels of at most one queued
+// edge per thread (flat_level): ce_narrow_level's latency-first body, with
 // element i going to thread i / G of CTA i % G (G = gridDim.x: a small level
 // spreads over every SM), in rounds of G x THREADS elements.  One element per
 // thread and round: these levels are chains of round trips whose length is
@@ -1932,6 +1932,16 @@ __device__ void ce_flat_level(const BfsParams &p, int it, int q, unsigned L, Sme
     }
 }
 
+// Whether a full-grid contract-expand level runs ce_flat_level: no chunked
+// lists, at most p.flat_max queued edges, and at most one per grid thread.
+// A second round of the latency-first body costs more than the tiled body
+// saves (grid3d 256^3: 4.72 ms with levels up to one round, 4.91 ms with
+// levels up to 262,144 edges, 1.7 rounds, on a 296 x 512 grid).
+template <int THREADS>
+__device__ __forceinline__ bool flat_level(const BfsParams &p, unsigned L, unsigned chunks) {
+    return chunks == 0u && L <= p.flat_max && L <= gridDim.x * unsigned(THREADS);
+}
+
 // The contract-expand level loop of the full grid.  It starts at
 // Counters::resume: 0, or the first level a narrow launch before it left.
 template <int THREADS, bool MP>
@@ -1958,7 +1968,7 @@ __device__ __forceinline__ void ce_search(const BfsParams &p) {
             atomicAdd(&c->total_queued, (unsigned long long)lc.raw);
             log_phase(p, it, lc.raw ? lc.raw : L, nch, nw);
         }
-        if (nch + nw == 0u && L <= p.flat_max)
+        if (flat_level<THREADS>(p, L, nch + nw))
             ce_flat_level<THREADS, MP>(p, it, it, L, sm);
         else
             ce_level<THREADS, MP>(p, it, it, L, nch, nw, sm, pol);
@@ -2233,7 +2243,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) hy_fused_kernel(
         // the level's edge frontier as the reference counts it (before the gather-time cull)
         const unsigned long long edges = level_edges<THREADS>(lc);
         if (edges <= saturation) {
-            if (nch + nw == 0u && L <= p.flat_max)
+            if (flat_level<THREADS>(p, L, nch + nw))
                 ce_flat_level<THREADS, MP>(p, it, q, L, sm);
             else
                 ce_level<THREADS, MP>(p, it, q, L, nch, nw, sm, pol);

@@ -229,10 +229,11 @@ int b40c_enactor_set_bottom_up_staging(b40c_enactor_t *enactor, int enable);
  *    hybrid's bound is at most its contract-expand bound, 4 edges per grid
  *    thread);
  *  - contract-expand and hybrid: full-grid contract-expand levels of at
- *    most grid_frontier queued entries without chunked lists run a
- *    latency-first level body (one element per thread, short lists copied by
- *    their own thread, one queue reservation per CTA) instead of the tiled
- *    one (grid_frontier = 0: never; expand-contract ignores it).
+ *    most grid_frontier queued entries, and at most one per grid thread,
+ *    without chunked lists run a latency-first level body (one element per
+ *    thread, short lists copied by their own thread, one queue reservation
+ *    per CTA) instead of the tiled one (grid_frontier = 0: never;
+ *    expand-contract ignores it).
  * Both are off by default.  Results are the same either way.  No counterpart
  * in the reference. */
 int b40c_enactor_set_narrow_levels(b40c_enactor_t *enactor, int team_ctas, int max_frontier,

@@ -65,9 +65,10 @@ def test_narrow_levels_match_oracle(cuda_device, oracle, team, strategy):
 @pytest.mark.parametrize("strategy", NARROW_STRATEGIES)
 @pytest.mark.parametrize("max_grid", [1, 2, 5])
 def test_latency_first_levels_on_small_grids(cuda_device, oracle, max_grid, strategy):
-    """A grid of a few CTAs makes most levels larger than one round of the
-    latency-first body (a thread per element): levels of many rounds, against
-    the oracle and the plain search's statistics."""
+    """On a grid of a few CTAs most levels are larger than one element per
+    grid thread, so they take the tiled body and the small ones the
+    latency-first body, level by level: against the oracle and the plain
+    search's statistics."""
     b = bfs_mod()
     for g, sources in _graphs(b):
         prob = b.CsrProblem(False).from_graph(g)
