@@ -267,10 +267,11 @@ class _Enactor:
         check(lib().b40c_enactor_set_bottom_up_staging(self._h, int(bool(enable))))
 
     def set_narrow_levels(self, team_ctas: int, max_frontier: int, grid_frontier: int = 0) -> None:
-        """Expand-contract, contract-expand and hybrid: the first levels of at most max_frontier queued
-        entries run on one cluster of team_ctas CTAs (0: none), and full-grid
-        levels of at most grid_frontier queued entries run the latency-first
-        level body (0: none).  Both off by default."""
+        """Fused searches: the first levels of at most max_frontier queued
+        entries run on one cluster of team_ctas CTAs (0: none), and
+        (contract-expand, hybrid) full-grid levels of at most grid_frontier
+        queued entries run the latency-first level body (0: none).  Both off
+        by default."""
         check(lib().b40c_enactor_set_narrow_levels(self._h, int(team_ctas), int(max_frontier), int(grid_frontier)))
 
     def narrow_team(self) -> int:

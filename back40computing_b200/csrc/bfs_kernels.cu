@@ -2148,6 +2148,182 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ec_narrow_kernel
     ec_narrow_search<THREADS, MP>(p);
 }
 
+// Two-phase contract phase qi = 2 * it of a narrow launch (latency first, as
+// ce_narrow_level): element i of the edge frontier goes to lane i % 32 of warp
+// i / 32; the lane claims its vertex with one atomicOr, labels it it, and the
+// warp appends the claimed vertices to the vertex queue with one atomicAdd.
+// c: the level counters (the narrow launch's copy in shared memory).
+template <int THREADS, bool MP>
+__device__ void tp_narrow_contract(const BfsParams &p, Counters *c, int it, int qi, unsigned L) {
+    const int *q_in = p.queue[qi & 1];
+    const int *pq_in = p.pred_queue[qi & 1];
+    int *q_out = p.queue[(qi + 1) & 1];
+    unsigned *qlen_out = &c->qlen[(qi + 1) & 3];
+    const unsigned W = unsigned(grid_warps()), lane = lane_id(), lt = lanemask_lt();
+    for (unsigned w = unsigned(global_warp()); w * 32u < L; w += W) {
+        const unsigned i = w * 32u + lane;
+        bool ok = i < L;
+        const int u = ok ? ld_cg(q_in + i) : 0;
+        const int pr = (MP && ok) ? ld_cg(pq_in + i) : 0;
+        if (ok && (unsigned)u >= (unsigned)p.nodes) {
+            atomicOr(&c->error, ERR_BAD_VERTEX);
+            ok = false;
+        }
+        const unsigned bit = 1u << ((unsigned)u & 31u);
+        const bool claimed = ok && !(atomicOr(p.mask + ((unsigned)u >> 5), bit) & bit);
+        if (claimed) p.labels[u] = MP ? pr : it;
+        const unsigned b = __ballot_sync(FULL, claimed);
+        if (b == 0u) continue;  // warp-uniform
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(qlen_out, unsigned(__popc(b)));
+        base = __shfl_sync(FULL, base, 0);
+        if (claimed) {
+            const unsigned long long pos = (unsigned long long)base + __popc(b & lt);
+            if (pos < (unsigned long long)p.qcap) q_out[pos] = u;
+            else atomicOr(&c->error, ERR_OVERFLOW);
+        }
+    }
+}
+
+// Two-phase expand phase qi = 2 * it + 1 of a narrow launch: frontier vertex
+// i goes to lane i % 32 of warp i / 32; its list goes to the chunk tables
+// when long (place4: the next level is then the full grid's), else the warp
+// reserves queue room for its lists with one atomicAdd and each lane copies
+// its own, the first entries loaded while the reservation is in flight.
+template <int THREADS, bool MP>
+__device__ void tp_narrow_expand(const BfsParams &p, Counters *c, int qi, unsigned L) {
+    const int *q_in = p.queue[qi & 1];
+    const int nq = (qi + 1) & 1;
+    int *q_out = p.queue[nq];
+    int *pq_out = p.pred_queue[nq];
+    unsigned *qlen_out = &c->qlen[(qi + 1) & 3];
+    const unsigned W = unsigned(grid_warps()), lane = lane_id();
+    unsigned raw = 0;
+    for (unsigned w = unsigned(global_warp()); w * 32u < L; w += W) {
+        const unsigned i = w * 32u + lane;
+        const bool ok = i < L;
+        const int u = ok ? ld_cg(q_in + i) : 0;
+        const int r0 = ok ? __ldg(p.row_offsets + u) : 0;
+        const int len = ok ? __ldg(p.row_offsets + u + 1) - r0 : 0;
+        if (p.count_raw) raw += unsigned(len);
+        const int st4[4] = {r0, 0, 0, 0}, ln4[4] = {len, 0, 0, 0}, own4[4] = {u, 0, 0, 0};
+        const unsigned placed = place4<THREADS>(p, qi + 1, len > 0 ? 1u : 0u, st4, ln4, own4, c);
+        const int n = placed ? 0 : len;
+        const int incl = warp_inclusive_scan(n);
+        const unsigned total = (unsigned)__shfl_sync(FULL, incl, 31);
+        if (total == 0u) continue;  // warp-uniform
+        int first[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) first[k] = k < n ? __ldg(p.col + r0 + k) : 0;
+        unsigned base = 0;
+        if (lane == 31) base = atomicAdd(qlen_out, total);
+        base = __shfl_sync(FULL, base, 31);
+        const unsigned long long pos = (unsigned long long)base + unsigned(incl - n);
+        for (int k = 0; k < n; k++) {
+            const int v = k == 0 ? first[0] : k == 1 ? first[1] : k == 2 ? first[2] : k == 3 ? first[3]
+                                                                                          : __ldg(p.col + r0 + k);
+            if (pos + k < (unsigned long long)p.qcap) {
+                q_out[pos + k] = v;
+                if (MP) pq_out[pos + k] = u;
+            } else {
+                atomicOr(&c->error, ERR_OVERFLOW);
+            }
+        }
+    }
+    if (p.count_raw) {
+        raw = __reduce_add_sync(FULL, raw);
+        if (lane == 0 && raw) atomicAdd(&c->raw[(qi + 1) & 3], raw);
+    }
+}
+
+// The two-phase level loop of a narrow launch: ce_narrow_search's structure
+// with both phases of a level on the cluster, each ending at the cluster's
+// hardware barrier.  It hands over only before a contract phase (the full-grid
+// kernel resumes at phase 2 * Counters::resume).  A contract phase that
+// discovers nothing ends the search as the reference does (no ++): the narrow
+// launch then finishes it itself (iteration, end marker, sticky error) and sets
+// Counters::resume to -1, so the full-grid launch after it does nothing.
+template <int THREADS, bool MP>
+__device__ __forceinline__ void tp_narrow_search(const BfsParams &p) {
+    __shared__ Counters shared_ctr;  // CTA 0's copy serves the cluster
+    Smem<THREADS, MP> &sm = kernel_smem<THREADS, MP>();
+    Counters *g = p.ctr;
+    constexpr int WORDS = int(offsetof(Counters, sticky) / 4);
+    if (blockIdx.x == 0) {
+        const unsigned *from = reinterpret_cast<const unsigned *>(g);
+        unsigned *to = reinterpret_cast<unsigned *>(&shared_ctr);
+        for (int i = threadIdx.x; i < WORDS; i += THREADS) to[i] = __ldcg(from + i);
+    }
+    cluster_sync_all();
+    Counters *c = cooperative_groups::this_cluster().map_shared_rank(&shared_ctr, 0);
+    int it = __ldcg(&g->resume), qi = 2 * it;
+    bool ended = false;  // a contract phase discovered nothing
+    if (threadIdx.x == 0) sm.lc = shared_counts(c, qi);
+    __syncthreads();
+    LevelCounts lc = sm.lc;
+    for (;;) {
+        const unsigned L = lc.L, nch = lc.nch, nw = lc.nw;
+        if (L + nch + nw + lc.raw == 0u) break;
+        if (level_limit_hit(it, p.nodes)) {
+            if (leader()) atomicOr(&c->error, ERR_LEVEL_LIMIT);
+            break;
+        }
+        if (nch + nw != 0u || L > p.narrow_max || (long long)L > p.qcap) break;
+        if (leader()) {
+            ring_prepare(c, qi);
+            atomicAdd(&g->total_queued, (unsigned long long)lc.raw);
+            log_phase(p, qi, lc.raw ? lc.raw : L, nch, nw);
+        }
+        tp_narrow_contract<THREADS, MP>(p, c, it, qi, L);
+        log_work_end(p, qi);
+        cluster_sync_all();
+        if (threadIdx.x == 0) sm.lc = shared_counts(c, qi + 1);
+        __syncthreads();
+        const unsigned Lv = sm.lc.L;
+        if (Lv == 0u || (long long)Lv > p.qcap) {  // no vertex discovered (or the vertex queue overflowed)
+            ended = true;
+            break;
+        }
+        if (leader()) {
+            ring_prepare(c, qi + 1);
+            log_phase(p, qi + 1, Lv, 0u, 0u);
+        }
+        tp_narrow_expand<THREADS, MP>(p, c, qi + 1, Lv);
+        log_work_end(p, qi + 1);
+        cluster_sync_all();
+        if (threadIdx.x == 0) sm.lc = shared_counts(c, qi + 2);
+        __syncthreads();
+        lc = sm.lc;
+        qi += 2;
+        it++;
+    }
+    cluster_sync_all();  // no CTA touches CTA 0's counters after this
+    if (blockIdx.x == 0 && threadIdx.x < 4) {
+        const int k = threadIdx.x;
+        g->qlen[k] = shared_ctr.qlen[k];
+        g->steal[k] = shared_ctr.steal[k];
+        g->big[k] = shared_ctr.big[k];
+        g->wch[k] = shared_ctr.wch[k];
+        g->raw[k] = shared_ctr.raw[k];
+        if (k == 0) {
+            if (shared_ctr.error) atomicOr(&g->error, shared_ctr.error);
+            g->resume = ended ? -1 : it;
+        }
+    }
+    if (ended && leader()) {  // as tp_fused_kernel's finish after an empty contract
+        g->iteration = it;
+        log_phase(p, qi + 2, 0u, 0u, 0u);  // end-of-search marker
+        atomicOr(&g->sticky, shared_ctr.error | __ldcg(&g->error));
+    }
+}
+
+// Two-phase levels of small frontiers on one thread-block cluster, launched
+// before tp_fused_kernel.
+template <int THREADS, bool MP>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_narrow_kernel(BfsParams p) {
+    tp_narrow_search<THREADS, MP>(p);
+}
+
 template <int THREADS, bool MP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) ce_fused_kernel(BfsParams p) {
     ce_search<THREADS, MP>(p);
@@ -2171,9 +2347,14 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS(THREADS)) tp_fused_kernel(
     const uint64_t pol = column_policy(p);
     Counters *c = p.ctr;
     BusyClock clk;
-    int it = 0, qi = 0;
-    LevelCounts lc = read_counts(c, 0, false, sm);
-    for (;;) {
+    // A narrow launch may have run the first levels (resume), or the whole
+    // search (resume -1: nothing left to do).
+    const int resume = __ldcg(&c->resume);
+    if (resume < 0) return;
+    int it = resume, qi = 2 * resume;
+    LevelCounts lc = read_counts(c, qi, false, sm);
+    const bool failed = ld_relaxed_gpu(&c->error) != 0u;  // as ce_search
+    for (; !failed;) {
         clk.start(p);
         unsigned L = lc.L;
         const unsigned nch = lc.nch, nw = lc.nw;
@@ -2606,6 +2787,13 @@ static KernelFn pick_fused(const KernelConfig &kc) {
 // runs them, and hy_fused_kernel resumes after it.  Expand-contract has its own.
 template <bool MP>
 static KernelFn narrow_fn_t(int threads, int strategy) {
+    if (strategy == STRATEGY_TWO_PHASE) {
+        switch (threads) {
+        case 128: return tp_narrow_kernel<128, MP>;
+        case 512: return tp_narrow_kernel<512, MP>;
+        default: return tp_narrow_kernel<256, MP>;
+        }
+    }
     if (strategy == STRATEGY_EXPAND_CONTRACT) {
         switch (threads) {
         case 128: return ec_narrow_kernel<128, MP>;
@@ -2613,8 +2801,7 @@ static KernelFn narrow_fn_t(int threads, int strategy) {
         default: return ec_narrow_kernel<256, MP>;
         }
     }
-    if (strategy != STRATEGY_CONTRACT_EXPAND && strategy != STRATEGY_HYBRID) return nullptr;
-    switch (threads) {
+    switch (threads) {  // contract-expand, hybrid
     case 128: return ce_narrow_kernel<128, MP>;
     case 512: return ce_narrow_kernel<512, MP>;
     default: return ce_narrow_kernel<256, MP>;

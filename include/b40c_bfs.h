@@ -213,15 +213,14 @@ int b40c_enactor_set_l2_persistence(b40c_enactor_t *enactor, int what);
  * counterpart in the reference, which reads row offsets per tile through the
  * texture path (contract_expand_atomic/cta.cuh:187-207). */
 int b40c_enactor_set_bottom_up_staging(b40c_enactor_t *enactor, int enable);
-/* Narrow levels (fused searches of expand-contract, contract-expand and the
- * hybrid, whose small levels are contract-expand levels; two-phase ignores
+/* Narrow levels (fused searches of every strategy; per-level launches ignore
  * it), for high-diameter graphs (lattices, road networks), whose levels are a
  * few thousand edges and whose search time is mostly the latency of each
  * level:
  *  - the levels whose input is a frontier (edges, or vertices for
  *    expand-contract) of at most max_frontier queued entries, without lists
  *    long enough to be cut into chunks, and, for expand-contract, that the
- *    direction switch keeps top-down, run
+ *    direction switch keeps top-down, run (two-phase: both phases of each)
  *    from the source on ONE thread-block cluster of team_ctas CTAs (at most
  *    16, fewer when the device cannot co-schedule that many), whose levels
  *    end at the cluster's hardware barrier; the first larger level and all

@@ -1,11 +1,11 @@
-"""Narrow levels (b40c_enactor_set_narrow_levels): expand-contract,
-contract-expand and hybrid searches whose small levels run on one
-thread-block cluster, and whose small full-grid levels run the latency-first
-level body, give the oracle's labels and valid predecessors, and the same
-search depth and total_queued as the plain search, whether the handover to
-the full grid comes at the source, in the middle of the search, or never, and
-whichever body each full-grid level runs (expand-contract with its direction
-switch on, as by default); two-phase ignores the option."""
+"""Narrow levels (b40c_enactor_set_narrow_levels): searches of every strategy
+whose small levels run on one thread-block cluster, and whose small full-grid
+levels run the latency-first level body (contract-expand, hybrid), give the
+oracle's labels and valid predecessors, and the same search depth and
+total_queued as the plain search, whether the handover to the full grid comes
+at the source, in the middle of the search, or never (two-phase searches that
+end on the cluster included), and whichever body each full-grid level runs
+(expand-contract with its direction switch on, as by default)."""
 from __future__ import annotations
 
 import pytest
@@ -13,7 +13,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 CE = 1
-NARROW_STRATEGIES = [0, 1, 3]  # expand-contract, contract-expand, hybrid
+NARROW_STRATEGIES = [0, 1, 2, 3]  # expand-contract, contract-expand, two-phase, hybrid
 
 
 def bfs_mod():
@@ -109,23 +109,28 @@ def test_narrow_levels_policies_and_predecessors(cuda_device, oracle, threads, s
 
 @pytest.mark.parametrize("strategy", NARROW_STRATEGIES)
 def test_narrow_levels_are_logged(cuda_device, oracle, strategy):
-    """The level log holds every level, the narrow ones included, in order,
-    each with its work-end time between its start and the next level's."""
+    """The level log of a search with narrow levels holds the same records as
+    the plain search's (one per level, one per phase for two-phase: frontier,
+    chunk counts, direction, end marker), the narrow ones included, each with
+    its work-end time between its start and the next record's."""
     b = bfs_mod()
     g = b.grid2d(96)
     src = 48 * 96 + 48
     ref, _ = oracle.bfs(g, src)
     prob = b.CsrProblem(False).from_graph(g)
-    en = b.make_enactor(strategy)
-    en.set_narrow_levels(8, 40)  # the first levels narrow, then the full grid
-    en.set_level_log(True)
-    b.check(prob.Reset(en.GetFrontierType(), 1.3))
-    b.check(en.EnactSearch(prob, src))
-    assert oracle.first_mismatch(prob.labels(), ref) == -1
-    log = en.level_log()
-    _, depth, _ = en.GetStatistics()
-    assert len(log) == depth + 2  # levels 0..depth and the end marker
-    for cur, nxt in zip(log[:-1], log[1:]):
+    logs = []
+    for setting in ((0, 0, 0), (8, 40, 0)):  # plain; the first levels narrow, then the full grid
+        en = b.make_enactor(strategy)
+        en.set_narrow_levels(*setting)
+        en.set_level_log(True)
+        b.check(prob.Reset(en.GetFrontierType(), 1.3))
+        b.check(en.EnactSearch(prob, src))
+        assert oracle.first_mismatch(prob.labels(), ref) == -1
+        logs.append(en.level_log())
+    plain, narrow = logs
+    keys = ("frontier", "chunks", "wchunks", "bottom_up")
+    assert [tuple(r[k] for k in keys) for r in narrow] == [tuple(r[k] for k in keys) for r in plain]
+    for cur, nxt in zip(narrow[:-1], narrow[1:]):
         assert cur["start_ns"] <= cur["work_end_ns"] <= nxt["start_ns"]
 
 
@@ -146,24 +151,32 @@ def test_narrow_levels_overflow_and_recovery(cuda_device, oracle, setting, strat
     assert oracle.first_mismatch(prob.labels(), ref) == -1
 
 
-def test_narrow_levels_arguments_and_other_strategies(cuda_device, oracle):
+def test_narrow_levels_arguments(cuda_device):
     b = bfs_mod()
     en = b.make_enactor(CE)
     for bad in ((17, 100, 0), (-1, 100, 0), (4, -1, 0), (4, 100, -1)):
         with pytest.raises(b.BfsError):
             en.set_narrow_levels(*bad)
-    assert en.narrow_team() == 0
-    g = b.grid2d(64)
-    src = 32 * 64 + 32
+    for strategy in NARROW_STRATEGIES:
+        other = b.make_enactor(strategy)
+        assert other.narrow_team() == 0  # off until set
+        other.set_narrow_levels(8, 100)
+        assert 1 <= other.narrow_team() <= 8
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_narrow_levels_leave_the_iterative_variant_alone(cuda_device, oracle, variant):
+    """Per-level launches ignore the setting; fused searches use it."""
+    b = bfs_mod()
+    g = b.grid2d(80)
+    src = 40 * 80 + 40
     ref, _ = oracle.bfs(g, src)
     prob = b.CsrProblem(False).from_graph(g)
-    assert b.make_enactor(3).narrow_team() == 0  # off until set
-    for strategy in (2,):
-        other = b.make_enactor(strategy)
-        other.set_narrow_levels(16, 1 << 20, 1 << 20)
-        assert other.narrow_team() == 0
-        b.check(prob.Reset(other.GetFrontierType(), 1.3))
-        b.check(other.EnactSearch(prob, src))
+    for strategy in (0, 1, 2):
+        en = b.make_enactor(strategy)
+        en.set_narrow_levels(16, 1 << 20, 1 << 20)
+        b.check(prob.Reset(en.GetFrontierType(), 1.3))
+        b.check(en.EnactFusedSearch(prob, src) if variant == 1 else en.EnactIterativeSearch(prob, src))
         assert oracle.first_mismatch(prob.labels(), ref) == -1
 
 

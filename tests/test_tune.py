@@ -14,13 +14,13 @@ def test_candidates_cover_the_knobs():
     assert {(c["alpha"], c["beta"]) for c in ec} == set(tune.DIRECTIONS)
     assert all("alpha" not in c for c in tune.candidates(1))  # no direction switch off expand-contract
     assert all(c["cta_gather_threshold"] >= c["warp_gather_threshold"] for c in ec)
-    # narrow levels: every strategy but two-phase, every setting with every other knob
-    for strategy in (0, 1, 3):
+    # narrow levels: every strategy, every setting with every other knob
+    base = len([1 for t in tune.CTA_THREADS for w in tune.WARP_THRESHOLDS for c in tune.CTA_THRESHOLDS if c >= w])
+    for strategy in (0, 1, 2, 3):
         cs = tune.candidates(strategy)
         assert {tuple(c["narrow"]) for c in cs} == set(tune.NARROW)
         dirs = len(tune.DIRECTIONS) if strategy == 0 else 1
-        assert len(cs) == len(tune.candidates(2)) * len(tune.NARROW) * dirs
-    assert all("narrow" not in c for c in tune.candidates(2))
+        assert len(cs) == base * len(tune.NARROW) * dirs
 
 
 def test_apply_enactor_policy_sets_every_knob():
