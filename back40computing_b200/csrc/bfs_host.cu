@@ -536,7 +536,9 @@ int launch_search(b40c_enactor *e, BfsParams &bp, const KernelConfig &kc, cudaSt
         }
         if (kc.strategy == B40C_CONTRACT_EXPAND || kc.strategy == B40C_HYBRID) bp.flat_max = e->flat_max;
         if (e->narrow_team > 0) {
-            const int key = (kc.threads << 8) | (kc.mark_pred ? 128 : 0) | e->narrow_team;
+            // the launch's shared memory depends on all but the team: a new
+            // configuration is checked (and opted in) before its first launch
+            const int key = (kc.threads << 8) | (kc.mark_pred ? 128 : 0) | (kc.stage_bu ? 64 : 0) | e->narrow_team;
             if (e->narrow_key != key) {
                 CUDA_TRY(narrow_team_limit(kc, e->narrow_team, &e->narrow_got), "cluster occupancy query");
                 e->narrow_key = key;

@@ -232,7 +232,7 @@ int b40c_enactor_set_bottom_up_staging(b40c_enactor_t *enactor, int enable);
  *    without chunked lists run a latency-first level body (one element per
  *    thread, short lists copied by their own thread, one queue reservation
  *    per CTA) instead of the tiled one (grid_frontier = 0: never;
- *    expand-contract ignores it).
+ *    expand-contract and two-phase ignore it).
  * Both are off by default.  Results are the same either way.  No counterpart
  * in the reference. */
 int b40c_enactor_set_narrow_levels(b40c_enactor_t *enactor, int team_ctas, int max_frontier,
