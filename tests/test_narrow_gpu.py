@@ -203,3 +203,29 @@ def test_narrow_levels_keep_the_direction_switch(cuda_device, oracle, alpha):
             assert all(r == runs[0] for r in runs), (g.name, int(s), runs)
             if alpha == 1 and g.name.startswith("rmat"):
                 assert any(runs[0][1])  # the switch did fire
+
+
+def test_narrow_levels_with_bottom_up_staging(cuda_device, oracle):
+    """One expand-contract enactor with narrow levels on, its bottom-up
+    staging switched on and off between searches (the staging changes the
+    kernels' shared memory, so each configuration is checked before its first
+    narrow launch): labels and statistics stay the plain search's."""
+    b = bfs_mod()
+    g = b.rmat(15, 8, seed=4)
+    prob = b.CsrProblem(False).from_graph(g)
+    en = b.make_enactor(0, INSTRUMENT=True)
+    en.set_direction_optimizing(1, 24)
+    en.set_narrow_levels(16, 1 << 20)
+    plain = b.make_enactor(0, INSTRUMENT=True)
+    plain.set_direction_optimizing(1, 24)
+    for staged in (False, True, False, True):
+        en.set_bottom_up_staging(staged)
+        for s in g.sample_sources(2, 53):
+            ref, _ = oracle.bfs(g, int(s))
+            b.check(prob.Reset(plain.GetFrontierType(), 1.3))
+            b.check(plain.EnactSearch(prob, int(s)))
+            stats = plain.GetStatistics()[:2]
+            b.check(prob.Reset(en.GetFrontierType(), 1.3))
+            b.check(en.EnactSearch(prob, int(s)))
+            assert oracle.first_mismatch(prob.labels(), ref) == -1, (staged, int(s))
+            assert en.GetStatistics()[:2] == stats, (staged, int(s))
