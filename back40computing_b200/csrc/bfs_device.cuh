@@ -16,6 +16,7 @@
 //     cta.cuh:213-258, backed by a label check, :264-304).
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -77,6 +78,12 @@ struct alignas(256) Counters {
     unsigned pad_g[59];
     unsigned sticky;  // OR of error over searches since the host last read it (not reset per search)
 };
+// Each group of counters above fills its own 256-byte block: a new field
+// takes padding of its block, never the next block's place.
+static_assert(sizeof(Counters) == 2048, "Counters: 8 blocks of 256 bytes");
+static_assert(offsetof(Counters, error) == 1280 && offsetof(Counters, mf) == 1536 &&
+                  offsetof(Counters, bar_count) == 1792 && offsetof(Counters, sticky) == 2044,
+              "Counters: block boundaries");
 
 // ---- PTX helpers ---------------------------------------------------------------
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
