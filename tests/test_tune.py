@@ -102,3 +102,32 @@ def test_tuned_policies_keep_labels(cuda_device, oracle):
     batch.run(gids, srcs)
     for i, (k, s) in enumerate(zip(gids, srcs)):
         assert oracle.first_mismatch(batch.labels(i), oracle.bfs(graphs[k], s)[0]) == -1
+
+
+@pytest.mark.gpu
+def test_shipped_policies_keep_labels(cuda_device, oracle):
+    """Every single-search policy the package ships (tuned on a B200 for the
+    bench graphs), applied to small graphs of each kind: the oracle's labels."""
+    import json
+    import back40computing_b200 as b
+    from back40computing_b200 import tune
+    table = json.loads(tune.SHIPPED.read_text())
+    graphs = [(b.grid2d(100), 50 * 100 + 50), (b.grid3d(20), 0), (b.rmat(12, 16, seed=3), None)]
+    refs = []
+    for g, s in graphs:
+        s = int(g.sample_sources(1, 9)[0]) if s is None else s
+        refs.append((g, s, oracle.bfs(g, s)[0], b.CsrProblem(False).from_graph(g), b.CsrProblem(True).from_graph(g)))
+    keys = [k for k in table if k.startswith("enactor/")]
+    assert keys
+    for key in keys:
+        strategy = int(key.split("/")[1])
+        en = b.make_enactor(strategy)
+        tune.apply_enactor_policy(en, table[key]["policy"])
+        for g, s, ref, prob, pprob in refs:
+            b.check(prob.Reset(en.GetFrontierType(), 1.3))
+            b.check(en.EnactSearch(prob, s))
+            assert oracle.first_mismatch(prob.labels(), ref) == -1, (key, g.name)
+            b.check(pprob.Reset(en.GetFrontierType(), 1.3))
+            b.check(en.EnactSearch(pprob, s))
+            bad, reason = oracle.check_predecessors(g, pprob.labels(), ref)
+            assert bad == -1, (key, g.name, bad, reason)
