@@ -54,6 +54,31 @@ def test_successive_halving_finds_the_minimum():
     assert len(calls) < 40 * 3  # later rounds measure only the leaders
 
 
+def test_shipped_table_is_well_formed():
+    """The shipped tunings: keys of the cache's form, knobs within the ranges
+    the library's setters accept (checked here, without a GPU)."""
+    import json
+    from back40computing_b200 import tune
+    table = json.loads(tune.SHIPPED.read_text())
+    assert table
+    for key, entry in table.items():
+        kind, rest = key.split("/", 1)
+        assert kind in ("enactor", "batch"), key
+        pol, ms = entry["policy"], entry["ms"]
+        assert ms > 0
+        assert pol["cta_threads"] in tune.CTA_THREADS
+        assert pol["warp_gather_threshold"] in tune.WARP_THRESHOLDS
+        assert pol["cta_gather_threshold"] in tune.CTA_THRESHOLDS
+        if kind == "enactor":
+            strategy, sig = rest.split("/", 1)
+            assert int(strategy) in (0, 1, 2, 3) and sig.startswith("n2^"), key
+            if "alpha" in pol:
+                assert int(strategy) == 0 and (pol["alpha"], pol["beta"]) in tune.DIRECTIONS, key
+            if "narrow" in pol:
+                team, max_frontier, grid_frontier = pol["narrow"]
+                assert 0 <= team <= 16 and max_frontier >= 0 and grid_frontier >= 0, key
+
+
 def test_cache_round_trip(tmp_path):
     from back40computing_b200 import tune
     path = tmp_path / "tune.json"
